@@ -1,0 +1,334 @@
+"""H_eff matvec benchmark (the m=1024 U(1) microbench) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--prec fp64] [--impl dmrgx|reference]
+
+One step = one application of the two-site effective Hamiltonian
+H_eff psi = (L W)((W R) psi) to one wavefunction of the synthetic microbench
+(m_l = m_r = 1024 in nine U(1) sectors, d = 2, MPO bond D = 5; 599,964-element
+psi, 190 + 190 block GEMMs, 3.862 GFLOP).  Inputs are resident in HBM; L2 is
+flushed (a 256 MiB write) between timed steps, outside the timed events.
+Multi-GPU runs are independent replicas (one process per GPU, no collective on
+the data path); the value is the total over ranks divided by the slowest
+rank's device time.
+
+Printed once by rank 0, one JSON line; see the keys below.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "H_eff matvec/s at m=1024 (U(1) microbench, two-site, D=5)"
+UNIT = "matvec/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--prec", default="fp64", choices=["fp64", "bf16x3", "tf32x3"])
+    p.add_argument("--impl", default="dmrgx", choices=["dmrgx", "reference"])
+    p.add_argument("--cpu-sample-s", type=float, default=12.0)
+    return p.parse_args()
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def fp64_gemm_peak(torch, dev):
+    """cuBLAS DGEMM 8192^3 burst on this GPU: the FP64 tensor-core ceiling,
+    measured in-run (the driver's peak file carries no FP64 figure)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * n ** 3 / best / 1e12
+
+
+def cpu_reference_rate(sample_s: float, w=None):
+    """The reference's CPU av (src/core.cpp:22-31: get_map task lists executed as
+    serial BLAS GEMMs, OpenBLAS on all host threads) on this workload.
+    Uses the reference build (oracle/_ref) when present, else the numpy port."""
+    from oracle import refbind
+    from dmrg_b200 import workloads
+    if w is None:
+        w = workloads.microbench(1024)
+    threads = os.cpu_count() or 1
+    if refbind.available("u1"):
+        R = refbind.Ref("u1")
+        le, re_ = R.py_to_qt(0, *w["lenv"]), R.py_to_qt(0, *w["renv"])
+        import ctypes as C
+        info = (C.c_int * 4)()
+        box = R.lib.oref_pv_build(0, le, re_, 3, 2, w["sector"], info)
+        n = info[0]
+        x = workloads.random_psi(n, seed=1)
+        y = np.zeros(n)
+        R.lib.oref_av(0, box, x.ctypes.data, y.ctypes.data)  # warm-up
+        cnt, t0 = 0, time.perf_counter()
+        while True:
+            R.lib.oref_av(0, box, x.ctypes.data, y.ctypes.data)
+            cnt += 1
+            el = time.perf_counter() - t0
+            if el >= sample_s or cnt >= 2000:
+                break
+        R.lib.oref_pv_free(0, box)
+        return dict(value=cnt / el, unit=UNIT, cores=threads, kind="reference",
+                    sample=f"{cnt} reference av() calls on the m=1024 microbench in {el:.1f} s "
+                           f"(reference get_map+av built from its sources, OpenBLAS "
+                           f"{threads} threads)")
+    from oracle import restate
+    from dmrg_b200 import native
+    n, ds, rmap, lmap = native.build_maps(w["lenv"][0], w["renv"][0], 3, 2, w["sector"], 32, 0)
+    le = restate.QT.from_ibuf(*w["lenv"])
+    re_ = restate.QT.from_ibuf(*w["renv"])
+    x = workloads.random_psi(n, seed=1)
+    cnt, t0 = 0, time.perf_counter()
+    while True:
+        st = np.zeros(ds)
+        restate.contract_map(re_, st, x, rmap, 2)
+        y = np.zeros(n)
+        restate.contract_map(le, y, st, lmap, 3)
+        cnt += 1
+        el = time.perf_counter() - t0
+        if el >= sample_s or cnt >= 2000:
+            break
+    return dict(value=cnt / el, unit=UNIT, cores=threads, kind="port",
+                sample=f"{cnt} numpy-port matvecs on the m=1024 microbench in {el:.1f} s")
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    from dmrg_b200 import workloads
+    w = workloads.microbench(1024)
+    rates = []
+    cb = cpu_reference_rate(min(2.0, args.cpu_sample_s), w)  # warm-up pass
+    t0 = time.perf_counter()
+    per = []
+    for _ in range(args.steps):
+        r = cpu_reference_rate(0.0, w)
+        per.append(1.0 / r["value"])
+    el = time.perf_counter() - t0
+    value = args.steps / sum(per)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(per) / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "H_eff matvec microbench m=1024, 9 U(1) sectors, d=2, D=5",
+                       "psi_elems": 599964, "tasks": [190, 190], "gflop_per_matvec": 3.862},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cb["cores"],
+                             "kind": cb["kind"], "sample": f"{args.steps} single-matvec steps; "
+                             + cb["sample"].split(";")[0]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "wall_s": el}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args)
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    from dmrg_b200 import native, workloads
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    prec = {"fp64": native.PREC_FP64, "bf16x3": native.PREC_BF16X3,
+            "tf32x3": native.PREC_TF32X3}[args.prec]
+
+    w = workloads.microbench(1024)
+    ctx = native.Context(native.F64, local)
+    ctx.set_precision(prec)
+    ctx.plan_build(w["lenv"], w["renv"], 3, 2, w["sector"], 32, 0)
+    n, flops = ctx.n, ctx.flops
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+
+    xs = torch.tensor(workloads.random_psi(n, seed=5), device=dev)
+    ys = torch.empty_like(xs)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+
+    def step_device(timed):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            if timed:
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record(stream)
+            ctx.av_device(xs.data_ptr(), ys.data_ptr())
+            if timed:
+                e.record(stream)
+                return s, e
+        return None
+
+    for _ in range(args.warmup):
+        step_device(False)
+    torch.cuda.synchronize()
+
+    try:
+        clocks = Clocks("GPU-" + str(torch.cuda.get_device_properties(dev).uuid))
+    except Exception:
+        clocks = Clocks(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    evs = [step_device(True) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    dev_s = sum(s.elapsed_time(e) for s, e in evs) / 1e3
+    if world > 1:
+        t = torch.tensor([dev_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_s = float(t.item())
+    per = dev_s / args.steps
+    value = world * args.steps / dev_s
+
+    # end to end through the C ABI with host buffers (copies inside the timing)
+    xh = workloads.random_psi(n, seed=6)
+    for _ in range(2):
+        ctx.av(xh)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        yh = ctx.av(xh)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    if rank == 0:
+        peaks, src = measured_peaks()
+        if args.prec == "fp64":
+            pk = fp64_gemm_peak(torch, dev)
+            peak_unit, bound = "TFLOP/s", "tensor"
+            peak_note = "in-run cuBLAS DGEMM 8192^3 burst (FP64 tensor cores)"
+        else:
+            pk = peaks["bf16_tflops"]
+            peak_unit, bound = "TFLOP/s", "tensor"
+            peak_note = f"bf16_tflops of MEASURED_PEAKS.json ({src})"
+        achieved = flops / per / 1e12
+        cpu = cpu_reference_rate(args.cpu_sample_s, w)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.prec == "fp64" else args.prec, "data": "synthetic",
+            "config": {"workload": "H_eff matvec microbench m=1024, 9 U(1) sectors, d=2, D=5",
+                       "psi_elems": n, "tasks": [ctx.n_rmap, ctx.n_lmap],
+                       "gflop_per_matvec": flops / 1e9, "precision": args.prec,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "flushed (256 MiB write) before every timed step"},
+            "roofline": {"bound": bound, "achieved": achieved, "peak": pk, "unit": peak_unit,
+                         "frac": achieved / pk, "traffic": None,
+                         "kernel": "grouped_gemm_nt_f64 (both stages)",
+                         "peak_source": peak_note},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * args.steps / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8},
+            "gpu_launches": 2 * args.steps,
+            "clocks": ck,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

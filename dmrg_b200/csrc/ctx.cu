@@ -1,0 +1,533 @@
+// C ABI of libdmrgx: contexts, plans, the H_eff matvec.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <string>
+
+#include "../../include/dmrgx.h"
+#include "ctx.h"
+#include "kernels.h"
+
+using namespace dmrgx;
+
+namespace dmrgx {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+
+void Stage::free_device() {
+  cudaFree(d_outs);
+  cudaFree(d_segs);
+  cudaFree(d_tiles);
+  d_outs = nullptr;
+  d_segs = nullptr;
+  d_tiles = nullptr;
+}
+
+cudaError_t DevBuf::ensure(size_t b) {
+  if (b <= bytes && p) return cudaSuccess;
+  release();
+  cudaError_t e = cudaMalloc(&p, b ? b : 16);
+  if (e == cudaSuccess) bytes = b;
+  return e;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+}  // namespace dmrgx
+
+#define CUDA_TRY(expr)                                                              \
+  do {                                                                              \
+    cudaError_t e_ = (expr);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      set_error(std::string(#expr) + ": " + cudaGetErrorString(e_));                \
+      return DMRGX_E_CUDA;                                                          \
+    }                                                                               \
+  } while (0)
+
+#define ARG_CHECK(cond, msg)  \
+  do {                        \
+    if (!(cond)) {            \
+      set_error(msg);         \
+      return DMRGX_E_ARG;     \
+    }                         \
+  } while (0)
+
+namespace {
+
+// Environment image on the host with the task signs folded into the blocks:
+// a block used only with alpha=-1 is stored negated, a block used with both
+// signs gets a negated copy appended.  plus/minus: real offsets per block.
+struct EnvImage {
+  std::vector<double> vals;
+  std::vector<int64_t> plus, minus;
+};
+
+EnvImage make_image(const double* src, const std::vector<int64_t>& off,
+                    const std::vector<int64_t>& size, const std::vector<MapRow>& rows, int f) {
+  const size_t nb = size.size();
+  std::vector<int> use(nb, 0);
+  for (auto& r : rows) use[r.blk] |= (r.alpha >= 0 ? 1 : 2);
+  EnvImage im;
+  int64_t total = off.empty() ? 0 : off.back();
+  int64_t extra = 0;
+  for (size_t b = 0; b < nb; b++)
+    if (use[b] == 3) extra += size[b];
+  im.vals.resize((size_t)(total + extra) * f);
+  std::memcpy(im.vals.data(), src, sizeof(double) * (size_t)total * f);
+  im.plus.assign(nb, -1);
+  im.minus.assign(nb, -1);
+  int64_t tail = total * f;
+  for (size_t b = 0; b < nb; b++) {
+    const int64_t o = off[b] * f, s = size[b] * f;
+    if (use[b] == 2) {
+      for (int64_t i = 0; i < s; i++) im.vals[o + i] = -im.vals[o + i];
+      im.minus[b] = o;
+    } else if (use[b] == 3) {
+      im.plus[b] = o;
+      for (int64_t i = 0; i < s; i++) im.vals[tail + i] = -im.vals[o + i];
+      im.minus[b] = tail;
+      tail += s;
+    } else {
+      im.plus[b] = o;
+    }
+  }
+  return im;
+}
+
+std::string build_stage(const std::vector<MapRow>& rows, const std::vector<int64_t>& blk_size,
+                        const EnvImage& im, int f, int64_t in_len, int64_t out_len, Stage& st,
+                        int64_t& flops) {
+  st.outs.clear();
+  st.segs.clear();
+  st.tiles.clear();
+  std::map<int64_t, int> by_off;  // output offset -> out index
+  std::vector<std::vector<DSeg>> per_out;
+  for (auto& r : rows) {
+    if (r.blk < 0 || r.blk >= (int)blk_size.size()) return "task row: block index out of range";
+    if (r.cols <= 0 || r.rows < 0) return "task row: bad rows/cols";
+    const int64_t S = blk_size[r.blk];
+    const int64_t K = r.cols, N = r.rows;
+    if (S % K) return "task row: block size is not a multiple of cols";
+    const int64_t M = S / K;
+    if (r.in_beg < 0 || r.in_beg + N * K > in_len) return "task row: input range out of bounds";
+    if (r.out_beg < 0 || r.out_beg + M * N > out_len) return "task row: output range out of bounds";
+    if (M * f > INT32_MAX || N * f > INT32_MAX || K * f > INT32_MAX)
+      return "task row: block extent too large";
+    auto it = by_off.find(r.out_beg);
+    int oi;
+    if (it == by_off.end()) {
+      oi = (int)st.outs.size();
+      by_off[r.out_beg] = oi;
+      DOut o;
+      o.c_off = r.out_beg * f;
+      o.m = (int32_t)M;
+      o.n = (int32_t)(N * f);
+      o.seg_begin = 0;
+      o.seg_count = 0;
+      st.outs.push_back(o);
+      per_out.emplace_back();
+    } else {
+      oi = it->second;
+      if (st.outs[oi].m != M || st.outs[oi].n != N * f)
+        return "task rows writing one output block disagree on its shape";
+    }
+    DSeg sg;
+    sg.a_off = r.alpha >= 0 ? im.plus[r.blk] : im.minus[r.blk];
+    sg.b_off = r.in_beg * f;
+    sg.k = (int32_t)(K * f);
+    sg.pad_ = 0;
+    per_out[oi].push_back(sg);
+    flops += 2 * M * N * K * (f == 2 ? 4 : 1);
+  }
+  int64_t covered = 0;
+  for (size_t o = 0; o < st.outs.size(); o++) {
+    st.outs[o].seg_begin = (int32_t)st.segs.size();
+    st.outs[o].seg_count = (int32_t)per_out[o].size();
+    st.segs.insert(st.segs.end(), per_out[o].begin(), per_out[o].end());
+    covered += (int64_t)st.outs[o].m * st.outs[o].n / f;
+  }
+  st.full_cover = covered == out_len;
+  // tiles, heaviest first
+  const int BM = f64_tile_m(), BN = f64_tile_n(), BK = f64_tile_k();
+  std::vector<std::pair<int64_t, DTile>> tl;
+  for (size_t o = 0; o < st.outs.size(); o++) {
+    int64_t kt = 0;
+    for (int s = 0; s < st.outs[o].seg_count; s++) kt += (st.segs[st.outs[o].seg_begin + s].k + BK - 1) / BK;
+    const int tm = (st.outs[o].m + BM - 1) / BM, tn = (st.outs[o].n + BN - 1) / BN;
+    if (tm > 32767 || tn > 32767) return "output block too large for the tile grid";
+    for (int a = 0; a < tm; a++)
+      for (int b = 0; b < tn; b++) {
+        DTile t;
+        t.out = (int32_t)o;
+        t.tm = (int16_t)a;
+        t.tn = (int16_t)b;
+        tl.push_back({kt, t});
+      }
+  }
+  std::stable_sort(tl.begin(), tl.end(),
+                   [](const std::pair<int64_t, DTile>& x, const std::pair<int64_t, DTile>& y) {
+                     return x.first > y.first;
+                   });
+  for (auto& p : tl) st.tiles.push_back(p.second);
+  return "";
+}
+
+int upload_stage(Stage& st, cudaStream_t s) {
+  st.free_device();
+  CUDA_TRY(cudaMalloc(&st.d_outs, sizeof(DOut) * std::max<size_t>(1, st.outs.size())));
+  CUDA_TRY(cudaMalloc(&st.d_segs, sizeof(DSeg) * std::max<size_t>(1, st.segs.size())));
+  CUDA_TRY(cudaMalloc(&st.d_tiles, sizeof(DTile) * std::max<size_t>(1, st.tiles.size())));
+  if (!st.outs.empty())
+    CUDA_TRY(cudaMemcpyAsync(st.d_outs, st.outs.data(), sizeof(DOut) * st.outs.size(),
+                             cudaMemcpyHostToDevice, s));
+  if (!st.segs.empty())
+    CUDA_TRY(cudaMemcpyAsync(st.d_segs, st.segs.data(), sizeof(DSeg) * st.segs.size(),
+                             cudaMemcpyHostToDevice, s));
+  if (!st.tiles.empty())
+    CUDA_TRY(cudaMemcpyAsync(st.d_tiles, st.tiles.data(), sizeof(DTile) * st.tiles.size(),
+                             cudaMemcpyHostToDevice, s));
+  return 0;
+}
+
+// Common tail of both plan entry points: sign-folded env images, stage
+// descriptors, device uploads, scratch.
+int finalize_plan(dmrgx_ctx* c, const double* renv_vals, const std::vector<int64_t>& roff,
+                  const std::vector<int64_t>& rsize, const double* lenv_vals,
+                  const std::vector<int64_t>& loff, const std::vector<int64_t>& lsize) {
+  const int f = c->f();
+  c->has_plan = false;
+  c->flops = 0;
+  EnvImage ri = make_image(renv_vals, roff, rsize, c->rmap, f);
+  EnvImage li = make_image(lenv_vals, loff, lsize, c->lmap, f);
+  std::string e = build_stage(c->rmap, rsize, ri, f, c->n, c->d_store, c->st1, c->flops);
+  if (e.empty()) e = build_stage(c->lmap, lsize, li, f, c->d_store, c->n, c->st2, c->flops);
+  if (!e.empty()) {
+    set_error(e);
+    return DMRGX_E_ARG;
+  }
+  std::map<int64_t, int> so;
+  for (auto& r : c->rmap) so[r.out_beg] = 1;
+  c->n_store_blocks = (int)so.size();
+  c->st1.a_len = (int64_t)ri.vals.size();
+  c->st2.a_len = (int64_t)li.vals.size();
+  CUDA_TRY(cudaSetDevice(c->device));
+  CUDA_TRY(c->renv.ensure(sizeof(double) * std::max<size_t>(1, ri.vals.size())));
+  CUDA_TRY(c->lenv.ensure(sizeof(double) * std::max<size_t>(1, li.vals.size())));
+  CUDA_TRY(c->store.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, c->d_store * f)));
+  CUDA_TRY(c->din.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, c->n * f)));
+  CUDA_TRY(c->dout.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, c->n * f)));
+  if (!ri.vals.empty())
+    CUDA_TRY(cudaMemcpyAsync(c->renv.p, ri.vals.data(), sizeof(double) * ri.vals.size(),
+                             cudaMemcpyHostToDevice, c->stream));
+  if (!li.vals.empty())
+    CUDA_TRY(cudaMemcpyAsync(c->lenv.p, li.vals.data(), sizeof(double) * li.vals.size(),
+                             cudaMemcpyHostToDevice, c->stream));
+  int rc = upload_stage(c->st1, c->stream);
+  if (rc) return rc;
+  rc = upload_stage(c->st2, c->stream);
+  if (rc) return rc;
+  const size_t need = sizeof(double) * (size_t)std::max<int64_t>(1, c->n * f);
+  if (need > c->h_cap) {
+    if (c->h_in) cudaFreeHost(c->h_in);
+    if (c->h_out) cudaFreeHost(c->h_out);
+    c->h_in = c->h_out = nullptr;
+    c->h_cap = 0;
+    CUDA_TRY(cudaMallocHost((void**)&c->h_in, need));
+    CUDA_TRY(cudaMallocHost((void**)&c->h_out, need));
+    c->h_cap = need;
+  }
+  // ri/li are host temporaries: wait for the uploads before they go away
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->has_plan = true;
+  return 0;
+}
+
+int run_matvec(dmrgx_ctx* c, const double* in, double* out) {
+  const bool cplx = c->dtype == DMRGX_C128;
+  const int grid = c->num_sms * 3;
+  double* store = (double*)c->store.p;
+  if (!c->st1.full_cover)
+    CUDA_TRY(cudaMemsetAsync(store, 0, sizeof(double) * c->d_store * c->f(), c->stream));
+  CUDA_TRY(launch_grouped_f64((const double*)c->renv.p, in, store, c->st1.d_tiles,
+                              (int)c->st1.tiles.size(), c->st1.d_outs, c->st1.d_segs, cplx, grid,
+                              c->stream));
+  if (!c->st2.full_cover)
+    CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double) * c->n * c->f(), c->stream));
+  CUDA_TRY(launch_grouped_f64((const double*)c->lenv.p, store, out, c->st2.d_tiles,
+                              (int)c->st2.tiles.size(), c->st2.d_outs, c->st2.d_segs, cplx, grid,
+                              c->stream));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dmrgx_last_error(void) { return g_err.c_str(); }
+const char* dmrgx_version(void) { return "dmrgx 0.1 (sm_100a)"; }
+
+int dmrgx_ctx_create(dmrgx_ctx** out, int dtype, int device) {
+  ARG_CHECK(out != nullptr, "ctx_create: null output pointer");
+  ARG_CHECK(dtype == DMRGX_F64 || dtype == DMRGX_C128, "ctx_create: dtype must be F64 or C128");
+  int ndev = 0;
+  CUDA_TRY(cudaGetDeviceCount(&ndev));
+  ARG_CHECK(device >= 0 && device < ndev, "ctx_create: no such CUDA device");
+  CUDA_TRY(cudaSetDevice(device));
+  dmrgx_ctx* c = new dmrgx_ctx();
+  c->dtype = dtype;
+  c->device = device;
+  cudaDeviceProp prop;
+  cudaError_t e = cudaGetDeviceProperties(&prop, device);
+  if (e == cudaSuccess) c->num_sms = prop.multiProcessorCount;
+  if (e == cudaSuccess && prop.major < 10) {
+    delete c;
+    set_error("ctx_create: this library is built for sm_100a (Blackwell B200)");
+    return DMRGX_E_CUDA;
+  }
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    set_error(std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    return DMRGX_E_CUDA;
+  }
+  *out = c;
+  return 0;
+}
+
+void dmrgx_ctx_destroy(dmrgx_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  c->st1.free_device();
+  c->st2.free_device();
+  c->renv.release();
+  c->lenv.release();
+  c->store.release();
+  c->din.release();
+  c->dout.release();
+  if (c->h_in) cudaFreeHost(c->h_in);
+  if (c->h_out) cudaFreeHost(c->h_out);
+  cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int dmrgx_set_precision(dmrgx_ctx* c, int prec) {
+  ARG_CHECK(c, "null context");
+  ARG_CHECK(prec == DMRGX_PREC_FP64, "set_precision: only DMRGX_PREC_FP64 is available");
+  c->prec = prec;
+  return 0;
+}
+
+int dmrgx_plan_build(dmrgx_ctx* c, const int* lenv_meta, const void* lenv_vals,
+                     const int* renv_meta, const void* renv_vals, int l_num, int r_num,
+                     int sector, int group_n, int fermion) {
+  ARG_CHECK(c, "null context");
+  ARG_CHECK(lenv_vals && renv_vals, "plan_build: null environment values");
+  ARG_CHECK(group_n >= 1 && group_n <= 4096, "plan_build: group_n out of range");
+  QMeta L, R;
+  std::string e = L.parse(lenv_meta);
+  ARG_CHECK(e.empty(), "plan_build: lenv metadata: " + e);
+  e = R.parse(renv_meta);
+  ARG_CHECK(e.empty(), "plan_build: renv metadata: " + e);
+  ARG_CHECK(l_num >= 2 && l_num <= L.nleg() && r_num >= 1 && r_num <= R.nleg(),
+            "plan_build: l_num/r_num out of range");
+  Group G;
+  G.n = group_n;
+  G.fermion = fermion != 0;
+  std::vector<std::vector<int>> dim, sym, dim_ret, sym_ret;
+  generate_dim_sym(G, L, l_num - 1, R, r_num, sector, dim, sym);
+  c->n = get_dimension(dim, sym);
+  e = get_map(G, R, dim, sym, r_num, 0, false, dim_ret, sym_ret, c->rmap);
+  ARG_CHECK(e.empty(), "plan_build: rmap: " + e);
+  c->d_store = get_dimension(dim_ret, sym_ret);
+  e = get_map(G, L, dim_ret, sym_ret, l_num, 0, true, dim, sym, c->lmap);
+  ARG_CHECK(e.empty(), "plan_build: lmap: " + e);
+  c->psi_dim = dim;
+  c->psi_sym = sym;
+  auto roff = R.block_offsets(), loff = L.block_offsets();
+  std::vector<int64_t> rsize(R.syms.size()), lsize(L.syms.size());
+  for (size_t b = 0; b < rsize.size(); b++) rsize[b] = R.block_size((int)b);
+  for (size_t b = 0; b < lsize.size(); b++) lsize[b] = L.block_size((int)b);
+  return finalize_plan(c, (const double*)renv_vals, roff, rsize, (const double*)lenv_vals, loff,
+                       lsize);
+}
+
+int dmrgx_build_maps(const int* lenv_meta, const int* renv_meta, int l_num, int r_num,
+                     int sector, int group_n, int fermion, int64_t* info, int* rmap,
+                     int64_t rmap_cap, int* lmap, int64_t lmap_cap) {
+  ARG_CHECK(info, "build_maps: null info");
+  ARG_CHECK(group_n >= 1 && group_n <= 4096, "build_maps: group_n out of range");
+  QMeta L, R;
+  std::string e = L.parse(lenv_meta);
+  ARG_CHECK(e.empty(), "build_maps: lenv metadata: " + e);
+  e = R.parse(renv_meta);
+  ARG_CHECK(e.empty(), "build_maps: renv metadata: " + e);
+  ARG_CHECK(l_num >= 2 && l_num <= L.nleg() && r_num >= 1 && r_num <= R.nleg(),
+            "build_maps: l_num/r_num out of range");
+  Group G;
+  G.n = group_n;
+  G.fermion = fermion != 0;
+  std::vector<std::vector<int>> dim, sym, dim_ret, sym_ret;
+  std::vector<MapRow> rr, lr;
+  generate_dim_sym(G, L, l_num - 1, R, r_num, sector, dim, sym);
+  e = get_map(G, R, dim, sym, r_num, 0, false, dim_ret, sym_ret, rr);
+  ARG_CHECK(e.empty(), "build_maps: rmap: " + e);
+  e = get_map(G, L, dim_ret, sym_ret, l_num, 0, true, dim, sym, lr);
+  ARG_CHECK(e.empty(), "build_maps: lmap: " + e);
+  info[0] = get_dimension(dim, sym);
+  info[1] = get_dimension(dim_ret, sym_ret);
+  info[2] = (int64_t)rr.size();
+  info[3] = (int64_t)lr.size();
+  if (!rmap || !lmap) return 0;
+  ARG_CHECK(rmap_cap >= (int64_t)rr.size() && lmap_cap >= (int64_t)lr.size(),
+            "build_maps: map buffer too small");
+  auto put = [](const std::vector<MapRow>& rows, int* o) {
+    for (size_t i = 0; i < rows.size(); i++) {
+      const MapRow& r = rows[i];
+      int* p = o + 7 * i;
+      p[0] = r.blk;
+      p[1] = (int)r.in_beg;
+      p[2] = (int)r.out_beg;
+      p[3] = r.rows;
+      p[4] = r.cols;
+      p[5] = r.beta;
+      p[6] = r.alpha;
+    }
+  };
+  put(rr, rmap);
+  put(lr, lmap);
+  return 0;
+}
+
+int dmrgx_plan_from_maps(dmrgx_ctx* c, int64_t n, int64_t d_store, const int* rmap, int n_rmap,
+                         const void* renv_vals, const int64_t* renv_sizes, int n_renv_blocks,
+                         const int* lmap, int n_lmap, const void* lenv_vals,
+                         const int64_t* lenv_sizes, int n_lenv_blocks) {
+  ARG_CHECK(c, "null context");
+  ARG_CHECK(n >= 0 && d_store >= 0, "plan_from_maps: negative length");
+  ARG_CHECK((n_rmap == 0 || rmap) && (n_lmap == 0 || lmap), "plan_from_maps: null map");
+  ARG_CHECK(renv_vals && lenv_vals && renv_sizes && lenv_sizes,
+            "plan_from_maps: null environment arrays");
+  c->n = n;
+  c->d_store = d_store;
+  auto rows_of = [](const int* m, int nr, std::vector<MapRow>& out) {
+    out.resize(nr);
+    for (int i = 0; i < nr; i++) {
+      const int* r = m + 7 * i;
+      out[i] = MapRow{r[0], r[1], r[2], r[3], r[4], r[5], r[6]};
+    }
+  };
+  rows_of(rmap, n_rmap, c->rmap);
+  rows_of(lmap, n_lmap, c->lmap);
+  c->psi_dim.clear();
+  c->psi_sym.clear();
+  std::vector<int64_t> rsize(renv_sizes, renv_sizes + n_renv_blocks);
+  std::vector<int64_t> lsize(lenv_sizes, lenv_sizes + n_lenv_blocks);
+  std::vector<int64_t> roff(n_renv_blocks + 1, 0), loff(n_lenv_blocks + 1, 0);
+  for (int b = 0; b < n_renv_blocks; b++) {
+    ARG_CHECK(rsize[b] >= 0, "plan_from_maps: negative block size");
+    roff[b + 1] = roff[b] + rsize[b];
+  }
+  for (int b = 0; b < n_lenv_blocks; b++) {
+    ARG_CHECK(lsize[b] >= 0, "plan_from_maps: negative block size");
+    loff[b + 1] = loff[b] + lsize[b];
+  }
+  return finalize_plan(c, (const double*)renv_vals, roff, rsize, (const double*)lenv_vals, loff,
+                       lsize);
+}
+
+int dmrgx_plan_info(dmrgx_ctx* c, int64_t* out) {
+  ARG_CHECK(c && out, "null argument");
+  if (!c->has_plan) {
+    set_error("plan_info: no plan");
+    return DMRGX_E_STATE;
+  }
+  out[0] = c->n;
+  out[1] = c->d_store;
+  out[2] = (int64_t)c->rmap.size();
+  out[3] = (int64_t)c->lmap.size();
+  out[4] = c->flops;
+  out[5] = (int64_t)c->psi_sym.size();
+  out[6] = c->n_store_blocks;
+  return 0;
+}
+
+int dmrgx_plan_maps(dmrgx_ctx* c, int* rmap, int* lmap) {
+  ARG_CHECK(c && rmap && lmap, "null argument");
+  if (!c->has_plan) {
+    set_error("plan_maps: no plan");
+    return DMRGX_E_STATE;
+  }
+  auto put = [](const std::vector<MapRow>& rows, int* o) {
+    for (size_t i = 0; i < rows.size(); i++) {
+      const MapRow& r = rows[i];
+      int* p = o + 7 * i;
+      p[0] = r.blk;
+      p[1] = (int)r.in_beg;
+      p[2] = (int)r.out_beg;
+      p[3] = r.rows;
+      p[4] = r.cols;
+      p[5] = r.beta;
+      p[6] = r.alpha;
+    }
+  };
+  put(c->rmap, rmap);
+  put(c->lmap, lmap);
+  return 0;
+}
+
+int dmrgx_plan_psi_layout(dmrgx_ctx* c, int* out, int64_t cap) {
+  ARG_CHECK(c && out, "null argument");
+  const auto& d = c->psi_dim;
+  const auto& s = c->psi_sym;
+  int64_t need = 2 + (int64_t)d.size() + (int64_t)s.size() * (int64_t)d.size();
+  for (auto& x : d) need += (int64_t)x.size();
+  ARG_CHECK(cap >= need, "plan_psi_layout: buffer too small");
+  int64_t k = 0;
+  out[k++] = (int)d.size();
+  out[k++] = (int)s.size();
+  for (auto& x : d) out[k++] = (int)x.size();
+  for (auto& x : d)
+    for (int v : x) out[k++] = v;
+  for (auto& b : s)
+    for (int v : b) out[k++] = v;
+  return 0;
+}
+
+int dmrgx_av(dmrgx_ctx* c, const void* in, void* out, int mem) {
+  ARG_CHECK(c, "null context");
+  ARG_CHECK(in && out, "av: null vector");
+  if (!c->has_plan) {
+    set_error("av: no plan");
+    return DMRGX_E_STATE;
+  }
+  CUDA_TRY(cudaSetDevice(c->device));
+  const size_t bytes = sizeof(double) * (size_t)c->n * c->f();
+  if (mem == DMRGX_MEM_DEVICE) return run_matvec(c, (const double*)in, (double*)out);
+  ARG_CHECK(mem == DMRGX_MEM_HOST, "av: mem must be DMRGX_MEM_HOST or DMRGX_MEM_DEVICE");
+  std::memcpy(c->h_in, in, bytes);
+  CUDA_TRY(cudaMemcpyAsync(c->din.p, c->h_in, bytes, cudaMemcpyHostToDevice, c->stream));
+  int rc = run_matvec(c, (const double*)c->din.p, (double*)c->dout.p);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(c->h_out, c->dout.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  std::memcpy(out, c->h_out, bytes);
+  return 0;
+}
+
+void* dmrgx_stream(dmrgx_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int dmrgx_sync(dmrgx_ctx* c) {
+  ARG_CHECK(c, "null context");
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,168 @@
+"""ctypes binding of libdmrgx.so (the C ABI declared in include/dmrgx.h).
+
+This module is plumbing: it loads the in-tree CUDA library and converts numpy
+arrays to pointers.  There is no fallback: if the library is missing the import
+of a context fails with an error that says how to build it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libdmrgx.so")
+
+F64, C128 = 0, 1
+PREC_FP64, PREC_BF16X3, PREC_TF32X3 = 0, 1, 2
+MEM_HOST, MEM_DEVICE = 0, 1
+
+# every entry point declared in include/dmrgx.h, with (restype, argtypes)
+_vp, _ip, _i, _i64 = C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_int64
+_i64p, _dp = C.POINTER(C.c_int64), C.POINTER(C.c_double)
+SIGNATURES = {
+    "dmrgx_last_error": (C.c_char_p, []),
+    "dmrgx_version": (C.c_char_p, []),
+    "dmrgx_ctx_create": (_i, [C.POINTER(_vp), _i, _i]),
+    "dmrgx_ctx_destroy": (None, [_vp]),
+    "dmrgx_set_precision": (_i, [_vp, _i]),
+    "dmrgx_plan_build": (_i, [_vp, _ip, _vp, _ip, _vp, _i, _i, _i, _i, _i]),
+    "dmrgx_build_maps": (_i, [_ip, _ip, _i, _i, _i, _i, _i, _i64p, _ip, _i64, _ip, _i64]),
+    "dmrgx_plan_from_maps": (_i, [_vp, _i64, _i64, _ip, _i, _vp, _i64p, _i, _ip, _i, _vp,
+                                  _i64p, _i]),
+    "dmrgx_plan_info": (_i, [_vp, _i64p]),
+    "dmrgx_plan_maps": (_i, [_vp, _ip, _ip]),
+    "dmrgx_plan_psi_layout": (_i, [_vp, _ip, _i64]),
+    "dmrgx_av": (_i, [_vp, _vp, _vp, _i]),
+    "dmrgx_stream": (_vp, [_vp]),
+    "dmrgx_sync": (_i, [_vp]),
+}
+
+_lib = None
+
+
+class DmrgxError(RuntimeError):
+    pass
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise DmrgxError(f"{LIB_PATH} is not built; run `python -m dmrg_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise DmrgxError(f"dmrgx error {rc}: {lib().dmrgx_last_error().decode()}")
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _i64p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+def build_maps(lenv_meta, renv_meta, l_num, r_num, sector, group_n, fermion):
+    """Host-only sector bookkeeping: (n, d_store, rmap, lmap) in the reference row format."""
+    lm = np.ascontiguousarray(lenv_meta, np.int32)
+    rm = np.ascontiguousarray(renv_meta, np.int32)
+    info = np.zeros(4, np.int64)
+    _check(lib().dmrgx_build_maps(_ip(lm), _ip(rm), l_num, r_num, sector, group_n, fermion,
+                                  _i64p(info), None, 0, None, 0))
+    rmap = np.zeros((max(1, info[2]), 7), np.int32)
+    lmap = np.zeros((max(1, info[3]), 7), np.int32)
+    _check(lib().dmrgx_build_maps(_ip(lm), _ip(rm), l_num, r_num, sector, group_n, fermion,
+                                  _i64p(info), _ip(rmap), rmap.shape[0], _ip(lmap),
+                                  lmap.shape[0]))
+    return int(info[0]), int(info[1]), rmap[: info[2]], lmap[: info[3]]
+
+
+class Context:
+    """A dmrgx context (one GPU stream, device environments, a matvec plan)."""
+
+    def __init__(self, dtype=F64, device=0):
+        self.dtype = dtype
+        self._np = np.complex128 if dtype == C128 else np.float64
+        p = C.c_void_p()
+        _check(lib().dmrgx_ctx_create(C.byref(p), dtype, device))
+        self.ptr = p
+        self.n = self.d_store = 0
+
+    def close(self):
+        if self.ptr:
+            lib().dmrgx_ctx_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_precision(self, prec):
+        _check(lib().dmrgx_set_precision(self.ptr, prec))
+
+    def plan_build(self, lenv, renv, l_num, r_num, sector, group_n, fermion=0):
+        """lenv/renv: (meta int array, packed values) pairs."""
+        lm = np.ascontiguousarray(lenv[0], np.int32)
+        rm = np.ascontiguousarray(renv[0], np.int32)
+        lv = np.ascontiguousarray(lenv[1], self._np)
+        rv = np.ascontiguousarray(renv[1], self._np)
+        _check(lib().dmrgx_plan_build(self.ptr, _ip(lm), lv.ctypes.data, _ip(rm), rv.ctypes.data,
+                                      l_num, r_num, sector, group_n, fermion))
+        self._refresh()
+
+    def plan_from_maps(self, n, d_store, rmap, renv_vals, renv_sizes, lmap, lenv_vals,
+                       lenv_sizes):
+        rmap = np.ascontiguousarray(rmap, np.int32).reshape(-1, 7)
+        lmap = np.ascontiguousarray(lmap, np.int32).reshape(-1, 7)
+        rv = np.ascontiguousarray(renv_vals, self._np)
+        lv = np.ascontiguousarray(lenv_vals, self._np)
+        rs = np.ascontiguousarray(renv_sizes, np.int64)
+        ls = np.ascontiguousarray(lenv_sizes, np.int64)
+        _check(lib().dmrgx_plan_from_maps(self.ptr, n, d_store, _ip(rmap), rmap.shape[0],
+                                          rv.ctypes.data, _i64p(rs), rs.size, _ip(lmap),
+                                          lmap.shape[0], lv.ctypes.data, _i64p(ls), ls.size))
+        self._refresh()
+
+    def _refresh(self):
+        info = np.zeros(8, np.int64)
+        _check(lib().dmrgx_plan_info(self.ptr, _i64p(info)))
+        self.n, self.d_store = int(info[0]), int(info[1])
+        self.n_rmap, self.n_lmap = int(info[2]), int(info[3])
+        self.flops = int(info[4])
+
+    def maps(self):
+        r = np.zeros((max(1, self.n_rmap), 7), np.int32)
+        l = np.zeros((max(1, self.n_lmap), 7), np.int32)
+        _check(lib().dmrgx_plan_maps(self.ptr, _ip(r), _ip(l)))
+        return r[: self.n_rmap], l[: self.n_lmap]
+
+    def av(self, x):
+        """Host arrays in/out (the reference-facing call)."""
+        x = np.ascontiguousarray(x, self._np)
+        assert x.size == self.n
+        y = np.empty(self.n, self._np)
+        _check(lib().dmrgx_av(self.ptr, x.ctypes.data, y.ctypes.data, MEM_HOST))
+        return y
+
+    def av_device(self, x_ptr: int, y_ptr: int):
+        """Device pointers (e.g. torch tensors' data_ptr()) on this context's stream."""
+        _check(lib().dmrgx_av(self.ptr, C.c_void_p(x_ptr), C.c_void_p(y_ptr), MEM_DEVICE))
+
+    def stream(self) -> int:
+        return int(lib().dmrgx_stream(self.ptr) or 0)
+
+    def sync(self):
+        _check(lib().dmrgx_sync(self.ptr))

@@ -1,0 +1,130 @@
+/* dmrgx: B200-native effective-Hamiltonian path for symmetry-blocked DMRG.
+ *
+ * C ABI of libdmrgx.so.  Plain pointers and sizes only.  Every function returns
+ * 0 on success and a negative DMRGX_E* code on failure; dmrgx_last_error()
+ * gives the message of the last failure on the calling thread.
+ *
+ * Terms follow the reference code (clover199/DMRG):
+ *  - a block-sparse tensor ("qtensor", include/qtensor.h:20-31) has, per leg, a
+ *    list of sector sizes, per block one sector label per leg, per leg a
+ *    fermion direction, and its blocks stored dense row-major (last index
+ *    fastest), packed one after another in block order;
+ *  - the wavefunction psi is the packed concatenation of its blocks in the order
+ *    generate_dim_sym produces (src/useful.cpp:151-194);
+ *  - a matvec plan is the pair of task lists ("maps") that get_map builds
+ *    (src/qtensor.cpp:997-1119), seven ints per row:
+ *    [env block, in offset, out offset, rows, cols, beta, alpha].
+ *
+ * Qtensor metadata ("meta") is an int array:
+ *   nleg, nblk, nsec[0..nleg), dims (all legs' sector sizes, leg by leg),
+ *   dir[0..nleg), sym[blk][leg] (nblk*nleg ints).
+ *
+ * Element types: DMRGX_F64 (double) or DMRGX_C128 (interleaved re,im doubles).
+ * A context owns one GPU stream, the device copies of the environments, the
+ * plan and its scratch; it is not shared between host threads.
+ */
+#ifndef DMRGX_H
+#define DMRGX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  DMRGX_OK = 0,
+  DMRGX_E_ARG = -1,      /* bad argument / inconsistent metadata */
+  DMRGX_E_CUDA = -2,     /* CUDA runtime or kernel error */
+  DMRGX_E_STATE = -3,    /* call not valid in this state (e.g. no plan) */
+  DMRGX_E_NOCONV = -4,   /* eigensolver did not converge */
+  DMRGX_E_TIMEOUT = -5,  /* a bounded device wait gave up */
+};
+
+enum { DMRGX_F64 = 0, DMRGX_C128 = 1 };
+
+/* matvec arithmetic of a context */
+enum {
+  DMRGX_PREC_FP64 = 0,   /* FP64 tensor-core (DMMA) grouped GEMM */
+  DMRGX_PREC_BF16X3 = 1, /* split precision: hi*hi + hi*lo + lo*hi in BF16, FP32 accumulate */
+  DMRGX_PREC_TF32X3 = 2, /* split precision in TF32, FP32 accumulate */
+};
+
+enum { DMRGX_MEM_HOST = 0, DMRGX_MEM_DEVICE = 1 };
+
+typedef struct dmrgx_ctx dmrgx_ctx;
+
+const char* dmrgx_last_error(void);
+const char* dmrgx_version(void);
+
+/* Create a context on CUDA device `device` for element type `dtype`. */
+int dmrgx_ctx_create(dmrgx_ctx** ctx, int dtype, int device);
+void dmrgx_ctx_destroy(dmrgx_ctx* ctx);
+
+/* Select the matvec arithmetic (DMRGX_PREC_*).  Default FP64. */
+int dmrgx_set_precision(dmrgx_ctx* ctx, int prec);
+
+/* Build a matvec plan from two block-sparse environments, the way the
+ * reference step functions do before calling the eigensolver
+ * (src/core.cpp:201-202, :236-247): psi layout from
+ * generate_dim_sym(lenv, l_num-1, renv, r_num, sector) (src/useful.cpp:151-194),
+ * rmap = renv.get_map(..., 'N','T', r_num, 0) and
+ * lmap = lenv.get_map(..., 'N','T', l_num, 0, back=true) (src/qtensor.cpp:997-1119).
+ * group_n: Z_N fusion rule (src/useful.cpp:30); fermion: apply the direction
+ * signs (src/qtensor.cpp:1078-1085); 0 for bosonic models.
+ * Environment values (host pointers) are copied to the device. */
+int dmrgx_plan_build(dmrgx_ctx* ctx, const int* lenv_meta, const void* lenv_vals,
+                     const int* renv_meta, const void* renv_vals, int l_num, int r_num,
+                     int sector, int group_n, int fermion);
+
+/* Build a plan from the reference's own task lists: the drop-in for a caller
+ * that already holds lanczos<T>::rmap/lmap (include/val_for_lanczos.h:7-24).
+ * n: psi length; d_store: length of the intermediate (get_dimension of the
+ * store layout, src/core.cpp:239).  env_vals: blocks packed in block order;
+ * env_sizes: element count of each block. */
+int dmrgx_plan_from_maps(dmrgx_ctx* ctx, int64_t n, int64_t d_store,
+                         const int* rmap, int n_rmap, const void* renv_vals,
+                         const int64_t* renv_sizes, int n_renv_blocks,
+                         const int* lmap, int n_lmap, const void* lenv_vals,
+                         const int64_t* lenv_sizes, int n_lenv_blocks);
+
+/* The sector bookkeeping of dmrgx_plan_build alone, on the host (no context, no
+ * GPU): psi layout and both task lists in the reference's row format.
+ * info[0]=n, info[1]=d_store, info[2]=rows of rmap, info[3]=rows of lmap.
+ * rmap/lmap may be NULL (or too small: caps are in rows) to query the sizes;
+ * returns DMRGX_E_ARG with the sizes in info when a buffer is too small. */
+int dmrgx_build_maps(const int* lenv_meta, const int* renv_meta, int l_num, int r_num,
+                     int sector, int group_n, int fermion, int64_t* info, int* rmap,
+                     int64_t rmap_cap, int* lmap, int64_t lmap_cap);
+
+/* Plan facts: out[0]=n, out[1]=d_store, out[2]=rows of rmap, out[3]=rows of lmap,
+ * out[4]=useful real flops of one matvec (2*M*N*K per task, x4 for complex),
+ * out[5]=psi blocks, out[6]=store blocks. */
+int dmrgx_plan_info(dmrgx_ctx* ctx, int64_t* out);
+
+/* Copy out the task lists of the current plan, reference row format. */
+int dmrgx_plan_maps(dmrgx_ctx* ctx, int* rmap, int* lmap);
+
+/* Copy out the psi layout: nleg, nblk, nsec[], dims..., sym[blk][leg]. */
+int dmrgx_plan_psi_layout(dmrgx_ctx* ctx, int* out, int64_t cap);
+
+/* out = H_eff in, exactly av() of the reference (src/core.cpp:22-31):
+ * store = renv (x)_{r_num} in, out = lenv (x)_{l_num} store.
+ * mem = DMRGX_MEM_HOST: in/out are host arrays (copied through the context's
+ * pinned staging buffers); DMRGX_MEM_DEVICE: device arrays on this context's
+ * device, ordered on the context's stream.  Psi sectors no task writes are set
+ * to zero (the reference leaves them untouched). */
+int dmrgx_av(dmrgx_ctx* ctx, const void* in, void* out, int mem);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own
+ * device work with dmrgx_av(..., DMRGX_MEM_DEVICE). */
+void* dmrgx_stream(dmrgx_ctx* ctx);
+
+/* Block until all work queued on the context's stream is done. */
+int dmrgx_sync(dmrgx_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DMRGX_H */

@@ -1,0 +1,499 @@
+/* Oracle hooks around the unmodified reference DMRG sources.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is compiled together with the reference
+ * sources (src/tensor.cpp, src/qtensor.cpp, src/core.cpp, ... under the
+ * reference tree) into oracle/_ref/liboref_<variant>.so.  Only tests, the
+ * smoke check and the CPU-baseline leg of the benchmark load it, as a checker.
+ *
+ * What it adds:
+ *  - the two `znaupd` overloads the reference expects from its ARPACK wrappers
+ *    (declared include/basic.h:12,28-29; reference bodies src/dsaupd.cpp:65-155
+ *    and src/znaupd.cpp:78-197).  ARPACK itself is not installed here, so the
+ *    eigensolve is handed to a callback that Python registers (it runs SciPy's
+ *    bundled ARPACK with the reference's settings: nev=6, tol=1e-10, ncv 24/36,
+ *    which SA/SR, maxiter 3n).  The callback receives the reference's own
+ *    `lanczos<T>` context, so it can call the reference `av()` (src/core.cpp:22-31)
+ *    and capture per-step fixtures;
+ *  - flat C entry points that serialise/deserialise `qtensor<T>`, run the
+ *    reference `generate_dim_sym` / `get_map` / `av` / `svd` / env-update
+ *    contractions on given inputs, and run the reference `dmrg()` / `ed()`
+ *    schedules for the shipped models.
+ *
+ * Serialised qtensor layout (ints): nleg, nblk, nsec[leg] x nleg,
+ * dims[leg][sec] (all legs, in order), dir[leg] x nleg, sym[blk][leg] x nblk*nleg.
+ * Values: blocks packed in block order, each block row-major (last index fastest),
+ * exactly as the reference stores `val_` (include/qtensor.h:26-31, include/tensor.h:36-45).
+ */
+#include "global.h"
+#define private public
+#include "qtensor.h"
+#include "mps.h"
+#include "mpo.h"
+#include "val_for_lanczos.h"
+#undef private
+#include "functions.h"
+#include "operators.h"
+#include "useful.h"
+
+#include <cstring>
+#include <cstdio>
+#include <unistd.h>
+#include <fcntl.h>
+
+template <typename T> void av(T* in, T* out, lanczos<T>& pass_val);
+
+extern "C" {
+typedef int (*oref_eig_cb_t)(int n, int nev, int is_complex, double* evals, void* evecs, void* pv);
+}
+
+static oref_eig_cb_t g_eig_cb = 0;
+static int g_quiet_fd = -1;
+
+extern "C" void oref_set_eig_callback(oref_eig_cb_t cb) { g_eig_cb = cb; }
+
+extern "C" int oref_symmetry() { return SYMMETRY; }
+extern "C" int oref_fermion()
+{
+#ifdef FERMION
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+/* Redirect the reference's chatty stdout to /dev/null (1) or restore it (0). */
+extern "C" void oref_quiet(int on)
+{
+  fflush(stdout);
+  std::cout.flush();
+  if (on && g_quiet_fd < 0) {
+    g_quiet_fd = dup(1);
+    int dn = open("/dev/null", O_WRONLY);
+    dup2(dn, 1);
+    close(dn);
+  } else if (!on && g_quiet_fd >= 0) {
+    dup2(g_quiet_fd, 1);
+    close(g_quiet_fd);
+    g_quiet_fd = -1;
+  }
+}
+
+/* ---- ARPACK replacement: same signatures as include/basic.h:12,28-29 ---- */
+void znaupd(int n, int nev, double* Evals, double* Evecs, lanczos<double>& pass_val)
+{
+  if (!g_eig_cb) { cerr << "oracle: no eigensolver callback registered\n"; return; }
+  g_eig_cb(n, nev, 0, Evals, (void*)Evecs, (void*)&pass_val);
+}
+
+void znaupd(int n, int nev, double* Evals, complex<double>* Evecs,
+            lanczos<complex<double> >& pass_val)
+{
+  if (!g_eig_cb) { cerr << "oracle: no eigensolver callback registered\n"; return; }
+  g_eig_cb(n, nev, 1, Evals, (void*)Evecs, (void*)&pass_val);
+}
+
+/* ---- the reference matvec on a captured or built context ---- */
+extern "C" void oref_av(int is_complex, void* pv, const void* in, void* out)
+{
+  if (is_complex)
+    av<complex<double> >((complex<double>*)in, (complex<double>*)out,
+                         *(lanczos<complex<double> >*)pv);
+  else
+    av<double>((double*)in, (double*)out, *(lanczos<double>*)pv);
+}
+
+template <typename T>
+static void pv_info_t(lanczos<T>* pv, int* out)
+{
+  out[0] = pv->l_num;
+  out[1] = pv->r_num;
+  out[2] = (int)pv->rmap.size();
+  out[3] = (int)pv->lmap.size();
+}
+
+extern "C" void oref_pv_info(int is_complex, void* pv, int* out)
+{
+  if (is_complex) pv_info_t((lanczos<complex<double> >*)pv, out);
+  else pv_info_t((lanczos<double>*)pv, out);
+}
+
+template <typename T>
+static void pv_maps_t(lanczos<T>* pv, int* rmap, int* lmap)
+{
+  for (size_t i = 0; i < pv->rmap.size(); i++)
+    for (int j = 0; j < 7; j++) rmap[i * 7 + j] = pv->rmap[i][j];
+  for (size_t i = 0; i < pv->lmap.size(); i++)
+    for (int j = 0; j < 7; j++) lmap[i * 7 + j] = pv->lmap[i][j];
+}
+
+extern "C" void oref_pv_maps(int is_complex, void* pv, int* rmap, int* lmap)
+{
+  if (is_complex) pv_maps_t((lanczos<complex<double> >*)pv, rmap, lmap);
+  else pv_maps_t((lanczos<double>*)pv, rmap, lmap);
+}
+
+/* which: 0 = lenv, 1 = renv */
+extern "C" void* oref_pv_env(int is_complex, void* pv, int which)
+{
+  if (is_complex) {
+    lanczos<complex<double> >* p = (lanczos<complex<double> >*)pv;
+    return which ? (void*)&p->renv : (void*)&p->lenv;
+  }
+  lanczos<double>* p = (lanczos<double>*)pv;
+  return which ? (void*)&p->renv : (void*)&p->lenv;
+}
+
+/* ---- qtensor (de)serialisation ---- */
+template <typename T>
+static long qt_ser_t(const qtensor<T>* q, int* ibuf, long ilen, T* vbuf, long vlen)
+{
+  long need_i = 2;
+  int nleg = (int)q->dim_.size();
+  for (int l = 0; l < nleg; l++) need_i += 1 + (long)q->dim_[l].size() + 1;
+  need_i += (long)q->sym_.size() * nleg;
+  long need_v = 0;
+  for (size_t b = 0; b < q->val_.size(); b++) need_v += (long)q->val_[b].val_.size();
+  if (!ibuf) return need_i;
+  if (!vbuf && vlen == -1) return need_v;
+  if (ilen < need_i || vlen < need_v) return -1;
+  long k = 0;
+  ibuf[k++] = nleg;
+  ibuf[k++] = (int)q->sym_.size();
+  for (int l = 0; l < nleg; l++) ibuf[k++] = (int)q->dim_[l].size();
+  for (int l = 0; l < nleg; l++)
+    for (size_t s = 0; s < q->dim_[l].size(); s++) ibuf[k++] = q->dim_[l][s];
+  for (int l = 0; l < nleg; l++) ibuf[k++] = l < (int)q->dir_.size() ? q->dir_[l] : 0;
+  for (size_t b = 0; b < q->sym_.size(); b++)
+    for (int l = 0; l < nleg; l++) ibuf[k++] = q->sym_[b][l];
+  long v = 0;
+  for (size_t b = 0; b < q->val_.size(); b++)
+    for (size_t i = 0; i < q->val_[b].val_.size(); i++) vbuf[v++] = q->val_[b].val_[i];
+  return 0;
+}
+
+/* Call with ibuf=NULL to get the int length, with vbuf=NULL and vlen=-1 to get
+   the value count, then with both buffers to fill them (returns 0). */
+extern "C" long oref_qt_serialize(int is_complex, const void* qt, int* ibuf, long ilen,
+                                  void* vbuf, long vlen)
+{
+  if (is_complex)
+    return qt_ser_t((const qtensor<complex<double> >*)qt, ibuf, ilen,
+                    (complex<double>*)vbuf, vlen);
+  return qt_ser_t((const qtensor<double>*)qt, ibuf, ilen, (double*)vbuf, vlen);
+}
+
+template <typename T>
+static qtensor<T>* qt_new_t(const int* ibuf, const T* vals)
+{
+  qtensor<T>* q = new qtensor<T>();
+  long k = 0;
+  int nleg = ibuf[k++];
+  int nblk = ibuf[k++];
+  q->dim_.resize(nleg);
+  for (int l = 0; l < nleg; l++) q->dim_[l].resize(ibuf[k++]);
+  for (int l = 0; l < nleg; l++)
+    for (size_t s = 0; s < q->dim_[l].size(); s++) q->dim_[l][s] = ibuf[k++];
+  q->dir_.resize(nleg);
+  for (int l = 0; l < nleg; l++) q->dir_[l] = ibuf[k++];
+  q->sym_.resize(nblk);
+  q->val_.resize(nblk);
+  long v = 0;
+  for (int b = 0; b < nblk; b++) {
+    q->sym_[b].resize(nleg);
+    for (int l = 0; l < nleg; l++) q->sym_[b][l] = ibuf[k++];
+    q->val_[b].index_.resize(nleg);
+    long sz = 1;
+    for (int l = 0; l < nleg; l++) {
+      q->val_[b].index_[l] = q->dim_[l][q->sym_[b][l]];
+      sz *= q->val_[b].index_[l];
+    }
+    q->val_[b].val_.assign(vals + v, vals + v + sz);
+    v += sz;
+  }
+  return q;
+}
+
+extern "C" void* oref_qt_new(int is_complex, const int* ibuf, const void* vals)
+{
+  if (is_complex) return qt_new_t(ibuf, (const complex<double>*)vals);
+  return qt_new_t(ibuf, (const double*)vals);
+}
+
+extern "C" void oref_qt_free(int is_complex, void* qt)
+{
+  if (is_complex) delete (qtensor<complex<double> >*)qt;
+  else delete (qtensor<double>*)qt;
+}
+
+/* ---- generate_dim_sym (src/useful.cpp:151-194) ----
+   out: nleg, nblk, nsec[leg], dims..., sym[blk][leg]...   returns ints written */
+template <typename T>
+static long gds_t(const qtensor<T>* le, int lnum, const qtensor<T>* re, int rnum, int sector,
+                  int* out, long olen)
+{
+  vector<vector<int> > dim, sym;
+  generate_dim_sym(dim, sym, *le, lnum, *re, rnum, sector);
+  long need = 2;
+  for (size_t l = 0; l < dim.size(); l++) need += 1 + (long)dim[l].size();
+  need += (long)sym.size() * (long)dim.size();
+  if (!out || olen < need) return need;
+  long k = 0;
+  out[k++] = (int)dim.size();
+  out[k++] = (int)sym.size();
+  for (size_t l = 0; l < dim.size(); l++) out[k++] = (int)dim[l].size();
+  for (size_t l = 0; l < dim.size(); l++)
+    for (size_t s = 0; s < dim[l].size(); s++) out[k++] = dim[l][s];
+  for (size_t b = 0; b < sym.size(); b++)
+    for (size_t l = 0; l < dim.size(); l++) out[k++] = sym[b][l];
+  return need;
+}
+
+extern "C" long oref_gen_dim_sym(int is_complex, const void* le, int lnum, const void* re,
+                                 int rnum, int sector, int* out, long olen)
+{
+  if (is_complex)
+    return gds_t((const qtensor<complex<double> >*)le, lnum,
+                 (const qtensor<complex<double> >*)re, rnum, sector, out, olen);
+  return gds_t((const qtensor<double>*)le, lnum, (const qtensor<double>*)re, rnum, sector,
+               out, olen);
+}
+
+/* ---- a matvec context built the way the reference step functions build it
+   (src/core.cpp:236-247 for update_two; the other steps differ only in
+   l_num/r_num).  info out: n, d_store, n_rmap, n_lmap ---- */
+template <typename T>
+struct OrefBox {
+  lanczos<T> pv;  /* must stay first: Python hands &box as the lanczos pointer */
+  vector<vector<int> > dim, sym, dim_ret, sym_ret;
+  int n, d_store;
+};
+
+template <typename T>
+static void* pv_build_t(const qtensor<T>* le, const qtensor<T>* re, int l_num, int r_num,
+                        int sector, int* info)
+{
+  OrefBox<T>* b = new OrefBox<T>();
+  b->pv.lenv = *le;
+  b->pv.renv = *re;
+  generate_dim_sym(b->dim, b->sym, b->pv.lenv, l_num - 1, b->pv.renv, r_num, sector);
+  b->n = get_dimension(b->dim, b->sym);
+  b->pv.r_num = r_num;
+  b->pv.l_num = l_num;
+  b->pv.renv.get_map(b->pv.rmap, b->dim_ret, b->sym_ret, b->dim, b->sym, 'N', 'T', r_num, 0);
+  b->d_store = get_dimension(b->dim_ret, b->sym_ret);
+  b->pv.lenv.get_map(b->pv.lmap, b->dim, b->sym, b->dim_ret, b->sym_ret, 'N', 'T', l_num, 0,
+                     true);
+  b->pv.store = new T[b->d_store > 0 ? b->d_store : 1];
+  info[0] = b->n;
+  info[1] = b->d_store;
+  info[2] = (int)b->pv.rmap.size();
+  info[3] = (int)b->pv.lmap.size();
+  return (void*)b;
+}
+
+extern "C" void* oref_pv_build(int is_complex, const void* le, const void* re, int l_num,
+                               int r_num, int sector, int* info)
+{
+  if (is_complex)
+    return pv_build_t((const qtensor<complex<double> >*)le,
+                      (const qtensor<complex<double> >*)re, l_num, r_num, sector, info);
+  return pv_build_t((const qtensor<double>*)le, (const qtensor<double>*)re, l_num, r_num,
+                    sector, info);
+}
+
+/* store layout of a built context: nleg, nblk, nsec[leg], dims..., sym[blk][leg] */
+template <typename T>
+static long box_store_t(OrefBox<T>* b, int* out, long olen)
+{
+  long need = 2;
+  for (size_t l = 0; l < b->dim_ret.size(); l++) need += 1 + (long)b->dim_ret[l].size();
+  need += (long)b->sym_ret.size() * (long)b->dim_ret.size();
+  if (!out || olen < need) return need;
+  long k = 0;
+  out[k++] = (int)b->dim_ret.size();
+  out[k++] = (int)b->sym_ret.size();
+  for (size_t l = 0; l < b->dim_ret.size(); l++) out[k++] = (int)b->dim_ret[l].size();
+  for (size_t l = 0; l < b->dim_ret.size(); l++)
+    for (size_t s = 0; s < b->dim_ret[l].size(); s++) out[k++] = b->dim_ret[l][s];
+  for (size_t i = 0; i < b->sym_ret.size(); i++)
+    for (size_t l = 0; l < b->dim_ret.size(); l++) out[k++] = b->sym_ret[i][l];
+  return need;
+}
+
+extern "C" long oref_pv_store_layout(int is_complex, void* box, int* out, long olen)
+{
+  if (is_complex) return box_store_t((OrefBox<complex<double> >*)box, out, olen);
+  return box_store_t((OrefBox<double>*)box, out, olen);
+}
+
+extern "C" void oref_pv_free(int is_complex, void* box)
+{
+  if (is_complex) {
+    OrefBox<complex<double> >* b = (OrefBox<complex<double> >*)box;
+    delete[] b->pv.store;
+    delete b;
+  } else {
+    OrefBox<double>* b = (OrefBox<double>*)box;
+    delete[] b->pv.store;
+    delete b;
+  }
+}
+
+/* ---- SVD with truncation (src/qtensor.cpp:1122-1262) ----
+   Returns the number of singular values (all, sorted as the reference sorts them);
+   U, S, V become new qtensors owned by the caller. */
+template <typename T>
+static int svd_t(const qtensor<T>* a, int num, int cutoff, void** U, void** S, void** V,
+                 double* s_out, int s_cap)
+{
+  qtensor<T> vec = *a;
+  qtensor<T>* u = new qtensor<T>();
+  qtensor<T>* v = new qtensor<T>();
+  qtensor<double>* sg = new qtensor<double>();
+  vector<double> s = vec.svd(*u, *sg, *v, num, cutoff);
+  for (int i = 0; i < (int)s.size() && i < s_cap; i++) s_out[i] = s[i];
+  *U = u;
+  *S = sg;
+  *V = v;
+  return (int)s.size();
+}
+
+extern "C" int oref_svd(int is_complex, const void* a, int num, int cutoff, void** U, void** S,
+                        void** V, double* s_out, int s_cap)
+{
+  if (is_complex)
+    return svd_t((const qtensor<complex<double> >*)a, num, cutoff, U, S, V, s_out, s_cap);
+  return svd_t((const qtensor<double>*)a, num, cutoff, U, S, V, s_out, s_cap);
+}
+
+/* ---- environment update (src/core.cpp:266-271):
+   side 0: L_new = U^T(conj) . (lenv . U)   [vec.contract(lenv,U,'N','N',num); U.conjugate();
+                                              new.contract(U,vec,'T','N',num)]
+   side 1: R_new = V(conj) . (renv . V^T)   [vec.contract(renv,V,'N','T',num); V.conjugate();
+                                              new.contract(V,vec,'N','N',num)] ---- */
+template <typename T>
+static void* env_update_t(const qtensor<T>* env, const qtensor<T>* uv, int side, int num)
+{
+  qtensor<T> e = *env;
+  qtensor<T> w = *uv;
+  qtensor<T> vec;
+  qtensor<T>* out = new qtensor<T>();
+  if (side == 0) {
+    vec.contract(e, w, 'N', 'N', num);
+    w.conjugate();
+    out->contract(w, vec, 'T', 'N', num);
+  } else {
+    vec.contract(e, w, 'N', 'T', num);
+    w.conjugate();
+    out->contract(w, vec, 'N', 'N', num);
+  }
+  return out;
+}
+
+extern "C" void* oref_env_update(int is_complex, const void* env, const void* uv, int side,
+                                 int num)
+{
+  if (is_complex)
+    return env_update_t((const qtensor<complex<double> >*)env,
+                        (const qtensor<complex<double> >*)uv, side, num);
+  return env_update_t((const qtensor<double>*)env, (const qtensor<double>*)uv, side, num);
+}
+
+/* ---- env (x) MPO fusion (src/core.cpp:188-192):
+   side 0: lenv = (L ._1 W).exchange(3,4)
+   side 1: renv = (R ._1 W.exchange(0,2), change=true).exchange(0,1) ---- */
+template <typename T>
+static void* fuse_t(const qtensor<T>* env, const qtensor<T>* w, int side)
+{
+  qtensor<T>* out = new qtensor<T>();
+  if (side == 0) {
+    out->contract(*env, 1, *w, 0);
+    *out = out->exchange(3, 4);
+  } else {
+    qtensor<T> ope = w->exchange(0, 2);
+    out->contract(*env, 1, ope, 0, true);
+    *out = out->exchange(0, 1);
+  }
+  return out;
+}
+
+extern "C" void* oref_fuse(int is_complex, const void* env, const void* w, int side)
+{
+  if (is_complex)
+    return fuse_t((const qtensor<complex<double> >*)env, (const qtensor<complex<double> >*)w,
+                  side);
+  return fuse_t((const qtensor<double>*)env, (const qtensor<double>*)w, side);
+}
+
+/* ---- model MPO tensors, built by the reference builders (src/operators.cpp) ----
+   model: 0 Kitaev(t,p,u)  1 XYZ(jx,jy,jz)  2 Potts3(f,j,p,t)
+   part:  0 bulk, 1 left edge, 2 right edge.  is_complex_out tells the element type. */
+extern "C" void* oref_mpo_tensor(int model, const double* par, int part, int* is_complex_out)
+{
+#ifdef FERMION
+  if (model == 0) {
+    qtensor<double> h = H_Kitaev(par[0], par[1], par[2]);
+    *is_complex_out = 0;
+    if (part == 1) return new qtensor<double>(h.left());
+    if (part == 2) return new qtensor<double>(h.right());
+    return new qtensor<double>(h);
+  }
+#endif
+  if (model == 1 || model == 2) {
+    qtensor<complex<double> > h =
+        model == 1 ? H_XYZ(par[0], par[1], par[2]) : H_Potts3(par[0], par[1], par[2], par[3]);
+    *is_complex_out = 1;
+    if (part == 1) return new qtensor<complex<double> >(h.left());
+    if (part == 2) return new qtensor<complex<double> >(h.right());
+    return new qtensor<complex<double> >(h);
+  }
+  *is_complex_out = -1;
+  return 0;
+}
+
+/* ---- the shipped drivers' set-up (kitaev.cpp:37-40, xyz.cpp:29-31, potts.cpp:36-38)
+   followed by the reference schedule.  schedule: 0 dmrg() (functions.cpp:157-227),
+   1 dmrg2() (:234-299), 2 ed() (:107-131).  Files energy<tag>/singular<tag> are
+   written to the current directory by the reference's printers. ---- */
+template <typename T>
+static void run_sched(mps<T>& s, mpo<T>& o, int m, int n, int sector, const string& tag,
+                      int schedule)
+{
+  if (schedule == 0) dmrg(s, o, m, n, sector, tag);
+  else if (schedule == 1) dmrg2(s, o, m, n, sector, tag);
+  else ed(s, o, m, n, sector, tag);
+}
+
+extern "C" int oref_run(int model, int L, int m, int n, int sector, const double* par,
+                        const char* tag, int schedule)
+{
+  string t(tag);
+#ifdef FERMION
+  if (model == 0) {
+    if (SYMMETRY != 2) return -2;
+    mpo<double> o(L);
+    for (int i = 0; i < L; i++) o[i] = H_Kitaev(par[0], par[1], par[2]);
+    o.edge(H_Kitaev(par[0], par[1], par[2]).left(), H_Kitaev(par[0], par[1], par[2]).right());
+    mps<double> s(o);
+    run_sched(s, o, m, n, sector, t, schedule);
+    return 0;
+  }
+#endif
+  if (model == 1) {
+    if (SYMMETRY != 2) return -2;
+    mpo<complex<double> > o(L, H_XYZ(par[0], par[1], par[2]));
+    o.edge();
+    mps<complex<double> > s(o);
+    run_sched(s, o, m, n, sector, t, schedule);
+    return 0;
+  }
+  if (model == 2) {
+    if (SYMMETRY != 3) return -2;
+    mpo<complex<double> > o(L, H_Potts3(par[0], par[1], par[2], par[3]));
+    o.edge();
+    mps<complex<double> > s(o);
+    run_sched(s, o, m, n, sector, t, schedule);
+    return 0;
+  }
+  return -1;
+}

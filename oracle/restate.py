@@ -1,0 +1,287 @@
+"""CPU restatement (numpy) of the reference's H_eff hot path.
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA path.  Only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may import it.
+
+Parity pin: every function here is checked against the reference itself, built
+from its own sources into ``oracle/_ref`` (``tests/test_oracle.py``), and
+against the golden fixtures committed under ``tests/golden/`` that were made
+from that build (``tests/golden/make_golden.py``).
+
+Block-sparse tensor convention (reference include/qtensor.h:26-31): ``dims[leg][sector]``
+sizes, ``syms[block][leg]`` sector labels, ``dirs[leg]`` fermion directions,
+``blocks[b]`` dense row-major (last index fastest, include/tensor.h:36-45).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from itertools import product
+
+import numpy as np
+
+
+# ----------------------------------------------------------------------------- fusion rule
+@dataclass(frozen=True)
+class Group:
+    """Z_N fusion rule ``ss`` and parity ``ff`` (src/useful.cpp:28-39).
+
+    ``fermion=False`` gives parity 0 everywhere: the bosonic models with the
+    reference's direction signs compiled out (the reference applies them to every
+    model, src/qtensor.cpp:1084, which makes bosonic H_eff non-Hermitian)."""
+    N: int
+    fermion: bool = False
+
+    def ss(self, a: int, b: int) -> int:
+        return (a + b + self.N) % self.N
+
+    def ff(self, a: int) -> int:
+        return (a % 2) if self.fermion else 0
+
+    def sign(self, x: int, y: int) -> int:
+        # 1 - 2*((ff(x)*ff(y)) % 2), the reference's sign form
+        return 1 - 2 * ((self.ff(x) * self.ff(y)) % 2)
+
+
+# ----------------------------------------------------------------------------- tensor type
+@dataclass
+class QT:
+    dims: list                      # dims[leg] = list of sector sizes
+    syms: list                      # list of tuples, one per block
+    blocks: list                    # list of ndarrays
+    dirs: list = field(default_factory=list)
+
+    @property
+    def nleg(self):
+        return len(self.dims)
+
+    def block_shape(self, sym):
+        return tuple(self.dims[l][s] for l, s in enumerate(sym))
+
+    def packed(self):
+        if not self.blocks:
+            return np.zeros(0)
+        return np.concatenate([b.reshape(-1) for b in self.blocks])
+
+    # serialised form shared with oracle/ref_hooks.cpp
+    def to_ibuf(self):
+        nl = self.nleg
+        out = [nl, len(self.syms)] + [len(d) for d in self.dims]
+        for d in self.dims:
+            out += list(d)
+        dirs = self.dirs if self.dirs else [0] * nl
+        out += list(dirs)
+        for s in self.syms:
+            out += list(s)
+        return np.array(out, np.int32)
+
+    @staticmethod
+    def from_ibuf(ib, vals):
+        ib = [int(x) for x in ib]
+        k = 0
+        nl, nb = ib[0], ib[1]
+        k = 2
+        nsec = ib[k:k + nl]
+        k += nl
+        dims = []
+        for l in range(nl):
+            dims.append(ib[k:k + nsec[l]])
+            k += nsec[l]
+        dirs = ib[k:k + nl]
+        k += nl
+        syms, blocks = [], []
+        v = 0
+        for b in range(nb):
+            s = tuple(ib[k:k + nl])
+            k += nl
+            shp = tuple(dims[l][s[l]] for l in range(nl))
+            sz = int(np.prod(shp)) if shp else 1
+            syms.append(s)
+            blocks.append(np.array(vals[v:v + sz]).reshape(shp))
+            v += sz
+        return QT(dims, syms, blocks, dirs)
+
+
+def generate_map(index):
+    """All label tuples in lexicographic order (src/useful.cpp:105-134)."""
+    return [tuple(t) for t in product(*[range(n) for n in index])]
+
+
+def get_dimension(dim, sym):
+    """Total size of a packed block list (src/useful.cpp:137-148)."""
+    return int(sum(np.prod([dim[j][s[j]] for j in range(len(dim))]) for s in sym))
+
+
+def generate_dim_sym(G: Group, ldims, lnum, rdims, rnum, sector):
+    """Sector list and ORDER of the packed wavefunction (src/useful.cpp:151-194).
+
+    dim = last ``lnum`` legs of the left env + last ``rnum`` legs of the right env.
+    Blocks ordered by left charge s = 0..N-1, then left label tuple, then right label
+    tuple (each lexicographic); kept where ss(lsym, rsym) == sector."""
+    dim = [list(d) for d in ldims[len(ldims) - lnum:]] + [list(d) for d in rdims[len(rdims) - rnum:]]
+    lmap = generate_map([len(d) for d in dim[:lnum]])
+    rmap = generate_map([len(d) for d in dim[lnum:]])
+    sym = []
+    if sector != -1:
+        for s in range(G.N):
+            t = G.ss(sector, -s)
+            for lt in lmap:
+                lsym = 0
+                for x in lt:
+                    lsym = G.ss(lsym, x)
+                for rt in rmap:
+                    rsym = 0
+                    for x in rt:
+                        rsym = G.ss(rsym, x)
+                    if lsym == s and rsym == t:
+                        sym.append(tuple(lt) + tuple(rt))
+    else:
+        sym = [tuple([0] * len(dim))]
+    return dim, sym
+
+
+def get_map(G: Group, T: QT, dim, sym, ta="N", tb="T", num=1, beta=0, back=False,
+            dim_ret=None, sym_ret=None):
+    """Task list of the block-sparse matvec (src/qtensor.cpp:997-1119).
+
+    Each row is [block, in_beg, out_beg, rows, cols, beta, alpha]; one GEMM
+    out[rows?] = alpha*T[block] x in^T per row.  With ``back=False`` the output
+    layout (dim_ret, sym_ret) is created in first-appearance order and alpha is
+    the fermionic sign; with ``back=True`` the given output layout is used, beta=0
+    on the first write to each output block and 1 afterwards, alpha = 1.
+    Returns (rows, dim_ret, sym_ret)."""
+    nT = T.nleg
+    indexa = nT - num if ta in "Nn" else 0
+    indexb = 0 if tb in "Nn" else len(dim) - num
+    for i in range(num):
+        if list(T.dims[indexa + i]) != list(dim[indexb + i]):
+            raise ValueError("get_map: dimensions differ")
+    new_dim_ret = [list(T.dims[i]) for i in range(nT) if i < indexa or i >= indexa + num] + \
+                  [list(dim[i]) for i in range(len(dim)) if i < indexb or i >= indexb + num]
+    # per input block: total size, "row" size, begin offset
+    sdim = []
+    beg = 0
+    for s in sym:
+        tot = int(np.prod([dim[k][s[k]] for k in range(len(dim))]))
+        if indexb:
+            row = int(np.prod([dim[k][s[k]] for k in range(indexb)]))
+        else:
+            row = int(np.prod([dim[k][s[k]] for k in range(num)]))
+        sdim.append((tot, row, beg))
+        beg += tot
+    rows = []
+    if back:
+        dim_ret = [list(d) for d in dim_ret]
+        keys = [_loc(s, dim_ret) for s in sym_ret]
+        offs = [0]
+        for s in sym_ret[:-1]:
+            offs.append(offs[-1] + int(np.prod([dim_ret[j][s[j]] for j in range(len(dim_ret))])))
+        first = [True] * len(keys)
+        sym_ret = list(sym_ret)
+    else:
+        dim_ret = new_dim_ret
+        keys, offs, sym_ret = [], [0], []
+        first = []
+    for i, ts in enumerate(T.syms):
+        for j, s in enumerate(sym):
+            if any(ts[indexa + k] != s[indexb + k] for k in range(num)):
+                continue
+            if sdim[j][0] == 0:
+                continue
+            row = [i, sdim[j][2], offs[-1], sdim[j][1], sdim[j][0] // sdim[j][1], beta, 1]
+            if not back:
+                d_b = 0
+                dirs = T.dirs if T.dirs else [0] * nT
+                for k in range(nT):
+                    d_b = G.ss(d_b, ts[k] * dirs[k])
+                a_p = 0
+                for k in range(len(dim) - num):
+                    a_p = G.ss(a_p, s[k])
+                row[6] = G.sign(d_b, a_p)
+            st = [ts[k] for k in range(nT) if k < indexa or k >= indexa + num] + \
+                 [s[k] for k in range(len(dim)) if k < indexb or k >= indexb + num]
+            loc = _loc(st, dim_ret)
+            same = False
+            for t, key in enumerate(keys):
+                if key == loc:
+                    row[2] = offs[t]
+                    if back and first[t]:
+                        first[t] = False
+                    else:
+                        row[5] = 1
+                    rows.append(list(row))
+                    same = True
+            if not same and not back:
+                d = int(np.prod([dim_ret[q][st[q]] for q in range(len(dim_ret))]))
+                offs.append(offs[-1] + d)
+                keys.append(loc)
+                sym_ret.append(tuple(st))
+                rows.append(list(row))
+    return np.array(rows, np.int64).reshape(-1, 7), dim_ret, sym_ret
+
+
+def _loc(st, dim_ret):
+    loc = 0
+    for q in range(len(dim_ret)):
+        loc = loc * len(dim_ret[q]) + st[q]
+    return loc
+
+
+def contract_map(T: QT, out, x, rows, num):
+    """Apply a task list (src/qtensor.cpp:986-994 -> src/tensor.cpp:698-718, 'N','T'):
+    out[ob : ob+M*N] = alpha * A[M x K] . X[N x K]^T + beta * out, row-major."""
+    for r in rows:
+        blk, ib, ob, nrow, ncol, beta, alpha = (int(v) for v in r)
+        A = T.blocks[blk]
+        K = int(np.prod(A.shape[A.ndim - num:]))
+        M = A.size // K
+        N, Kx = nrow, ncol
+        assert Kx == K
+        Am = A.reshape(M, K)
+        X = x[ib: ib + N * K].reshape(N, K)
+        C = alpha * (Am @ X.T)
+        if beta:
+            out[ob: ob + M * N] += C.reshape(-1)
+        else:
+            out[ob: ob + M * N] = C.reshape(-1)
+
+
+@dataclass
+class MatvecContext:
+    """The reference's ``lanczos<T>`` matvec context (include/val_for_lanczos.h:7-24)."""
+    lenv: QT
+    renv: QT
+    l_num: int
+    r_num: int
+    rmap: np.ndarray
+    lmap: np.ndarray
+    dim: list
+    sym: list
+    dim_ret: list
+    sym_ret: list
+    n: int
+    d_store: int
+
+
+def build_context(G: Group, lenv: QT, renv: QT, l_num: int, r_num: int, sector: int):
+    """What a reference step function does before the eigensolve
+    (src/core.cpp:201-202 and :236-247 for update_two)."""
+    dim, sym = generate_dim_sym(G, lenv.dims, l_num - 1, renv.dims, r_num, sector)
+    n = get_dimension(dim, sym)
+    rmap, dim_ret, sym_ret = get_map(G, renv, dim, sym, "N", "T", r_num, 0)
+    d_store = get_dimension(dim_ret, sym_ret)
+    # input = the store layout, output = the fixed wavefunction layout (back=True)
+    lmap, _, _ = get_map(G, lenv, dim_ret, sym_ret, "N", "T", l_num, 0, True, dim, sym)
+    return MatvecContext(lenv, renv, l_num, r_num, rmap, lmap, dim, sym, dim_ret, sym_ret,
+                         n, d_store)
+
+
+def av(ctx: MatvecContext, x):
+    """out = lenv (x)_{l_num} (renv (x)_{r_num} x)   (src/core.cpp:22-31).
+
+    Output sectors that no task writes are zero here (the reference leaves them
+    untouched)."""
+    store = np.zeros(ctx.d_store, np.result_type(x, ctx.renv.blocks[0]))
+    contract_map(ctx.renv, store, x, ctx.rmap, ctx.r_num)
+    out = np.zeros(ctx.n, store.dtype)
+    contract_map(ctx.lenv, out, store, ctx.lmap, ctx.l_num)
+    return out

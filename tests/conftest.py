@@ -1,0 +1,48 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+def load_steps(model):
+    """Golden per-step matvec fixtures of one model (see tests/golden/make_golden.py)."""
+    z = np.load(os.path.join(GOLDEN, f"steps_{model}.npz"))
+    gn, ferm, sector = (int(v) for v in z["group"])
+    out = []
+    for k in range(int(z["nsteps"])):
+        p = f"s{k}_"
+        out.append(dict(
+            lenv=(z[p + "lenv_meta"], z[p + "lenv_vals"]),
+            renv=(z[p + "renv_meta"], z[p + "renv_vals"]),
+            l_num=int(z[p + "nums"][0]), r_num=int(z[p + "nums"][1]),
+            rmap=z[p + "rmap"], lmap=z[p + "lmap"], x=z[p + "x"], ax=z[p + "ax"],
+            evals=z[p + "evals"], evec=z[p + "evec"],
+            group_n=gn, fermion=ferm, sector=sector,
+            complex=np.iscomplexobj(z[p + "lenv_vals"])))
+    return out
+
+
+def load_microbench_m64():
+    z = np.load(os.path.join(GOLDEN, "microbench_m64.npz"))
+    n, d_store, sector, gn = (int(v) for v in z["info"])
+    return dict(lenv=(z["lenv_meta"], z["lenv_vals"]), renv=(z["renv_meta"], z["renv_vals"]),
+                rmap=z["rmap"], lmap=z["lmap"], x=z["x"], ax=z["ax"], n=n, d_store=d_store,
+                sector=sector, group_n=gn, l_num=3, r_num=2, fermion=0, complex=False)
+
+
+MODELS = ("kitaev", "xyz", "potts")
+
+
+@pytest.fixture(scope="session")
+def golden_steps():
+    return {m: load_steps(m) for m in MODELS}

@@ -1,0 +1,116 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+    make -C oracle && python tests/golden/make_golden.py
+
+Runs the reference DMRG code (built unmodified from its sources into
+oracle/_ref by oracle/Makefile) and records:
+
+  steps_<model>.npz   per-step matvec fixtures captured inside the reference's
+                      eigensolver call: both environments (metadata + values),
+                      the reference task lists rmap/lmap, a seeded random psi x
+                      and the reference av(x) (src/core.cpp:22-31), the six
+                      lowest Ritz values and the lowest Ritz vector.  One step
+                      of each kind the schedule uses: update_two (l_num,r_num)
+                      = (3,2), move2right (3,1), move2left (2,2).
+  microbench_m64.npz  the U(1) microbench structure at m=64 (same generator as
+                      the m=1024 benchmark input), with the reference maps and
+                      av(x) from the Z_32-embedded reference build.
+  energies.json       final energies and truncation errors of small reference
+                      runs, with the exact energies (BdG / ED) beside them.
+
+The files are small (tens of KB) and committed; the GPU box never needs the
+reference tree.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import exact, refbind  # noqa: E402
+from dmrg_b200 import workloads    # noqa: E402
+
+RUNS = {
+    # model: (variant, L, m, sweeps, params, group_n, fermion, exact energy fn)
+    "kitaev": ("kitaev", 8, 16, 2, [1.0, 1.0, 0.25], 2, 1,
+               lambda: exact.kitaev_bdg(8, 1.0, 1.0, 0.25)),
+    "xyz": ("xyz", 8, 16, 2, [1.0, 0.8, 0.5], 2, 0,
+            lambda: exact.xyz_ed(8, 1.0, 0.8, 0.5, 0)),
+    "potts": ("potts", 6, 27, 2, [1.0, 1.0, 0.0, 0.0], 3, 0,
+              lambda: exact.potts_ed(6, 1.0, 1.0, 0)),
+}
+
+
+def pick_steps(steps):
+    """Last captured step of each (l_num, r_num) kind (largest bond dimension)."""
+    out = {}
+    for st in steps:
+        k = (st["info"]["l_num"], st["info"]["r_num"])
+        out[k] = st
+    return [out[k] for k in sorted(out)]
+
+
+def main():
+    energies = {}
+    for model, (variant, L, m, n, par, gn, ferm, exact_fn) in RUNS.items():
+        R = refbind.Ref(variant)
+        cap = refbind.StepCapture(want=lambda i, info: True)
+        res = R.run(model, L, m, n, 0, par, capture=cap)
+        chosen = pick_steps(cap.steps)
+        arrs = {}
+        for k, st in enumerate(chosen):
+            p = f"s{k}_"
+            arrs[p + "lenv_meta"], arrs[p + "lenv_vals"] = st["lenv"]
+            arrs[p + "renv_meta"], arrs[p + "renv_vals"] = st["renv"]
+            arrs[p + "nums"] = np.array([st["info"]["l_num"], st["info"]["r_num"]], np.int32)
+            arrs[p + "rmap"] = st["rmap"]
+            arrs[p + "lmap"] = st["lmap"]
+            arrs[p + "x"] = st["x"]
+            arrs[p + "ax"] = st["ax"]
+            arrs[p + "evals"] = st["evals"]
+            arrs[p + "evec"] = st["evec"]
+        arrs["nsteps"] = np.array(len(chosen))
+        arrs["group"] = np.array([gn, ferm, 0], np.int32)  # group_n, fermion, sector
+        np.savez_compressed(os.path.join(HERE, f"steps_{model}.npz"), **arrs)
+        e_exact = exact_fn()
+        energies[model] = dict(
+            args=dict(L=L, m=m, n=n, params=par, sector=0),
+            final_energy=float(res["energy"][-1, 2]),
+            energy_rows=res["energy"][:, :3].tolist(),
+            trunc_err_rows=res["singular"][:, [0, 1, -1]].tolist(),
+            exact=e_exact)
+        print(model, "steps", len(cap.steps), "E", res["energy"][-1, 2], "exact", e_exact)
+
+    # microbench at m=64 through the Z_32 reference build
+    w = workloads.microbench(64)
+    R = refbind.Ref("u1")
+    le = R.py_to_qt(0, *w["lenv"])
+    re_ = R.py_to_qt(0, *w["renv"])
+    info = (refbind.C.c_int * 4)()
+    box = R.lib.oref_pv_build(0, le, re_, 3, 2, w["sector"], info)
+    n = info[0]
+    pv_info = dict(l_num=3, r_num=2, n_rmap=info[2], n_lmap=info[3])
+    rmap, lmap = R.pv_maps(0, box, pv_info)
+    x = workloads.random_psi(n, seed=11)
+    ax = np.zeros(n)
+    R.lib.oref_av(0, box, x.ctypes.data, ax.ctypes.data)
+    np.savez_compressed(os.path.join(HERE, "microbench_m64.npz"),
+                        lenv_meta=w["lenv"][0], lenv_vals=w["lenv"][1],
+                        renv_meta=w["renv"][0], renv_vals=w["renv"][1],
+                        rmap=rmap, lmap=lmap, x=x, ax=ax,
+                        info=np.array([n, info[1], w["sector"], w["group_n"]], np.int64))
+    R.lib.oref_pv_free(0, box)
+    print("microbench m=64: n", n, "d_store", info[1], "tasks", info[2], info[3])
+
+    with open(os.path.join(HERE, "energies.json"), "w") as fh:
+        json.dump(energies, fh, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,124 @@
+"""H_eff matvec on the GPU (FP64 path) against the reference.
+
+Tolerance: FP64 with a different summation order than BLAS; every check is
+max|y - y_ref| <= 1e-13 * max|y_ref| (1e-12 at the m=1024 size)."""
+import numpy as np
+import pytest
+
+from conftest import MODELS, load_microbench_m64, load_steps
+from dmrg_b200 import native, workloads
+from oracle import restate
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-13
+
+
+def block_sizes(meta):
+    q = restate.QT.from_ibuf(meta, np.zeros(10 ** 8))
+    return np.array([b.size for b in q.blocks], np.int64)
+
+
+def close(y, ref, tol=TOL):
+    scale = max(np.abs(ref).max(), 1e-300)
+    return np.abs(y - ref).max() <= tol * scale
+
+
+@pytest.mark.parametrize("model", MODELS)
+def test_av_plan_build_matches_reference(model):
+    for st in load_steps(model):
+        ctx = native.Context(native.C128 if st["complex"] else native.F64)
+        ctx.plan_build(st["lenv"], st["renv"], st["l_num"], st["r_num"], st["sector"],
+                       st["group_n"], st["fermion"])
+        r, l = ctx.maps()
+        assert np.array_equal(r, st["rmap"]) and np.array_equal(l, st["lmap"])
+        assert close(ctx.av(st["x"]), st["ax"])
+        ctx.close()
+
+
+@pytest.mark.parametrize("model", MODELS)
+def test_av_from_reference_maps(model):
+    """The drop-in entry: the reference's own rmap/lmap and env blocks."""
+    for st in load_steps(model):
+        ctx = native.Context(native.C128 if st["complex"] else native.F64)
+        n = st["x"].size
+        rs, ls = block_sizes(st["renv"][0]), block_sizes(st["lenv"][0])
+        # d_store = end of the furthest stage-1 output block
+        d_store = 0
+        for row in st["rmap"]:
+            M = rs[row[0]] // row[4]
+            d_store = max(d_store, row[2] + M * row[3])
+        ctx.plan_from_maps(n, d_store, st["rmap"], st["renv"][1], rs, st["lmap"], st["lenv"][1], ls)
+        assert close(ctx.av(st["x"]), st["ax"])
+        ctx.close()
+
+
+def test_av_microbench_m64():
+    mb = load_microbench_m64()
+    ctx = native.Context(native.F64)
+    ctx.plan_build(mb["lenv"], mb["renv"], 3, 2, mb["sector"], mb["group_n"], 0)
+    assert ctx.n == mb["n"]
+    assert close(ctx.av(mb["x"]), mb["ax"])
+
+
+def test_av_microbench_full_size_against_restatement():
+    w = workloads.microbench(1024)
+    ctx = native.Context(native.F64)
+    ctx.plan_build(w["lenv"], w["renv"], 3, 2, w["sector"], 32, 0)
+    assert ctx.n == 599964 and ctx.flops == 3861687920
+    le = restate.QT.from_ibuf(*w["lenv"])
+    re_ = restate.QT.from_ibuf(*w["renv"])
+    rmap, lmap = ctx.maps()
+    x = workloads.random_psi(ctx.n, seed=2)
+    store = np.zeros(ctx.d_store)
+    restate.contract_map(re_, store, x, rmap, 2)
+    ref = np.zeros(ctx.n)
+    restate.contract_map(le, ref, store, lmap, 3)
+    y = ctx.av(x)
+    assert close(y, ref, 1e-12)
+    # linearity at full size
+    x2 = workloads.random_psi(ctx.n, seed=3)
+    y2 = ctx.av(x2)
+    y3 = ctx.av(2.0 * x - 0.5 * x2)
+    assert close(y3, 2.0 * y - 0.5 * y2, 1e-12)
+
+
+@pytest.mark.parametrize("model", MODELS)
+def test_av_is_hermitian_on_physical_steps(model):
+    """<u|H v> = <H u|v>: the reference's check_hermitian (src/core.cpp:40-83) as a
+    size-independent property (bosonic models need the sign fix)."""
+    rng = np.random.default_rng(0)
+    for st in load_steps(model):
+        ctx = native.Context(native.C128 if st["complex"] else native.F64)
+        ctx.plan_build(st["lenv"], st["renv"], st["l_num"], st["r_num"], st["sector"],
+                       st["group_n"], st["fermion"])
+        u = rng.standard_normal(ctx.n) + (1j * rng.standard_normal(ctx.n) if st["complex"] else 0)
+        v = rng.standard_normal(ctx.n) + (1j * rng.standard_normal(ctx.n) if st["complex"] else 0)
+        a = np.vdot(u, ctx.av(v))
+        b = np.vdot(ctx.av(u), v)
+        assert abs(a - b) <= 1e-11 * max(abs(a), 1.0)
+
+
+def test_av_small_odd_and_empty_blocks():
+    """Tiny, odd and zero-size sectors: m=2..7 microbench structures."""
+    for m in (9, 13, 21, 35):
+        w = workloads.microbench(m, seed=m)
+        ctx = native.Context(native.F64)
+        ctx.plan_build(w["lenv"], w["renv"], 3, 2, w["sector"], 32, 0)
+        le = restate.QT.from_ibuf(*w["lenv"])
+        re_ = restate.QT.from_ibuf(*w["renv"])
+        rc = restate.build_context(restate.Group(32), le, re_, 3, 2, w["sector"])
+        x = workloads.random_psi(rc.n, seed=m)
+        assert close(ctx.av(x), restate.av(rc, x))
+
+
+def test_av_device_pointers():
+    import torch
+    mb = load_microbench_m64()
+    ctx = native.Context(native.F64)
+    ctx.plan_build(mb["lenv"], mb["renv"], 3, 2, mb["sector"], mb["group_n"], 0)
+    x = torch.tensor(mb["x"], device="cuda:0")
+    y = torch.empty_like(x)
+    torch.cuda.synchronize()
+    ctx.av_device(x.data_ptr(), y.data_ptr())
+    ctx.sync()
+    assert close(y.cpu().numpy(), mb["ax"])

@@ -1,0 +1,81 @@
+"""The oracle itself, pinned against the reference's golden outputs (CPU only)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, MODELS, load_microbench_m64, load_steps
+from oracle import exact, restate
+
+
+def _ctx(st):
+    G = restate.Group(st["group_n"], bool(st["fermion"]))
+    le = restate.QT.from_ibuf(*st["lenv"])
+    re_ = restate.QT.from_ibuf(*st["renv"])
+    return restate.build_context(G, le, re_, st["l_num"], st["r_num"], st["sector"])
+
+
+@pytest.mark.parametrize("model", MODELS)
+def test_restatement_maps_and_av_match_reference(model):
+    for st in load_steps(model):
+        ctx = _ctx(st)
+        assert np.array_equal(ctx.rmap, st["rmap"])
+        assert np.array_equal(ctx.lmap, st["lmap"])
+        y = restate.av(ctx, st["x"])
+        assert np.allclose(y, st["ax"], rtol=0, atol=1e-13 * np.abs(st["ax"]).max())
+
+
+@pytest.mark.parametrize("model", MODELS)
+def test_reference_ritz_pair(model):
+    """The captured Ritz vector is an eigenvector of the captured operator."""
+    for st in load_steps(model):
+        ctx = _ctx(st)
+        v = st["evec"] / np.linalg.norm(st["evec"])
+        hv = restate.av(ctx, v)
+        e = np.vdot(v, hv).real
+        assert abs(e - st["evals"][0]) < 1e-8 * max(1.0, abs(e))
+        assert np.linalg.norm(hv - e * v) < 1e-6 * max(1.0, abs(e))
+
+
+def test_restatement_microbench_m64():
+    mb = load_microbench_m64()
+    ctx = _ctx(dict(mb, l_num=3, r_num=2))
+    assert ctx.n == mb["n"] and ctx.d_store == mb["d_store"]
+    assert np.array_equal(ctx.rmap, mb["rmap"]) and np.array_equal(ctx.lmap, mb["lmap"])
+    y = restate.av(ctx, mb["x"])
+    assert np.allclose(y, mb["ax"], rtol=0, atol=1e-13 * np.abs(mb["ax"]).max())
+
+
+def test_exact_energies_pin_reference_runs():
+    with open(os.path.join(GOLDEN, "energies.json")) as fh:
+        en = json.load(fh)
+    ex = {"kitaev": exact.kitaev_bdg(8, 1.0, 1.0, 0.25),
+          "xyz": exact.xyz_ed(8, 1.0, 0.8, 0.5, 0),
+          "potts": exact.potts_ed(6, 1.0, 1.0, 0)}
+    for m in MODELS:
+        assert abs(en[m]["exact"] - ex[m]) < 1e-12
+        # the reference prints 10 digits after the point (global.h ACC)
+        assert abs(en[m]["final_energy"] - ex[m]) < 2e-10 * abs(ex[m]) + 1e-10
+
+
+def test_restatement_against_live_reference():
+    """When the reference build is present, restatement == reference on fresh inputs."""
+    from oracle import refbind
+    if not refbind.available("u1"):
+        pytest.skip("oracle/_ref not built in this checkout")
+    from dmrg_b200 import workloads
+    w = workloads.microbench(48, seed=5)
+    R = refbind.Ref("u1")
+    le, re_ = R.py_to_qt(0, *w["lenv"]), R.py_to_qt(0, *w["renv"])
+    info = (refbind.C.c_int * 4)()
+    box = R.lib.oref_pv_build(0, le, re_, 3, 2, w["sector"], info)
+    rmap, lmap = R.pv_maps(0, box, dict(n_rmap=info[2], n_lmap=info[3]))
+    x = workloads.random_psi(info[0], seed=3)
+    y = np.zeros_like(x)
+    R.lib.oref_av(0, box, x.ctypes.data, y.ctypes.data)
+    ctx = _ctx(dict(lenv=w["lenv"], renv=w["renv"], l_num=3, r_num=2, sector=w["sector"],
+                    group_n=32, fermion=0))
+    assert np.array_equal(ctx.rmap, rmap) and np.array_equal(ctx.lmap, lmap)
+    assert np.allclose(restate.av(ctx, x), y, rtol=0, atol=1e-13 * np.abs(y).max())
+    R.lib.oref_pv_free(0, box)
