@@ -120,6 +120,8 @@ std::string build_stage(const std::vector<MapRow>& rows, const std::vector<int64
     if (r.out_beg < 0 || r.out_beg + M * N > out_len) return "task row: output range out of bounds";
     if (M * f > INT32_MAX || N * f > INT32_MAX || K * f > INT32_MAX)
       return "task row: block extent too large";
+    // an empty output block writes nothing (and shares its offset with the next block)
+    if (M == 0 || N == 0) continue;
     auto it = by_off.find(r.out_beg);
     int oi;
     if (it == by_off.end()) {
