@@ -35,6 +35,8 @@ SIGNATURES = {
     "dmrgx_plan_maps": (_i, [_vp, _ip, _ip]),
     "dmrgx_plan_psi_layout": (_i, [_vp, _ip, _i64]),
     "dmrgx_av": (_i, [_vp, _vp, _vp, _i]),
+    "dmrgx_av_noalloc": (_i, [_i, _i64, _i64, _ip, _i, _vp, _i64p, _i, _ip, _i, _vp, _i64p, _i,
+                              _vp, _vp, _vp]),
     "dmrgx_stream": (_vp, [_vp]),
     "dmrgx_sync": (_i, [_vp]),
 }
@@ -86,6 +88,22 @@ def build_maps(lenv_meta, renv_meta, l_num, r_num, sector, group_n, fermion):
                                   _i64p(info), _ip(rmap), rmap.shape[0], _ip(lmap),
                                   lmap.shape[0]))
     return int(info[0]), int(info[1]), rmap[: info[2]], lmap[: info[3]]
+
+
+def av_noalloc(dtype, n, d_store, rmap, renv_dev, renv_sizes, lmap, lenv_dev, lenv_sizes,
+               in_dev, out_dev, stream=0):
+    """dmrgx_av_noalloc: device pointers for values and vectors, host task lists.
+
+    The work is queued on ``stream`` (0 = legacy default stream); nothing is
+    allocated on the device."""
+    rmap = np.ascontiguousarray(rmap, np.int32).reshape(-1, 7)
+    lmap = np.ascontiguousarray(lmap, np.int32).reshape(-1, 7)
+    rs = np.ascontiguousarray(renv_sizes, np.int64)
+    ls = np.ascontiguousarray(lenv_sizes, np.int64)
+    _check(lib().dmrgx_av_noalloc(dtype, n, d_store, _ip(rmap), rmap.shape[0],
+                                  C.c_void_p(renv_dev), _i64p(rs), rs.size, _ip(lmap),
+                                  lmap.shape[0], C.c_void_p(lenv_dev), _i64p(ls), ls.size,
+                                  C.c_void_p(in_dev), C.c_void_p(out_dev), C.c_void_p(stream)))
 
 
 class Context:

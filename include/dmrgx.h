@@ -117,6 +117,32 @@ int dmrgx_plan_psi_layout(dmrgx_ctx* ctx, int* out, int64_t cap);
  * to zero (the reference leaves them untouched). */
 int dmrgx_av(dmrgx_ctx* ctx, const void* in, void* out, int mem);
 
+/* H_eff matvec that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc/cudaFree while they apply H_eff: an
+ * eigensolver loop inside a host framework whose own allocator has reserved the
+ * device memory, or a loop that cannot afford the device-wide synchronisation
+ * that allocation may cause.  Same arithmetic as dmrgx_plan_from_maps followed
+ * by dmrgx_av, without a context:
+ *   renv/lenv  device arrays, environment blocks packed in the reference's
+ *              block order (the values of lanczos<T>::renv / lenv);
+ *   rmap/lmap  host arrays, the reference's task lists (7 ints per row);
+ *   *_sizes    host arrays, element count of every environment block;
+ *   in/out     device arrays of n elements; stream: a cudaStream_t (NULL = legacy
+ *              default stream).  The work is queued on `stream`; the call returns
+ *              without waiting for it.
+ * The intermediate (d_store elements) and the task descriptors live in one
+ * static device array of the library (32 MiB for the intermediate, 4 MiB for
+ * descriptors), held by every GPU that loads the library until exit.  Larger
+ * problems (d_store * element size > 32 MiB, more than 16384 task rows per
+ * stage or 65536 blocks per environment) return DMRGX_E_ARG.  The first call on a
+ * device looks the array up on that device (make it before any stream
+ * capture).  All calls share the array: calls whose GPU work overlaps race. */
+int dmrgx_av_noalloc(int dtype, int64_t n, int64_t d_store, const int* rmap, int n_rmap,
+                     const void* renv, const int64_t* renv_sizes, int n_renv_blocks,
+                     const int* lmap, int n_lmap, const void* lenv, const int64_t* lenv_sizes,
+                     int n_lenv_blocks, const void* in, void* out, void* stream);
+
 /* The context's CUDA stream (a cudaStream_t), for callers that order their own
  * device work with dmrgx_av(..., DMRGX_MEM_DEVICE). */
 void* dmrgx_stream(dmrgx_ctx* ctx);
