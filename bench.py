@@ -38,7 +38,7 @@ def parse():
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=5)
-    p.add_argument("--prec", default="fp64", choices=["fp64", "bf16x3", "tf32x3"])
+    p.add_argument("--prec", default="bf16x3", choices=["fp64", "bf16x3", "tf32x3"])
     p.add_argument("--impl", default="dmrgx", choices=["dmrgx", "reference"])
     p.add_argument("--cpu-sample-s", type=float, default=12.0)
     return p.parse_args()
@@ -212,6 +212,35 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def time_matvecs(torch, ctx, stream, xs, ys, flush, steps, warmup, profile=False):
+    """Device time of `steps` matvecs (inputs resident, L2 flushed before each,
+    outside the events).  Returns (seconds, per-slot profile or None)."""
+    def one(timed):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            if timed:
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record(stream)
+            ctx.av_device(xs.data_ptr(), ys.data_ptr())
+            if timed:
+                e.record(stream)
+                return s, e
+        return None
+
+    for _ in range(warmup):
+        one(False)
+    torch.cuda.synchronize()
+    if profile:
+        ctx.profile(True)
+    evs = [one(True) for _ in range(steps)]
+    torch.cuda.synchronize()
+    prof = None
+    if profile:
+        prof = ctx.profile_read()
+        ctx.profile(False)
+    return sum(s.elapsed_time(e) for s, e in evs) / 1e3, prof
+
+
 def main():
     args = parse()
     world, rank, local = dist_init(args)
@@ -235,26 +264,15 @@ def main():
     ctx.plan_build(w["lenv"], w["renv"], 3, 2, w["sector"], 32, 0)
     n, flops = ctx.n, ctx.flops
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    ref = None
+    if prec != native.PREC_FP64:   # the plain FP64 GPU path on the same input, for the ratio
+        ref = native.Context(native.F64, local)
+        ref.plan_build(w["lenv"], w["renv"], 3, 2, w["sector"], 32, 0)
+        ref_stream = torch.cuda.ExternalStream(ref.stream(), device=dev)
 
     xs = torch.tensor(workloads.random_psi(n, seed=5), device=dev)
     ys = torch.empty_like(xs)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    torch.cuda.synchronize()
-
-    def step_device(timed):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-            if timed:
-                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                s.record(stream)
-            ctx.av_device(xs.data_ptr(), ys.data_ptr())
-            if timed:
-                e.record(stream)
-                return s, e
-        return None
-
-    for _ in range(args.warmup):
-        step_device(False)
     torch.cuda.synchronize()
 
     try:
@@ -266,16 +284,31 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     clocks.start()
-    evs = [step_device(True) for _ in range(args.steps)]
-    torch.cuda.synchronize()
+    dev_s, _ = time_matvecs(torch, ctx, stream, xs, ys, flush, args.steps, args.warmup)
     ck = clocks.stop()
-    dev_s = sum(s.elapsed_time(e) for s, e in evs) / 1e3
     if world > 1:
         t = torch.tensor([dev_s], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev_s = float(t.item())
     per = dev_s / args.steps
     value = world * args.steps / dev_s
+    y_main = ys.cpu().numpy()
+
+    # per-launch device times of the same workload (events between launches)
+    _, prof = time_matvecs(torch, ctx, stream, xs, ys, flush, args.steps, 1, profile=True)
+    cnt, slots = prof
+
+    fp64 = None
+    if ref is not None:
+        ys64 = torch.empty_like(xs)
+        f_s, _ = time_matvecs(torch, ref, ref_stream, xs, ys64, flush, args.steps, args.warmup)
+        _, (fc, fslots) = time_matvecs(torch, ref, ref_stream, xs, ys64, flush, args.steps, 1,
+                                       profile=True)
+        y64 = ys64.cpu().numpy()
+        rel_err = float(np.linalg.norm(y_main - y64) / np.linalg.norm(y64))
+        fp64 = {"value": args.steps / f_s, "ms_per_step": 1e3 * f_s / args.steps,
+                "stage_ms": [float(x / fc) for x in fslots[1:]],
+                "tflops": flops / (float(fslots[1] + fslots[2]) / fc / 1e3) / 1e12}
 
     # end to end through the C ABI with host buffers (copies inside the timing)
     xh = workloads.random_psi(n, seed=6)
@@ -294,15 +327,20 @@ def main():
 
     if rank == 0:
         peaks, src = measured_peaks()
+        gemm_s = float(slots[1] + slots[2]) / cnt / 1e3   # both stage launches of the kernel
+        achieved = flops / gemm_s / 1e12
         if args.prec == "fp64":
             pk = fp64_gemm_peak(torch, dev)
-            peak_unit, bound = "TFLOP/s", "tensor"
-            peak_note = "in-run cuBLAS DGEMM 8192^3 burst (FP64 tensor cores)"
-        else:
+            peak_note = "in-run cuBLAS DGEMM 8192^3 burst (FP64 tensor cores); no FP64 figure in MEASURED_PEAKS.json"
+            kernel = "grouped_gemm_nt_f64 (stage 1 + stage 2 launches)"
+        elif args.prec == "bf16x3":
             pk = peaks["bf16_tflops"]
-            peak_unit, bound = "TFLOP/s", "tensor"
-            peak_note = f"bf16_tflops of MEASURED_PEAKS.json ({src})"
-        achieved = flops / per / 1e12
+            peak_note = f"bf16_tflops of MEASURED_PEAKS.json ({src}, burst)"
+            kernel = "grouped_split_tc<bf16> (stage 1 + stage 2 launches)"
+        else:
+            pk = peaks["bf16_tflops"] / 2
+            peak_note = f"half the bf16_tflops of MEASURED_PEAKS.json ({src}): TF32 runs at half the BF16 rate"
+            kernel = "grouped_split_tc<tf32> (stage 1 + stage 2 launches)"
         cpu = cpu_reference_rate(args.cpu_sample_s, w)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -314,18 +352,26 @@ def main():
                        "gflop_per_matvec": flops / 1e9, "precision": args.prec,
                        "parallelism": f"replicas x{world}",
                        "l2": "flushed (256 MiB write) before every timed step"},
-            "roofline": {"bound": bound, "achieved": achieved, "peak": pk, "unit": peak_unit,
-                         "frac": achieved / pk, "traffic": None,
-                         "kernel": "grouped_gemm_nt_f64 (both stages)",
-                         "peak_source": peak_note},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
+                         "frac": achieved / pk, "traffic": None, "kernel": kernel,
+                         "peak_source": peak_note,
+                         "note": "achieved = algorithmic flops (2MNK per task, not counting the "
+                                 "3 split products) / summed device time of the stage launches",
+                         "stage_ms": [float(x / cnt) for x in slots]},
             "cpu_baseline": cpu,
             "e2e": {"value": world * args.steps / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8},
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": (2 if args.prec == "fp64" else 3) * args.steps,
             "clocks": ck,
         }
+        if fp64 is not None:
+            line["fp64_path"] = fp64
+            line["split_vs_fp64"] = value / fp64["value"]
+            line["split_rel_err"] = rel_err
         print(json.dumps(line), flush=True)
     ctx.close()
+    if ref is not None:
+        ref.close()
     if world > 1:
         dist.destroy_process_group()
 

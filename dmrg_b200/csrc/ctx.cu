@@ -9,10 +9,14 @@
 #include "../../include/dmrgx.h"
 #include "ctx.h"
 #include "kernels.h"
+#include "split.h"
 
 using namespace dmrgx;
 
 namespace dmrgx {
+
+int build_split_plan(dmrgx_ctx* c, int eb);
+int run_matvec_split(dmrgx_ctx* c, const double* in, double* out);
 
 static thread_local std::string g_err;
 void set_error(const std::string& msg) { g_err = msg; }
@@ -33,6 +37,18 @@ cudaError_t DevBuf::ensure(size_t b) {
   if (e == cudaSuccess) bytes = b;
   return e;
 }
+
+}  // namespace dmrgx
+
+void dmrgx_ctx::prof_mark() {
+  if (!prof) return;
+  cudaEvent_t e;
+  if (cudaEventCreate(&e) != cudaSuccess) return;
+  cudaEventRecord(e, stream);
+  prof_ev.push_back(e);
+}
+
+namespace dmrgx {
 
 void DevBuf::release() {
   if (p) cudaFree(p);
@@ -247,12 +263,35 @@ int finalize_plan(dmrgx_ctx* c, const double* renv_vals, const std::vector<int64
   }
   // ri/li are host temporaries: wait for the uploads before they go away
   CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->sp.free_device();
+  c->sp = SplitPlan();
+  if (c->prec != DMRGX_PREC_FP64) {
+    rc = build_split_plan(c, c->prec == DMRGX_PREC_BF16X3 ? 2 : 4);
+    if (rc) return rc;
+  }
   c->has_plan = true;
   return 0;
 }
 
+// error word of the bounded device waits (split path); 0 = fine
+int check_device_error(dmrgx_ctx* c) {
+  if (!c->err.p) return 0;
+  int h = 0;
+  CUDA_TRY(cudaMemcpyAsync(&h, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (h) {
+    set_error("a bounded device wait timed out in the split-precision matvec");
+    CUDA_TRY(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+    return DMRGX_E_TIMEOUT;
+  }
+  return 0;
+}
+
 int run_matvec(dmrgx_ctx* c, const double* in, double* out) {
+  if (c->prec != DMRGX_PREC_FP64) return run_matvec_split(c, in, out);
   const bool cplx = c->dtype == DMRGX_C128;
+  c->prof_mark();
+  c->prof_mark();
   const int grid = c->num_sms * 3;
   double* store = (double*)c->store.p;
   if (!c->st1.full_cover)
@@ -260,11 +299,13 @@ int run_matvec(dmrgx_ctx* c, const double* in, double* out) {
   CUDA_TRY(launch_grouped_f64((const double*)c->renv.p, in, store, c->st1.d_tiles,
                               (int)c->st1.tiles.size(), c->st1.d_outs, c->st1.d_segs, cplx, grid,
                               c->stream));
+  c->prof_mark();
   if (!c->st2.full_cover)
     CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double) * c->n * c->f(), c->stream));
   CUDA_TRY(launch_grouped_f64((const double*)c->lenv.p, store, out, c->st2.d_tiles,
                               (int)c->st2.tiles.size(), c->st2.d_outs, c->st2.d_segs, cplx, grid,
                               c->stream));
+  c->prof_mark();
   return 0;
 }
 
@@ -309,6 +350,10 @@ void dmrgx_ctx_destroy(dmrgx_ctx* c) {
   cudaStreamSynchronize(c->stream);
   c->st1.free_device();
   c->st2.free_device();
+  for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+  c->sp.free_device();
+  for (DevBuf* b : {&c->sa1, &c->sa2, &c->spsi, &c->sstore, &c->sws, &c->err})
+    b->release();
   c->renv.release();
   c->lenv.release();
   c->store.release();
@@ -322,8 +367,22 @@ void dmrgx_ctx_destroy(dmrgx_ctx* c) {
 
 int dmrgx_set_precision(dmrgx_ctx* c, int prec) {
   ARG_CHECK(c, "null context");
-  ARG_CHECK(prec == DMRGX_PREC_FP64, "set_precision: only DMRGX_PREC_FP64 is available");
+  ARG_CHECK(prec == DMRGX_PREC_FP64 || prec == DMRGX_PREC_BF16X3 || prec == DMRGX_PREC_TF32X3,
+            "set_precision: unknown precision");
+  ARG_CHECK(prec == DMRGX_PREC_FP64 || c->dtype == DMRGX_F64,
+            "set_precision: split precision is available for F64 contexts");
+  if (prec == c->prec) return 0;
   c->prec = prec;
+  c->sp.free_device();
+  c->sp = SplitPlan();
+  if (c->has_plan && prec != DMRGX_PREC_FP64) {
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc = build_split_plan(c, prec == DMRGX_PREC_BF16X3 ? 2 : 4);
+    if (rc) {
+      c->has_plan = false;
+      return rc;
+    }
+  }
   return 0;
 }
 
@@ -520,7 +579,34 @@ int dmrgx_av(dmrgx_ctx* c, const void* in, void* out, int mem) {
   if (rc) return rc;
   CUDA_TRY(cudaMemcpyAsync(c->h_out, c->dout.p, bytes, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
+  rc = check_device_error(c);
+  if (rc) return rc;
   std::memcpy(out, c->h_out, bytes);
+  return 0;
+}
+
+int dmrgx_profile(dmrgx_ctx* c, int enable) {
+  ARG_CHECK(c, "null context");
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+  c->prof_ev.clear();
+  c->prof = enable != 0;
+  return 0;
+}
+
+int dmrgx_profile_read(dmrgx_ctx* c, double* out, int cap) {
+  ARG_CHECK(c && out && cap >= 4, "profile_read: need a context and 4 output slots");
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < cap; i++) out[i] = 0.0;
+  const size_t n = c->prof_ev.size() / 4;
+  for (size_t m = 0; m < n; m++) {
+    for (int k = 0; k < 3; k++) {
+      float ms = 0.f;
+      CUDA_TRY(cudaEventElapsedTime(&ms, c->prof_ev[4 * m + k], c->prof_ev[4 * m + k + 1]));
+      out[1 + k] += ms;
+    }
+  }
+  out[0] = (double)n;
   return 0;
 }
 
@@ -529,7 +615,7 @@ void* dmrgx_stream(dmrgx_ctx* c) { return c ? (void*)c->stream : nullptr; }
 int dmrgx_sync(dmrgx_ctx* c) {
   ARG_CHECK(c, "null context");
   CUDA_TRY(cudaStreamSynchronize(c->stream));
-  return 0;
+  return check_device_error(c);
 }
 
 }  // extern "C"

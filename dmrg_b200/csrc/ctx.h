@@ -9,6 +9,7 @@
 
 #include "grouped.h"
 #include "qmeta.h"
+#include "split.h"
 
 namespace dmrgx {
 
@@ -34,6 +35,35 @@ struct DevBuf {
   void release();
 };
 
+// The split-precision form of a plan: descriptors of one stage.
+struct SplitStage {
+  std::vector<SOut> outs;
+  std::vector<SSeg2> segs;
+  std::vector<SUnit> units;
+  std::vector<SRed> reds;
+  std::vector<CUtensorMap> maps;
+  SOut* d_outs = nullptr;
+  SSeg2* d_segs = nullptr;
+  SUnit* d_units = nullptr;
+  SRed* d_reds = nullptr;
+  CUtensorMap* d_maps = nullptr;
+  int nslots = 0;
+  bool full_cover = true;
+  void free_device();
+};
+
+// Split-precision plan: (hi, lo) operand images (hi at [0, len), lo at
+// [len, 2 len) of one buffer each) and the two stages.
+struct SplitPlan {
+  int eb = 0;                      // element bytes of the pairs: 2 BF16, 4 TF32 (0 = none)
+  SplitStage s1, s2;
+  int64_t a1_len = 0, a2_len = 0, psi_len = 0, store_len = 0;   // elements per half
+  std::vector<PadJob> psi_jobs;    // per-matvec FP64 psi -> (hi, lo)
+  PadJob* d_psi_jobs = nullptr;
+  int64_t psi_max_job = 0;
+  void free_device();
+};
+
 }  // namespace dmrgx
 
 struct dmrgx_ctx {
@@ -51,6 +81,11 @@ struct dmrgx_ctx {
   dmrgx::Stage st1, st2;
 
   dmrgx::DevBuf renv, lenv, store, din, dout;  // device
+  dmrgx::SplitPlan sp;                            // split-precision form (built on demand)
+  dmrgx::DevBuf sa1, sa2, spsi, sstore, sws, err;  // split-precision buffers
+  bool prof = false;                            // per-launch event timing
+  std::vector<cudaEvent_t> prof_ev;             // 4 per timed matvec
+  void prof_mark();                             // record one event if profiling
   double* h_in = nullptr;                       // pinned staging
   double* h_out = nullptr;
   size_t h_cap = 0;

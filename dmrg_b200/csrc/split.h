@@ -1,0 +1,71 @@
+// Split-precision (hi/lo BF16 or TF32 pairs) grouped GEMM on tcgen05: descriptors
+// and launchers (split.cu: operand conversion, tc_gemm.cu: the GEMM).
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "grouped.h"
+
+namespace dmrgx {
+
+// Output block of the split path.  Offsets/extents in elements of the arrays
+// the kernel writes: the padded (hi, lo) intermediate for stage 1, the packed FP64
+// psi for stage 2.
+struct SOut {
+  int64_t c_off;
+  int32_t m, n;      // rows, columns
+  int32_t ldc;       // row stride of C (>= n)
+  int32_t seg_begin, seg_count;
+  int32_t pad_;
+};
+
+// One segment of an output block: tensor-map indices of its A block (m x kp) and
+// B block (n x kp), its k-tile count, and the row count of the B map's box.
+struct SSeg2 {
+  int32_t amap, bmap;
+  int32_t nkt;
+  int32_t brows;
+};
+
+// Work unit: k-tiles [kt0, kt1) (over the output block's segments, in order) of
+// the output tile (tm, tn).  slot >= 0: write the FP32 partial to that
+// workspace slot (the tile is split along K); slot < 0: write the result.
+struct SUnit {
+  int32_t out;
+  int16_t tm, tn;
+  int32_t kt0, kt1;
+  int32_t slot, pad_;
+};
+
+// A K-split output tile: its partials are workspace slots [slot0, slot0+nslots).
+struct SRed {
+  int32_t out;
+  int16_t tm, tn;
+  int32_t slot0, nslots;
+};
+
+// FP64 -> (hi, lo) conversion job: rows x (groups x cols) source elements,
+// destination rows of groups x colsp elements (colsp >= cols, zero padding).
+struct PadJob {
+  int64_t src, dst;
+  int32_t rows, groups, cols, colsp;
+};
+
+int tc_smem_bytes();
+int tc_tile_m();
+int tc_tile_n();
+int tc_ktile_bytes();
+
+cudaError_t launch_pad_split(int eb, const double* src, void* hi, void* lo, const PadJob* jobs,
+                             int njobs, int64_t max_elems, cudaStream_t st);
+
+// One stage: the warp-specialized TMA/tcgen05 kernel over `units`, then the
+// reduction of K-split tiles (if any).
+cudaError_t launch_tc_gemm(int eb, bool out_split, const CUtensorMap* maps, const SUnit* units,
+                           int nunits, const SOut* outs, const SSeg2* segs, void* c_hi, void* c_lo,
+                           double* c64, float* ws, const SRed* reds, int nreds, int* err, int grid,
+                           cudaStream_t st);
+
+}  // namespace dmrgx

@@ -1,0 +1,386 @@
+// Split-precision form of a matvec plan, derived from the FP64 plan of the same
+// context: padded (hi, lo) operand images, one TMA tensor map per operand block,
+// and K-split work units for the warp-specialized tcgen05 kernel (tc_gemm.cu).
+//
+// Stage 1 (store = renv (x) psi):
+//   A1 = renv blocks, M1 x K1 -> rows padded to K1p (a multiple of 16 bytes)
+//   B1 = psi blocks as stage 1 views them, N1 x K1 -> N1 x K1p, split every matvec
+//   C1 = the intermediate, M1 x N1 -> written as (hi, lo) with row stride N1p
+// Stage 2 (out = lenv (x) store):
+//   the intermediate block (M1 x N1p) read as N2 x (D x N1p) with D = M1 / N2
+//   (its rows are the stage-2 rows times the MPO channel, src/core.cpp:188-192),
+//   A2 = lenv blocks M2 x (D x N1) -> M2 x (D x N1p), zeros in each slice's padding
+//   C2 = packed FP64 psi.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+
+#include "../../include/dmrgx.h"
+#include "ctx.h"
+#include "split.h"
+
+namespace dmrgx {
+
+void SplitStage::free_device() {
+  cudaFree(d_outs);
+  cudaFree(d_segs);
+  cudaFree(d_units);
+  cudaFree(d_reds);
+  cudaFree(d_maps);
+  d_outs = nullptr;
+  d_segs = nullptr;
+  d_units = nullptr;
+  d_reds = nullptr;
+  d_maps = nullptr;
+}
+
+void SplitPlan::free_device() {
+  s1.free_device();
+  s2.free_device();
+  cudaFree(d_psi_jobs);
+  d_psi_jobs = nullptr;
+}
+
+namespace {
+
+#define SP_TRY(expr)                                                                   \
+  do {                                                                                 \
+    cudaError_t e_ = (expr);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      set_error(std::string("split plan: ") + #expr + ": " + cudaGetErrorString(e_));  \
+      return DMRGX_E_CUDA;                                                             \
+    }                                                                                  \
+  } while (0)
+
+int64_t rup(int64_t x, int64_t p) { return (x + p - 1) / p * p; }
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// Tensor map of one padded block: dims (K elements, rows, hi|lo), box (one k-tile
+// row of 64 bytes, box_rows, 2), 64-byte swizzle.
+bool make_map(CUtensorMap* m, int eb, void* base, int64_t kp, int64_t rows, int64_t half_elems,
+              int box_rows, std::string& why) {
+  auto fn = encode_fn();
+  if (!fn) {
+    why = "cuTensorMapEncodeTiled is not available from the driver";
+    return false;
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)rows, 2};
+  const cuuint64_t strides[2] = {(cuuint64_t)(kp * eb), (cuuint64_t)(half_elems * eb)};
+  const cuuint32_t box[3] = {(cuuint32_t)(tc_ktile_bytes() / eb), (cuuint32_t)box_rows, 2};
+  const cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = fn(m, eb == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                  3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    why = "cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) + ")";
+    return false;
+  }
+  return true;
+}
+
+// Work units of one stage: tiles of 128 rows x <=256 columns; tiles longer than
+// `split_kt` k-tiles are cut along K into near-equal parts with workspace slots.
+void make_units(SplitStage& st, int num_sms) {
+  const int TM = tc_tile_m(), TN = tc_tile_n();
+  struct T { int out, tm, tn; int kt; };
+  std::vector<T> tiles;
+  int64_t total = 0;
+  for (size_t o = 0; o < st.outs.size(); o++) {
+    int kt = 0;
+    for (int s = 0; s < st.outs[o].seg_count; s++) kt += st.segs[st.outs[o].seg_begin + s].nkt;
+    const int tm = (st.outs[o].m + TM - 1) / TM, tn = (st.outs[o].n + TN - 1) / TN;
+    for (int a = 0; a < tm; a++)
+      for (int b = 0; b < tn; b++) {
+        tiles.push_back({(int)o, a, b, kt});
+        total += kt;
+      }
+  }
+  const int split_kt = (int)std::max<int64_t>(16, (total + num_sms - 1) / num_sms);
+  std::vector<std::pair<int, SUnit>> us;
+  st.reds.clear();
+  int slot = 0;
+  for (auto& t : tiles) {
+    const int parts = t.kt > split_kt ? (t.kt + split_kt - 1) / split_kt : 1;
+    if (parts > 1) {
+      SRed r;
+      r.out = t.out;
+      r.tm = (int16_t)t.tm;
+      r.tn = (int16_t)t.tn;
+      r.slot0 = slot;
+      r.nslots = parts;
+      st.reds.push_back(r);
+    }
+    for (int p = 0; p < parts; p++) {
+      SUnit u;
+      u.out = t.out;
+      u.tm = (int16_t)t.tm;
+      u.tn = (int16_t)t.tn;
+      u.kt0 = (int)((int64_t)t.kt * p / parts);
+      u.kt1 = (int)((int64_t)t.kt * (p + 1) / parts);
+      u.slot = parts > 1 ? slot++ : -1;
+      u.pad_ = 0;
+      us.push_back({u.kt1 - u.kt0, u});
+    }
+  }
+  std::stable_sort(us.begin(), us.end(), [](const std::pair<int, SUnit>& x,
+                                            const std::pair<int, SUnit>& y) {
+    return x.first > y.first;
+  });
+  st.units.clear();
+  for (auto& p : us) st.units.push_back(p.second);
+  st.nslots = slot;
+}
+
+template <class V, class P>
+int upload_vec(const std::vector<V>& v, P*& d, cudaStream_t s) {
+  cudaFree(d);
+  d = nullptr;
+  SP_TRY(cudaMalloc(&d, sizeof(V) * std::max<size_t>(1, v.size())));
+  if (!v.empty()) SP_TRY(cudaMemcpyAsync(d, v.data(), sizeof(V) * v.size(), cudaMemcpyHostToDevice, s));
+  return 0;
+}
+
+int upload(SplitStage& st, cudaStream_t s) {
+  int rc = upload_vec(st.outs, st.d_outs, s);
+  if (!rc) rc = upload_vec(st.segs, st.d_segs, s);
+  if (!rc) rc = upload_vec(st.units, st.d_units, s);
+  if (!rc) rc = upload_vec(st.reds, st.d_reds, s);
+  if (!rc) rc = upload_vec(st.maps, st.d_maps, s);
+  return rc;
+}
+
+int run_jobs(int eb, const double* src, void* hi, void* lo, const std::vector<PadJob>& jobs,
+             cudaStream_t s) {
+  if (jobs.empty()) return 0;
+  PadJob* d = nullptr;
+  SP_TRY(cudaMalloc(&d, sizeof(PadJob) * jobs.size()));
+  SP_TRY(cudaMemcpyAsync(d, jobs.data(), sizeof(PadJob) * jobs.size(), cudaMemcpyHostToDevice, s));
+  int64_t mx = 0;
+  for (auto& j : jobs) mx = std::max<int64_t>(mx, (int64_t)j.rows * j.groups * j.cols);
+  SP_TRY(launch_pad_split(eb, src, hi, lo, d, (int)jobs.size(), mx, s));
+  SP_TRY(cudaStreamSynchronize(s));
+  cudaFree(d);
+  return 0;
+}
+
+}  // namespace
+
+int build_split_plan(dmrgx_ctx* c, int eb) {
+  SplitPlan& sp = c->sp;
+  sp.free_device();
+  sp = SplitPlan();
+  if (c->dtype != DMRGX_F64) {
+    set_error("split precision is available for F64 contexts");
+    return DMRGX_E_ARG;
+  }
+  const int64_t P = 16 / eb;                     // padding granularity (elements)
+  const int64_t BK = tc_ktile_bytes() / eb;      // elements per k-tile row
+  const Stage& f1 = c->st1;
+  const Stage& f2 = c->st2;
+  struct MapReq { int which; int64_t off, kp, rows; int box_rows; };  // which: 0 a1,1 psi,2 a2,3 store
+  std::vector<MapReq> req1, req2;
+
+  // ---- stage 1 layout
+  std::map<int64_t, int> a1_map, psi_map;
+  std::map<int64_t, int64_t> st_off;
+  std::map<int64_t, std::pair<int, int>> st_shape;  // FP64 store offset -> (M1, N1)
+  std::vector<PadJob> a1_jobs;
+  int64_t a1_len = 0, psi_len = 0, st_len = 0;
+  for (size_t o = 0; o < f1.outs.size(); o++) {
+    const DOut& d = f1.outs[o];
+    SOut so;
+    if (st_off.find(d.c_off) == st_off.end()) {
+      st_off[d.c_off] = st_len;
+      st_shape[d.c_off] = {d.m, d.n};
+      st_len += (int64_t)d.m * rup(d.n, P);
+    }
+    so.c_off = st_off[d.c_off];
+    so.m = d.m;
+    so.n = d.n;
+    so.ldc = (int32_t)rup(d.n, P);
+    so.seg_begin = (int32_t)sp.s1.segs.size();
+    so.seg_count = d.seg_count;
+    so.pad_ = 0;
+    for (int s = 0; s < d.seg_count; s++) {
+      const DSeg& g = f1.segs[d.seg_begin + s];
+      const int64_t kp = rup(g.k, P);
+      SSeg2 ss;
+      auto ia = a1_map.find(g.a_off);
+      if (ia == a1_map.end()) {
+        a1_jobs.push_back(PadJob{g.a_off, a1_len, d.m, 1, g.k, (int32_t)kp});
+        a1_map[g.a_off] = (int)req1.size();
+        req1.push_back({0, a1_len, kp, d.m, 128});
+        a1_len += (int64_t)d.m * kp;
+      }
+      ss.amap = a1_map[g.a_off];
+      auto ib = psi_map.find(g.b_off);
+      if (ib == psi_map.end()) {
+        sp.psi_jobs.push_back(PadJob{g.b_off, psi_len, d.n, 1, g.k, (int32_t)kp});
+        psi_map[g.b_off] = (int)req1.size();
+        req1.push_back({1, psi_len, kp, d.n, (int)std::min<int64_t>(256, rup(d.n, 16))});
+        psi_len += (int64_t)d.n * kp;
+      }
+      ss.bmap = psi_map[g.b_off];
+      ss.nkt = (int32_t)((kp + BK - 1) / BK);
+      ss.brows = req1[ss.bmap].box_rows;
+      sp.s1.segs.push_back(ss);
+    }
+    sp.s1.outs.push_back(so);
+  }
+  sp.s1.full_cover = f1.full_cover;
+
+  // ---- stage 2 layout
+  std::map<int64_t, int> a2_map, stb_map;
+  std::vector<PadJob> a2_jobs;
+  int64_t a2_len = 0;
+  for (size_t o = 0; o < f2.outs.size(); o++) {
+    const DOut& d = f2.outs[o];
+    SOut so;
+    so.c_off = d.c_off;
+    so.m = d.m;
+    so.n = d.n;
+    so.ldc = d.n;
+    so.seg_begin = (int32_t)sp.s2.segs.size();
+    so.seg_count = d.seg_count;
+    so.pad_ = 0;
+    for (int s = 0; s < d.seg_count; s++) {
+      const DSeg& g = f2.segs[d.seg_begin + s];
+      auto is = st_shape.find(g.b_off);
+      if (is == st_shape.end()) {
+        set_error("split plan: a stage-2 task reads no stage-1 output block");
+        return DMRGX_E_ARG;
+      }
+      const int M1 = is->second.first, N1 = is->second.second;
+      if (g.k % N1 != 0 || (int64_t)(g.k / N1) * d.n != M1) {
+        set_error("split plan: stage-2 K does not factor as channels x stage-1 columns");
+        return DMRGX_E_ARG;
+      }
+      const int D = g.k / N1;
+      const int64_t n1p = rup(N1, P), kp = D * n1p;
+      SSeg2 ss;
+      auto ia = a2_map.find(g.a_off);
+      if (ia == a2_map.end()) {
+        a2_jobs.push_back(PadJob{g.a_off, a2_len, d.m, D, N1, (int32_t)n1p});
+        a2_map[g.a_off] = (int)req2.size();
+        req2.push_back({2, a2_len, kp, d.m, 128});
+        a2_len += (int64_t)d.m * kp;
+      }
+      ss.amap = a2_map[g.a_off];
+      auto ib = stb_map.find(g.b_off);
+      if (ib == stb_map.end()) {
+        stb_map[g.b_off] = (int)req2.size();
+        req2.push_back({3, st_off[g.b_off], kp, d.n, (int)std::min<int64_t>(256, rup(d.n, 16))});
+      }
+      ss.bmap = stb_map[g.b_off];
+      ss.nkt = (int32_t)((kp + BK - 1) / BK);
+      ss.brows = req2[ss.bmap].box_rows;
+      sp.s2.segs.push_back(ss);
+    }
+    sp.s2.outs.push_back(so);
+  }
+  sp.s2.full_cover = f2.full_cover;
+  make_units(sp.s1, c->num_sms);
+  make_units(sp.s2, c->num_sms);
+  // halves rounded to 256 bytes so hi and lo both start aligned
+  auto half = [eb](int64_t n) { return rup(std::max<int64_t>(n, 1), 256 / eb); };
+  sp.a1_len = half(a1_len);
+  sp.a2_len = half(a2_len);
+  sp.psi_len = half(psi_len);
+  sp.store_len = half(st_len);
+  for (auto& j : sp.psi_jobs)
+    sp.psi_max_job = std::max<int64_t>(sp.psi_max_job, (int64_t)j.rows * j.groups * j.cols);
+
+  // ---- device buffers and images
+  cudaStream_t s = c->stream;
+  SP_TRY(c->sa1.ensure(2 * sp.a1_len * eb));
+  SP_TRY(c->sa2.ensure(2 * sp.a2_len * eb));
+  SP_TRY(c->spsi.ensure(2 * sp.psi_len * eb));
+  SP_TRY(c->sstore.ensure(2 * sp.store_len * eb));
+  const int slots = std::max(1, std::max(sp.s1.nslots, sp.s2.nslots));
+  SP_TRY(c->sws.ensure((size_t)slots * tc_tile_m() * tc_tile_n() * sizeof(float)));
+  SP_TRY(c->err.ensure(16));
+  SP_TRY(cudaMemsetAsync(c->sa1.p, 0, 2 * sp.a1_len * eb, s));
+  SP_TRY(cudaMemsetAsync(c->sa2.p, 0, 2 * sp.a2_len * eb, s));
+  SP_TRY(cudaMemsetAsync(c->spsi.p, 0, 2 * sp.psi_len * eb, s));
+  SP_TRY(cudaMemsetAsync(c->sstore.p, 0, 2 * sp.store_len * eb, s));
+  SP_TRY(cudaMemsetAsync(c->err.p, 0, 16, s));
+  uint8_t* a1 = (uint8_t*)c->sa1.p;
+  uint8_t* a2 = (uint8_t*)c->sa2.p;
+  uint8_t* psi = (uint8_t*)c->spsi.p;
+  uint8_t* stb = (uint8_t*)c->sstore.p;
+  int rc = run_jobs(eb, (const double*)c->renv.p, a1, a1 + sp.a1_len * eb, a1_jobs, s);
+  if (rc) return rc;
+  rc = run_jobs(eb, (const double*)c->lenv.p, a2, a2 + sp.a2_len * eb, a2_jobs, s);
+  if (rc) return rc;
+  // ---- tensor maps
+  std::string why;
+  auto build_maps = [&](const std::vector<MapReq>& req, std::vector<CUtensorMap>& out) -> bool {
+    out.resize(req.size());
+    for (size_t i = 0; i < req.size(); i++) {
+      const MapReq& r = req[i];
+      uint8_t* base = r.which == 0 ? a1 : r.which == 1 ? psi : r.which == 2 ? a2 : stb;
+      const int64_t h = r.which == 0 ? sp.a1_len : r.which == 1 ? sp.psi_len
+                        : r.which == 2 ? sp.a2_len : sp.store_len;
+      if (!make_map(&out[i], eb, base + r.off * eb, r.kp, r.rows, h, r.box_rows, why))
+        return false;
+    }
+    return true;
+  };
+  if (!build_maps(req1, sp.s1.maps) || !build_maps(req2, sp.s2.maps)) {
+    set_error("split plan: " + why);
+    return DMRGX_E_CUDA;
+  }
+  rc = upload(sp.s1, s);
+  if (!rc) rc = upload(sp.s2, s);
+  if (rc) return rc;
+  if (!sp.psi_jobs.empty()) {
+    SP_TRY(cudaMalloc(&sp.d_psi_jobs, sizeof(PadJob) * sp.psi_jobs.size()));
+    SP_TRY(cudaMemcpyAsync(sp.d_psi_jobs, sp.psi_jobs.data(), sizeof(PadJob) * sp.psi_jobs.size(),
+                           cudaMemcpyHostToDevice, s));
+  }
+  SP_TRY(cudaStreamSynchronize(s));
+  sp.eb = eb;
+  return 0;
+}
+
+int run_matvec_split(dmrgx_ctx* c, const double* in, double* out) {
+  SplitPlan& sp = c->sp;
+  cudaStream_t s = c->stream;
+  const int eb = sp.eb;
+  uint8_t* psi = (uint8_t*)c->spsi.p;
+  uint8_t* stb = (uint8_t*)c->sstore.p;
+  c->prof_mark();
+  SP_TRY(launch_pad_split(eb, in, psi, psi + sp.psi_len * eb, sp.d_psi_jobs,
+                          (int)sp.psi_jobs.size(), sp.psi_max_job, s));
+  c->prof_mark();
+  SP_TRY(launch_tc_gemm(eb, true, sp.s1.d_maps, sp.s1.d_units, (int)sp.s1.units.size(),
+                        sp.s1.d_outs, sp.s1.d_segs, stb, stb + sp.store_len * eb, nullptr,
+                        (float*)c->sws.p, sp.s1.d_reds, (int)sp.s1.reds.size(), (int*)c->err.p,
+                        c->num_sms, s));
+  c->prof_mark();
+  if (!sp.s2.full_cover) SP_TRY(cudaMemsetAsync(out, 0, sizeof(double) * c->n, s));
+  SP_TRY(launch_tc_gemm(eb, false, sp.s2.d_maps, sp.s2.d_units, (int)sp.s2.units.size(),
+                        sp.s2.d_outs, sp.s2.d_segs, nullptr, nullptr, out, (float*)c->sws.p,
+                        sp.s2.d_reds, (int)sp.s2.reds.size(), (int*)c->err.p, c->num_sms, s));
+  c->prof_mark();
+  return 0;
+}
+
+}  // namespace dmrgx

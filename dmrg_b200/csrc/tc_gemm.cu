@@ -1,0 +1,470 @@
+// Split-precision grouped GEMM, warp-specialized: TMA -> tcgen05.mma (TMEM) -> epilogue.
+//
+// Each FP64 operand x is carried as a pair (hi, lo) of low-precision numbers,
+// hi = rn(x), lo = rn(x - hi), and every product a.b is evaluated as
+//     a_hi.b_hi + a_hi.b_lo + a_lo.b_hi          (the lo.lo term is dropped)
+// by three tcgen05.mma instructions accumulating into one FP32 TMEM accumulator.
+// Element types: BF16 pairs (kind::f16, K=16 per instruction) or TF32 pairs in
+// 32-bit containers (kind::tf32, K=8 per instruction).
+//
+// Operand blocks are row-major with K contiguous, rows padded to 16 bytes, the
+// lo array a fixed distance after the hi array.  One 3-D tensor map per block
+// (K, rows, hi|lo) with 64-byte swizzle brings a k-tile of 64 bytes per row for
+// both halves in one TMA instruction, straight into the UMMA canonical K-major
+// SW64 layout (8-row atoms of 512 B).  Rows and K past the block edge are
+// zero-filled by TMA.
+//
+// Roles (192 threads):
+//   warp 0      TMA producer: walks the work unit's k-tiles over its segments,
+//               fills a STAGES-deep smem ring (full/empty mbarrier pairs)
+//   warp 1      TMEM allocator and MMA issuer: 3 products x k-steps per k-tile,
+//               commits each k-tile to its ring slot's empty barrier and the
+//               last one of a unit to the accumulator's full barrier
+//   warps 2..5  epilogue: tcgen05.ld of the 128 accumulator rows (warp w reads
+//               TMEM lanes 32*(w%4)..), writes the unit's result
+// Two TMEM accumulators (2 x 256 columns) let the epilogue of one unit overlap
+// the MMAs of the next.
+//
+// Work unit = (output tile of 128 rows x <=256 columns, a range of its k-tiles).
+// Long tiles are split along K so every SM gets work; a split unit writes its
+// FP32 partial to a workspace slot and split_reduce sums the slots in a fixed
+// order (deterministic).  The MMA N of a unit is its tile's column count
+// rounded up to 16, chosen at run time in the instruction descriptor.
+//
+// Every wait is bounded: a timed-out wait sets the error word, the thread stops
+// its role, the CTA drains and frees its TMEM and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "split.h"
+
+namespace dmrgx {
+
+namespace {
+
+constexpr int THREADS = 192;
+constexpr int TM = 128;
+constexpr int TNMAX = 256;
+constexpr int STAGES = 4;
+constexpr int ROWB = 64;                      // bytes per row of one k-tile
+constexpr int A_BYTES = 2 * TM * ROWB;        // hi + lo: 16 KB
+constexpr int B_BYTES = 2 * TNMAX * ROWB;     // hi + lo: 32 KB
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int SBO = 8 * ROWB;                 // 512 B between 8-row atoms
+constexpr uint32_t TMEM_COLS = 512;           // two 256-column accumulators
+constexpr long long WAIT_LIMIT = 1ll << 23;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < WAIT_LIMIT; i++) {
+    if (mbar_try(bar, parity)) return true;
+    if (i > 32) __nanosleep(32);
+  }
+  return false;
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            int z, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t addr) {
+  // K-major, 64-byte swizzle: LBO unused (1), SBO = 512 B, version 1, layout 4
+  return (uint64_t)((addr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(SBO >> 4) << 32) |
+         (1ull << 46) | (4ull << 61);
+}
+template <int EB>
+__device__ __forceinline__ uint32_t instr_desc(int n) {
+  constexpr uint32_t fmt = EB == 2 ? 1u : 2u;  // BF16 (kind::f16) or TF32 (kind::tf32)
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(TM >> 4) << 24);
+}
+template <int EB>
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                    uint32_t accum) {
+  if (EB == 2)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accum)
+        : "memory");
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accum)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+      "%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+template <int EB>
+__device__ __forceinline__ void split_f32(float v, uint32_t& hi, uint32_t& lo) {
+  if (EB == 2) {
+    __nv_bfloat16 h = __float2bfloat16_rn(v);
+    __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+    hi = __bfloat16_as_ushort(h);
+    lo = __bfloat16_as_ushort(l);
+  } else {
+    hi = tf32_rna(v);
+    lo = tf32_rna(v - __uint_as_float(hi));
+  }
+}
+
+// Final store of 16 consecutive columns of one row (cols [col0, col0+16)).
+template <int EB, bool OUT_SPLIT>
+__device__ __forceinline__ void store16(const SOut& o, int row, int col0, const float* v,
+                                        uint8_t* c_hi, uint8_t* c_lo, double* c64) {
+  const int64_t rbase = o.c_off + (int64_t)row * o.ldc + col0;
+  if (OUT_SPLIT) {
+    constexpr int EPC = 16 / EB;
+#pragma unroll
+    for (int gq = 0; gq < 16 / EPC; gq++) {
+      if (col0 + gq * EPC >= o.ldc) break;
+      uint32_t hw[4], lw[4];
+      if (EB == 2) {
+#pragma unroll
+        for (int p = 0; p < 4; p++) {
+          uint32_t h0, l0, h1, l1;
+          split_f32<2>(v[gq * 8 + 2 * p], h0, l0);
+          split_f32<2>(v[gq * 8 + 2 * p + 1], h1, l1);
+          hw[p] = h0 | (h1 << 16);
+          lw[p] = l0 | (l1 << 16);
+        }
+      } else {
+#pragma unroll
+        for (int p = 0; p < 4; p++) split_f32<4>(v[gq * 4 + p], hw[p], lw[p]);
+      }
+      const int64_t eoff = (rbase + gq * EPC) * EB;
+      *reinterpret_cast<uint4*>(c_hi + eoff) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+      *reinterpret_cast<uint4*>(c_lo + eoff) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+      if (col0 + i < o.n) c64[rbase + i] = (double)v[i];
+  }
+}
+
+template <int EB, bool OUT_SPLIT>
+__global__ void __launch_bounds__(THREADS, 1)
+tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ units, int nunits,
+                const SOut* __restrict__ outs, const SSeg2* __restrict__ segs,
+                uint8_t* __restrict__ c_hi, uint8_t* __restrict__ c_lo, double* __restrict__ c64,
+                float* __restrict__ ws, int* __restrict__ err) {
+  extern __shared__ uint8_t smem_raw[];
+  // 1024-aligned ring (the swizzle pattern repeats every 512 B)
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* tfull = empty + STAGES;
+  uint64_t* tempty = tfull + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+
+  constexpr int BK = ROWB / EB;   // elements per k-tile row
+  constexpr int NKS = BK / (32 / EB);  // MMA k-steps (32 bytes each) per k-tile
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t sbase = smem_u32(smem);
+
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 1);
+    }
+    for (int a = 0; a < 2; a++) {
+      mbar_init(smem_u32(&tfull[a]), 1);
+      mbar_init(smem_u32(&tempty[a]), 4);  // one arrive per epilogue warp
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ TMA producer
+    if (lane == 0) {
+      uint32_t g = 0;
+      bool ok = true;
+      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+        const SUnit un = units[u];
+        const SOut o = outs[un.out];
+        // locate the unit's first k-tile
+        int s = o.seg_begin, base = 0;
+        while (s < o.seg_begin + o.seg_count && base + segs[s].nkt <= un.kt0) {
+          base += segs[s].nkt;
+          s++;
+        }
+        int kin = un.kt0 - base;
+        for (int kt = un.kt0; kt < un.kt1; kt++) {
+          const SSeg2 sg = segs[s];
+          const uint32_t slot = g % STAGES;
+          if (g >= STAGES) ok = mbar_wait(smem_u32(&empty[slot]), ((g / STAGES) - 1) & 1);
+          if (!ok) {
+            atomicExch(err, 2);
+            break;
+          }
+          const uint32_t st = sbase + slot * STAGE_BYTES;
+          const uint32_t bar = smem_u32(&full[slot]);
+          mbar_expect_tx(bar, (uint32_t)(A_BYTES + 2 * sg.brows * ROWB));
+          tma_load_3d(st, maps + sg.amap, kin * BK, un.tm * TM, 0, bar);
+          tma_load_3d(st + A_BYTES, maps + sg.bmap, kin * BK, un.tn * TNMAX, 0, bar);
+          g++;
+          if (++kin >= sg.nkt) {
+            kin = 0;
+            s++;
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      uint32_t g = 0, ua = 0;
+      bool ok = true;
+      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+        const SUnit un = units[u];
+        if (un.kt1 <= un.kt0) continue;
+        const SOut o = outs[un.out];
+        const int ncols = min(TNMAX, o.n - un.tn * TNMAX);
+        const int nmma = (ncols + 15) & ~15;
+        const uint32_t idesc = instr_desc<EB>(nmma);
+        const uint32_t acc = ua & 1;
+        if (ua >= 2) ok = mbar_wait(smem_u32(&tempty[acc]), ((ua / 2) - 1) & 1);
+        if (!ok) {
+          atomicExch(err, 3);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t tacc = tmem + acc * TNMAX;
+        int s = o.seg_begin, base = 0;
+        while (s < o.seg_begin + o.seg_count && base + segs[s].nkt <= un.kt0) {
+          base += segs[s].nkt;
+          s++;
+        }
+        int kin = un.kt0 - base;
+        for (int kt = un.kt0; kt < un.kt1; kt++) {
+          const SSeg2 sg = segs[s];
+          const uint32_t slot = g % STAGES;
+          ok = mbar_wait(smem_u32(&full[slot]), (g / STAGES) & 1);
+          if (!ok) {
+            atomicExch(err, 4);
+            break;
+          }
+          tc_fence_after();
+          const uint32_t st = sbase + slot * STAGE_BYTES;
+          const uint32_t a_hi = st, a_lo = st + TM * ROWB;
+          const uint32_t b_hi = st + A_BYTES, b_lo = st + A_BYTES + sg.brows * ROWB;
+#pragma unroll
+          for (int j = 0; j < NKS; j++) {
+            const uint32_t ko = j * 32;
+            const uint64_t ah = sw64_desc(a_hi + ko), al = sw64_desc(a_lo + ko);
+            const uint64_t bh = sw64_desc(b_hi + ko), bl = sw64_desc(b_lo + ko);
+            mma<EB>(tacc, ah, bh, idesc, (kt > un.kt0 || j > 0) ? 1u : 0u);
+            mma<EB>(tacc, ah, bl, idesc, 1u);
+            mma<EB>(tacc, al, bh, idesc, 1u);
+          }
+          mma_commit(smem_u32(&empty[slot]));
+          g++;
+          if (++kin >= sg.nkt) {
+            kin = 0;
+            s++;
+          }
+        }
+        if (!ok) break;
+        mma_commit(smem_u32(&tfull[acc]));
+        ua++;
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue (warps 2..5)
+    const int q = warp & 3;              // TMEM lane quarter this warp may access
+    const int row = q * 32 + lane;
+    uint32_t ua = 0;
+    bool ok = true;
+    for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+      const SUnit un = units[u];
+      const SOut o = outs[un.out];
+      const int ncols = min(TNMAX, o.n - un.tn * TNMAX);
+      const int nmma = (ncols + 15) & ~15;
+      const int m0 = un.tm * TM, n0 = un.tn * TNMAX;
+      const bool has = un.kt1 > un.kt0;
+      const uint32_t acc = ua & 1;
+      if (has) {
+        ok = mbar_wait(smem_u32(&tfull[acc]), (ua / 2) & 1);
+        if (!ok) {
+          atomicExch(err, 5);
+          break;
+        }
+        tc_fence_after();
+      }
+      const uint32_t taddr = tmem + acc * TNMAX + ((uint32_t)(q * 32) << 16);
+      for (int cc = 0; cc < nmma; cc += 16) {
+        float v[16];
+        if (has) {
+          tmem_ld16(taddr + cc, v);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; i++) v[i] = 0.f;
+        }
+        if (m0 + row >= o.m) continue;
+        if (un.slot >= 0) {
+          float* p = ws + ((int64_t)un.slot * TM + row) * TNMAX + cc;
+#pragma unroll
+          for (int i = 0; i < 16; i += 4)
+            *reinterpret_cast<float4*>(p + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+        } else {
+          store16<EB, OUT_SPLIT>(o, m0 + row, n0 + cc, v, c_hi, c_lo, c64);
+        }
+      }
+      if (has) {
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&tempty[acc]));
+        ua++;
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                 "r"(TMEM_COLS)
+                 : "memory");
+}
+
+// Sum the K-split partials of one output tile in slot order and store them.
+template <int EB, bool OUT_SPLIT>
+__global__ void split_reduce(const SRed* __restrict__ reds, const SOut* __restrict__ outs,
+                             const float* __restrict__ ws, uint8_t* __restrict__ c_hi,
+                             uint8_t* __restrict__ c_lo, double* __restrict__ c64) {
+  const SRed rd = reds[blockIdx.x];
+  const SOut o = outs[rd.out];
+  const int m0 = rd.tm * TM, n0 = rd.tn * TNMAX;
+  const int rows = min(TM, o.m - m0);
+  const int ncols = min(TNMAX, o.n - n0);
+  const int nmma = (ncols + 15) & ~15;
+  const int groups = nmma / 16;
+  for (int e = threadIdx.x; e < rows * groups; e += blockDim.x) {
+    const int r = e / groups, cc = (e - r * groups) * 16;
+    float v[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = 0.f;
+    for (int s = 0; s < rd.nslots; s++) {
+      const float* p = ws + ((int64_t)(rd.slot0 + s) * TM + r) * TNMAX + cc;
+#pragma unroll
+      for (int i = 0; i < 16; i += 4) {
+        const float4 t = *reinterpret_cast<const float4*>(p + i);
+        v[i] += t.x;
+        v[i + 1] += t.y;
+        v[i + 2] += t.z;
+        v[i + 3] += t.w;
+      }
+    }
+    store16<EB, OUT_SPLIT>(o, m0 + r, n0 + cc, v, c_hi, c_lo, c64);
+  }
+}
+
+}  // namespace
+
+int tc_smem_bytes() { return STAGES * STAGE_BYTES + 1024 + (2 * STAGES + 4) * 8 + 16; }
+int tc_tile_m() { return TM; }
+int tc_tile_n() { return TNMAX; }
+int tc_ktile_bytes() { return ROWB; }
+
+cudaError_t launch_tc_gemm(int eb, bool out_split, const CUtensorMap* maps, const SUnit* units,
+                           int nunits, const SOut* outs, const SSeg2* segs, void* c_hi, void* c_lo,
+                           double* c64, float* ws, const SRed* reds, int nreds, int* err, int grid,
+                           cudaStream_t st) {
+  if (nunits <= 0) return cudaSuccess;
+  if (grid > nunits) grid = nunits;
+  const int sm = tc_smem_bytes();
+#define DMRGX_TC_LAUNCH(EB, OS)                                                               \
+  do {                                                                                        \
+    cudaError_t e = cudaFuncSetAttribute(tc_grouped_gemm<EB, OS>,                             \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, sm);    \
+    if (e != cudaSuccess) return e;                                                           \
+    tc_grouped_gemm<EB, OS><<<grid, THREADS, sm, st>>>(maps, units, nunits, outs, segs,       \
+                                                      (uint8_t*)c_hi, (uint8_t*)c_lo, c64, ws, \
+                                                      err);                                   \
+    if (nreds > 0)                                                                            \
+      split_reduce<EB, OS><<<nreds, 256, 0, st>>>(reds, outs, ws, (uint8_t*)c_hi,             \
+                                                 (uint8_t*)c_lo, c64);                        \
+  } while (0)
+  if (eb == 2) {
+    if (out_split) DMRGX_TC_LAUNCH(2, true);
+    else DMRGX_TC_LAUNCH(2, false);
+  } else {
+    if (out_split) DMRGX_TC_LAUNCH(4, true);
+    else DMRGX_TC_LAUNCH(4, false);
+  }
+#undef DMRGX_TC_LAUNCH
+  return cudaGetLastError();
+}
+
+}  // namespace dmrgx

@@ -37,6 +37,8 @@ SIGNATURES = {
     "dmrgx_av": (_i, [_vp, _vp, _vp, _i]),
     "dmrgx_av_noalloc": (_i, [_i, _i64, _i64, _ip, _i, _vp, _i64p, _i, _ip, _i, _vp, _i64p, _i,
                               _vp, _vp, _vp]),
+    "dmrgx_profile": (_i, [_vp, _i]),
+    "dmrgx_profile_read": (_i, [_vp, _dp, _i]),
     "dmrgx_stream": (_vp, [_vp]),
     "dmrgx_sync": (_i, [_vp]),
 }
@@ -178,6 +180,15 @@ class Context:
     def av_device(self, x_ptr: int, y_ptr: int):
         """Device pointers (e.g. torch tensors' data_ptr()) on this context's stream."""
         _check(lib().dmrgx_av(self.ptr, C.c_void_p(x_ptr), C.c_void_p(y_ptr), MEM_DEVICE))
+
+    def profile(self, enable: bool):
+        _check(lib().dmrgx_profile(self.ptr, 1 if enable else 0))
+
+    def profile_read(self):
+        """(matvecs, ms per slot [split, stage 1, stage 2]) since profile(True)."""
+        out = np.zeros(4)
+        _check(lib().dmrgx_profile_read(self.ptr, out.ctypes.data_as(_dp), 4))
+        return int(out[0]), out[1:4].copy()
 
     def stream(self) -> int:
         return int(lib().dmrgx_stream(self.ptr) or 0)

@@ -143,6 +143,15 @@ int dmrgx_av_noalloc(int dtype, int64_t n, int64_t d_store, const int* rmap, int
                      const int* lmap, int n_lmap, const void* lenv, const int64_t* lenv_sizes,
                      int n_lenv_blocks, const void* in, void* out, void* stream);
 
+/* Per-launch device timing of the matvec, for roofline measurements: CUDA
+ * events recorded on the context's stream around each launch of every matvec
+ * while enabled (enable=1 clears the totals and starts, 0 stops).
+ * dmrgx_profile_read synchronises the stream and fills out[0] = matvecs timed,
+ * out[1..3] = summed milliseconds of the launch slots [operand split (split
+ * precision only), stage 1, stage 2].  cap >= 4. */
+int dmrgx_profile(dmrgx_ctx* ctx, int enable);
+int dmrgx_profile_read(dmrgx_ctx* ctx, double* out, int cap);
+
 /* The context's CUDA stream (a cudaStream_t), for callers that order their own
  * device work with dmrgx_av(..., DMRGX_MEM_DEVICE). */
 void* dmrgx_stream(dmrgx_ctx* ctx);
