@@ -273,6 +273,13 @@ int finalize_plan(dmrgx_ctx* c, const double* renv_vals, const std::vector<int64
   return 0;
 }
 
+int run_matvec_fp64(dmrgx_ctx* c, const double* in, double* out);
+
+int run_matvec(dmrgx_ctx* c, const double* in, double* out) {
+  if (c->prec != DMRGX_PREC_FP64) return run_matvec_split(c, in, out);
+  return run_matvec_fp64(c, in, out);
+}
+
 // error word of the bounded device waits (split path); 0 = fine
 int check_device_error(dmrgx_ctx* c) {
   if (!c->err.p) return 0;
@@ -287,8 +294,7 @@ int check_device_error(dmrgx_ctx* c) {
   return 0;
 }
 
-int run_matvec(dmrgx_ctx* c, const double* in, double* out) {
-  if (c->prec != DMRGX_PREC_FP64) return run_matvec_split(c, in, out);
+int run_matvec_fp64(dmrgx_ctx* c, const double* in, double* out) {
   const bool cplx = c->dtype == DMRGX_C128;
   c->prof_mark();
   c->prof_mark();
@@ -310,6 +316,13 @@ int run_matvec(dmrgx_ctx* c, const double* in, double* out) {
 }
 
 }  // namespace
+
+namespace dmrgx {
+// the context's matvec (fp64=false) or its FP64 form regardless of precision
+int run_matvec_any(dmrgx_ctx* c, const double* in, double* out, bool fp64) {
+  return fp64 ? run_matvec_fp64(c, in, out) : run_matvec(c, in, out);
+}
+}  // namespace dmrgx
 
 extern "C" {
 

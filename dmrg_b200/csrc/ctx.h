@@ -39,13 +39,17 @@ struct DevBuf {
 struct SplitStage {
   std::vector<SOut> outs;
   std::vector<SSeg2> segs;
-  std::vector<SUnit> units;
+  std::vector<SUnit> units;      // grouped by CTA
+  std::vector<int> cta_begin;    // CTA c runs units [cta_begin[c], cta_begin[c+1])
   std::vector<SRed> reds;
+  std::vector<SRedBlk> redblk;
   std::vector<CUtensorMap> maps;
   SOut* d_outs = nullptr;
   SSeg2* d_segs = nullptr;
   SUnit* d_units = nullptr;
+  int* d_cta_begin = nullptr;
   SRed* d_reds = nullptr;
+  SRedBlk* d_redblk = nullptr;
   CUtensorMap* d_maps = nullptr;
   int nslots = 0;
   bool full_cover = true;
@@ -59,8 +63,9 @@ struct SplitPlan {
   SplitStage s1, s2;
   int64_t a1_len = 0, a2_len = 0, psi_len = 0, store_len = 0;   // elements per half
   std::vector<PadJob> psi_jobs;    // per-matvec FP64 psi -> (hi, lo)
+  std::vector<PadRow> psi_rows;
   PadJob* d_psi_jobs = nullptr;
-  int64_t psi_max_job = 0;
+  PadRow* d_psi_rows = nullptr;
   void free_device();
 };
 

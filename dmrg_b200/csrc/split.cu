@@ -23,31 +23,35 @@ __device__ __forceinline__ uint32_t tf32_rna(float x) {
   return r;
 }
 
-// FP64 blocks -> (hi, lo) pairs with padded rows.  Element (r, grp, j) of a job
-// goes to dst + r*groups*colsp + grp*colsp + j; padding is left untouched (zero).
+// FP64 rows -> (hi, lo) pairs with padded rows.  Block b converts row
+// rows[b].row of job rows[b].job: element (grp, j) of the source row goes to
+// dst + row*groups*colsp + grp*colsp + j.
 template <int EB>
 __global__ void pad_split_kernel(const double* __restrict__ src, uint8_t* __restrict__ hi,
-                                 uint8_t* __restrict__ lo, const PadJob* __restrict__ jobs) {
-  const PadJob jb = jobs[blockIdx.y];
-  const int64_t total = (int64_t)jb.rows * jb.groups * jb.cols;
+                                 uint8_t* __restrict__ lo, const PadJob* __restrict__ jobs,
+                                 const PadRow* __restrict__ rows) {
+  const PadRow pr = rows[blockIdx.x];
+  const PadJob jb = jobs[pr.job];
   const int gc = jb.groups * jb.cols;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = e / gc;
-    const int rem = (int)(e - r * gc);
-    const int grp = rem / jb.cols, j = rem - grp * jb.cols;
-    const double x = src[jb.src + e];
-    const int64_t d = jb.dst + r * (int64_t)jb.groups * jb.colsp + (int64_t)grp * jb.colsp + j;
-    if (EB == 2) {
-      __nv_bfloat16 h = __double2bfloat16(x);
-      __nv_bfloat16 l = __double2bfloat16(x - (double)__bfloat162float(h));
-      reinterpret_cast<__nv_bfloat16*>(hi)[d] = h;
-      reinterpret_cast<__nv_bfloat16*>(lo)[d] = l;
-    } else {
-      const uint32_t h = tf32_rna((float)x);
-      const uint32_t l = tf32_rna((float)(x - (double)__uint_as_float(h)));
-      reinterpret_cast<uint32_t*>(hi)[d] = h;
-      reinterpret_cast<uint32_t*>(lo)[d] = l;
+  const double* s = src + jb.src + (int64_t)pr.row * gc;
+  const int64_t d0 = jb.dst + (int64_t)pr.row * jb.groups * jb.colsp;
+  for (int grp = 0; grp < jb.groups; grp++) {
+    const int64_t d = d0 + (int64_t)grp * jb.colsp;
+    for (int j = threadIdx.x; j < jb.cols; j += blockDim.x) {
+      const double x = s[grp * jb.cols + j];
+      if (EB == 2) {
+        // hi from the FP32 rounding of x (any nearby BF16 value will do: lo
+        // takes the exact FP64 remainder)
+        __nv_bfloat16 h = __float2bfloat16_rn((float)x);
+        __nv_bfloat16 l = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
+        reinterpret_cast<__nv_bfloat16*>(hi)[d + j] = h;
+        reinterpret_cast<__nv_bfloat16*>(lo)[d + j] = l;
+      } else {
+        const uint32_t h = tf32_rna((float)x);
+        const uint32_t l = tf32_rna((float)(x - (double)__uint_as_float(h)));
+        reinterpret_cast<uint32_t*>(hi)[d + j] = h;
+        reinterpret_cast<uint32_t*>(lo)[d + j] = l;
+      }
     }
   }
 }
@@ -55,16 +59,13 @@ __global__ void pad_split_kernel(const double* __restrict__ src, uint8_t* __rest
 }  // namespace
 
 cudaError_t launch_pad_split(int eb, const double* src, void* hi, void* lo, const PadJob* jobs,
-                             int njobs, int64_t max_elems, cudaStream_t st) {
-  if (njobs <= 0) return cudaSuccess;
-  int bx = (int)std::min<int64_t>(64, (max_elems + 255) / 256);
-  if (bx < 1) bx = 1;
-  for (int j0 = 0; j0 < njobs; j0 += 65535) {
-    dim3 grid(bx, std::min(65535, njobs - j0));
+                             const PadRow* rows, int nrows, cudaStream_t st) {
+  for (int r0 = 0; r0 < nrows; r0 += 1 << 30) {
+    const int n = std::min(nrows - r0, 1 << 30);
     if (eb == 2)
-      pad_split_kernel<2><<<grid, 256, 0, st>>>(src, (uint8_t*)hi, (uint8_t*)lo, jobs + j0);
+      pad_split_kernel<2><<<n, 128, 0, st>>>(src, (uint8_t*)hi, (uint8_t*)lo, jobs, rows + r0);
     else
-      pad_split_kernel<4><<<grid, 256, 0, st>>>(src, (uint8_t*)hi, (uint8_t*)lo, jobs + j0);
+      pad_split_kernel<4><<<n, 128, 0, st>>>(src, (uint8_t*)hi, (uint8_t*)lo, jobs, rows + r0);
   }
   return cudaGetLastError();
 }

@@ -18,7 +18,7 @@ struct SOut {
   int32_t m, n;      // rows, columns
   int32_t ldc;       // row stride of C (>= n)
   int32_t seg_begin, seg_count;
-  int32_t pad_;
+  int32_t tnw;       // tile width (columns per tile, <= 256, a multiple of 16)
 };
 
 // One segment of an output block: tensor-map indices of its A block (m x kp) and
@@ -46,6 +46,16 @@ struct SRed {
   int32_t slot0, nslots;
 };
 
+// One block of the reduction launch: rows [r0, r0+rows) of K-split tile `red`.
+struct SRedBlk {
+  int32_t red, r0;
+};
+
+// One block of the conversion launch: row `row` of conversion job `job`.
+struct PadRow {
+  int32_t job, row;
+};
+
 // FP64 -> (hi, lo) conversion job: rows x (groups x cols) source elements,
 // destination rows of groups x colsp elements (colsp >= cols, zero padding).
 struct PadJob {
@@ -58,14 +68,17 @@ int tc_tile_m();
 int tc_tile_n();
 int tc_ktile_bytes();
 
+// Convert the rows listed in `rows` (one thread block each).
 cudaError_t launch_pad_split(int eb, const double* src, void* hi, void* lo, const PadJob* jobs,
-                             int njobs, int64_t max_elems, cudaStream_t st);
+                             const PadRow* rows, int nrows, cudaStream_t st);
 
 // One stage: the warp-specialized TMA/tcgen05 kernel over `units`, then the
 // reduction of K-split tiles (if any).
+// One stage: the warp-specialized TMA/tcgen05 kernel, CTA c running units
+// [cta_begin[c], cta_begin[c+1]) in order, then the reduction of K-split tiles.
 cudaError_t launch_tc_gemm(int eb, bool out_split, const CUtensorMap* maps, const SUnit* units,
-                           int nunits, const SOut* outs, const SSeg2* segs, void* c_hi, void* c_lo,
-                           double* c64, float* ws, const SRed* reds, int nreds, int* err, int grid,
-                           cudaStream_t st);
+                           const int* cta_begin, int nctas, const SOut* outs, const SSeg2* segs,
+                           void* c_hi, void* c_lo, double* c64, float* ws, const SRed* reds,
+                           const SRedBlk* redblk, int nredblk, int* err, cudaStream_t st);
 
 }  // namespace dmrgx

@@ -16,6 +16,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cmath>
 #include <map>
 #include <string>
 
@@ -29,12 +30,16 @@ void SplitStage::free_device() {
   cudaFree(d_outs);
   cudaFree(d_segs);
   cudaFree(d_units);
+  cudaFree(d_cta_begin);
   cudaFree(d_reds);
+  cudaFree(d_redblk);
   cudaFree(d_maps);
   d_outs = nullptr;
   d_segs = nullptr;
   d_units = nullptr;
+  d_cta_begin = nullptr;
   d_reds = nullptr;
+  d_redblk = nullptr;
   d_maps = nullptr;
 }
 
@@ -42,7 +47,9 @@ void SplitPlan::free_device() {
   s1.free_device();
   s2.free_device();
   cudaFree(d_psi_jobs);
+  cudaFree(d_psi_rows);
   d_psi_jobs = nullptr;
+  d_psi_rows = nullptr;
 }
 
 namespace {
@@ -95,29 +102,52 @@ bool make_map(CUtensorMap* m, int eb, void* base, int64_t kp, int64_t rows, int6
   return true;
 }
 
-// Work units of one stage: tiles of 128 rows x <=256 columns; tiles longer than
-// `split_kt` k-tiles are cut along K into near-equal parts with workspace slots.
+// Tile width (columns of one work unit) of an output block with n columns.
+// Stage 1 halves wide blocks (more, smaller units, no partial sums); stage 2
+// keeps them whole and splits long K instead.
+int tile_width(int n, bool halve_wide) {
+  const int full = (int)std::min<int64_t>(256, rup(n, 16));
+  if (halve_wide && n > 128) return (int)rup((n + 1) / 2, 16);
+  return full;
+}
+
+// Work units of one stage and their assignment to CTAs.
+// Cost of a unit (SM clock cycles, rough): the larger of its MMA issue time
+// (6 MMAs of N/2 cycles per k-tile) and its operand bytes at ~48 B/cycle, plus a
+// fixed 800.  Tiles costlier than half the mean CTA load are cut along K
+// (partials + fixed-order reduction).  Units go to CTAs longest-first onto the
+// least-loaded CTA.
 void make_units(SplitStage& st, int num_sms) {
-  const int TM = tc_tile_m(), TN = tc_tile_n();
-  struct T { int out, tm, tn; int kt; };
+  const int TM = tc_tile_m();
+  const int A_B = 2 * TM * tc_ktile_bytes();
+  struct T { int out, tm, tn, kt; double per_kt; };
   std::vector<T> tiles;
-  int64_t total = 0;
+  double total = 0;
   for (size_t o = 0; o < st.outs.size(); o++) {
+    const SOut& so = st.outs[o];
     int kt = 0;
-    for (int s = 0; s < st.outs[o].seg_count; s++) kt += st.segs[st.outs[o].seg_begin + s].nkt;
-    const int tm = (st.outs[o].m + TM - 1) / TM, tn = (st.outs[o].n + TN - 1) / TN;
+    for (int s = 0; s < so.seg_count; s++) kt += st.segs[so.seg_begin + s].nkt;
+    const int brows = so.seg_count ? st.segs[so.seg_begin].brows : so.tnw;
+    const int tm = (so.m + TM - 1) / TM, tn = (so.n + so.tnw - 1) / so.tnw;
     for (int a = 0; a < tm; a++)
       for (int b = 0; b < tn; b++) {
-        tiles.push_back({(int)o, a, b, kt});
-        total += kt;
+        const int ncols = std::min(so.tnw, so.n - b * so.tnw);
+        const int nmma = (int)rup(ncols, 16);
+        const double per = std::max(3.0 * nmma, (A_B + 2.0 * brows * tc_ktile_bytes()) / 48.0);
+        tiles.push_back({(int)o, a, b, kt, per});
+        total += kt * per + 800;
       }
   }
-  const int split_kt = (int)std::max<int64_t>(16, (total + num_sms - 1) / num_sms);
-  std::vector<std::pair<int, SUnit>> us;
+  const double cap = std::max(4000.0, 0.5 * total / std::max(1, num_sms));
+  struct U { double cost; SUnit u; };
+  std::vector<U> us;
   st.reds.clear();
+  st.redblk.clear();
   int slot = 0;
   for (auto& t : tiles) {
-    const int parts = t.kt > split_kt ? (t.kt + split_kt - 1) / split_kt : 1;
+    const double c = t.kt * t.per_kt;
+    int parts = 1;
+    if (c > cap && t.kt > 1) parts = (int)std::min<double>(t.kt, std::ceil(c / cap));
     if (parts > 1) {
       SRed r;
       r.out = t.out;
@@ -125,6 +155,8 @@ void make_units(SplitStage& st, int num_sms) {
       r.tn = (int16_t)t.tn;
       r.slot0 = slot;
       r.nslots = parts;
+      const int rows = std::min(TM, st.outs[t.out].m - t.tm * TM);
+      for (int r0 = 0; r0 < rows; r0 += 4) st.redblk.push_back(SRedBlk{(int)st.reds.size(), r0});
       st.reds.push_back(r);
     }
     for (int p = 0; p < parts; p++) {
@@ -136,15 +168,26 @@ void make_units(SplitStage& st, int num_sms) {
       u.kt1 = (int)((int64_t)t.kt * (p + 1) / parts);
       u.slot = parts > 1 ? slot++ : -1;
       u.pad_ = 0;
-      us.push_back({u.kt1 - u.kt0, u});
+      us.push_back({(u.kt1 - u.kt0) * t.per_kt + 800, u});
     }
   }
-  std::stable_sort(us.begin(), us.end(), [](const std::pair<int, SUnit>& x,
-                                            const std::pair<int, SUnit>& y) {
-    return x.first > y.first;
-  });
+  std::stable_sort(us.begin(), us.end(), [](const U& x, const U& y) { return x.cost > y.cost; });
+  const int nctas = (int)std::min<size_t>(num_sms, us.size());
+  std::vector<std::vector<SUnit>> per(nctas);
+  std::vector<double> load(nctas, 0.0);
+  for (auto& x : us) {
+    int best = 0;
+    for (int c = 1; c < nctas; c++)
+      if (load[c] < load[best]) best = c;
+    load[best] += x.cost;
+    per[best].push_back(x.u);
+  }
   st.units.clear();
-  for (auto& p : us) st.units.push_back(p.second);
+  st.cta_begin.assign(1, 0);
+  for (int c = 0; c < nctas; c++) {
+    st.units.insert(st.units.end(), per[c].begin(), per[c].end());
+    st.cta_begin.push_back((int)st.units.size());
+  }
   st.nslots = slot;
 }
 
@@ -161,22 +204,35 @@ int upload(SplitStage& st, cudaStream_t s) {
   int rc = upload_vec(st.outs, st.d_outs, s);
   if (!rc) rc = upload_vec(st.segs, st.d_segs, s);
   if (!rc) rc = upload_vec(st.units, st.d_units, s);
+  if (!rc) rc = upload_vec(st.cta_begin, st.d_cta_begin, s);
   if (!rc) rc = upload_vec(st.reds, st.d_reds, s);
+  if (!rc) rc = upload_vec(st.redblk, st.d_redblk, s);
   if (!rc) rc = upload_vec(st.maps, st.d_maps, s);
   return rc;
+}
+
+std::vector<PadRow> rows_of(const std::vector<PadJob>& jobs) {
+  std::vector<PadRow> r;
+  for (size_t j = 0; j < jobs.size(); j++)
+    for (int i = 0; i < jobs[j].rows; i++) r.push_back(PadRow{(int)j, i});
+  return r;
 }
 
 int run_jobs(int eb, const double* src, void* hi, void* lo, const std::vector<PadJob>& jobs,
              cudaStream_t s) {
   if (jobs.empty()) return 0;
   PadJob* d = nullptr;
+  PadRow* dr = nullptr;
+  const std::vector<PadRow> rows = rows_of(jobs);
   SP_TRY(cudaMalloc(&d, sizeof(PadJob) * jobs.size()));
+  SP_TRY(cudaMalloc(&dr, sizeof(PadRow) * std::max<size_t>(1, rows.size())));
   SP_TRY(cudaMemcpyAsync(d, jobs.data(), sizeof(PadJob) * jobs.size(), cudaMemcpyHostToDevice, s));
-  int64_t mx = 0;
-  for (auto& j : jobs) mx = std::max<int64_t>(mx, (int64_t)j.rows * j.groups * j.cols);
-  SP_TRY(launch_pad_split(eb, src, hi, lo, d, (int)jobs.size(), mx, s));
+  if (!rows.empty())
+    SP_TRY(cudaMemcpyAsync(dr, rows.data(), sizeof(PadRow) * rows.size(), cudaMemcpyHostToDevice, s));
+  SP_TRY(launch_pad_split(eb, src, hi, lo, d, dr, (int)rows.size(), s));
   SP_TRY(cudaStreamSynchronize(s));
   cudaFree(d);
+  cudaFree(dr);
   return 0;
 }
 
@@ -217,7 +273,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
     so.ldc = (int32_t)rup(d.n, P);
     so.seg_begin = (int32_t)sp.s1.segs.size();
     so.seg_count = d.seg_count;
-    so.pad_ = 0;
+    so.tnw = tile_width(d.n, true);
     for (int s = 0; s < d.seg_count; s++) {
       const DSeg& g = f1.segs[d.seg_begin + s];
       const int64_t kp = rup(g.k, P);
@@ -234,7 +290,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
       if (ib == psi_map.end()) {
         sp.psi_jobs.push_back(PadJob{g.b_off, psi_len, d.n, 1, g.k, (int32_t)kp});
         psi_map[g.b_off] = (int)req1.size();
-        req1.push_back({1, psi_len, kp, d.n, (int)std::min<int64_t>(256, rup(d.n, 16))});
+        req1.push_back({1, psi_len, kp, d.n, tile_width(d.n, true)});
         psi_len += (int64_t)d.n * kp;
       }
       ss.bmap = psi_map[g.b_off];
@@ -259,7 +315,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
     so.ldc = d.n;
     so.seg_begin = (int32_t)sp.s2.segs.size();
     so.seg_count = d.seg_count;
-    so.pad_ = 0;
+    so.tnw = tile_width(d.n, false);
     for (int s = 0; s < d.seg_count; s++) {
       const DSeg& g = f2.segs[d.seg_begin + s];
       auto is = st_shape.find(g.b_off);
@@ -286,7 +342,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
       auto ib = stb_map.find(g.b_off);
       if (ib == stb_map.end()) {
         stb_map[g.b_off] = (int)req2.size();
-        req2.push_back({3, st_off[g.b_off], kp, d.n, (int)std::min<int64_t>(256, rup(d.n, 16))});
+        req2.push_back({3, st_off[g.b_off], kp, d.n, tile_width(d.n, false)});
       }
       ss.bmap = stb_map[g.b_off];
       ss.nkt = (int32_t)((kp + BK - 1) / BK);
@@ -304,8 +360,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
   sp.a2_len = half(a2_len);
   sp.psi_len = half(psi_len);
   sp.store_len = half(st_len);
-  for (auto& j : sp.psi_jobs)
-    sp.psi_max_job = std::max<int64_t>(sp.psi_max_job, (int64_t)j.rows * j.groups * j.cols);
+  sp.psi_rows = rows_of(sp.psi_jobs);
 
   // ---- device buffers and images
   cudaStream_t s = c->stream;
@@ -350,11 +405,9 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
   rc = upload(sp.s1, s);
   if (!rc) rc = upload(sp.s2, s);
   if (rc) return rc;
-  if (!sp.psi_jobs.empty()) {
-    SP_TRY(cudaMalloc(&sp.d_psi_jobs, sizeof(PadJob) * sp.psi_jobs.size()));
-    SP_TRY(cudaMemcpyAsync(sp.d_psi_jobs, sp.psi_jobs.data(), sizeof(PadJob) * sp.psi_jobs.size(),
-                           cudaMemcpyHostToDevice, s));
-  }
+  rc = upload_vec(sp.psi_jobs, sp.d_psi_jobs, s);
+  if (!rc) rc = upload_vec(sp.psi_rows, sp.d_psi_rows, s);
+  if (rc) return rc;
   SP_TRY(cudaStreamSynchronize(s));
   sp.eb = eb;
   return 0;
@@ -367,18 +420,19 @@ int run_matvec_split(dmrgx_ctx* c, const double* in, double* out) {
   uint8_t* psi = (uint8_t*)c->spsi.p;
   uint8_t* stb = (uint8_t*)c->sstore.p;
   c->prof_mark();
-  SP_TRY(launch_pad_split(eb, in, psi, psi + sp.psi_len * eb, sp.d_psi_jobs,
-                          (int)sp.psi_jobs.size(), sp.psi_max_job, s));
+  SP_TRY(launch_pad_split(eb, in, psi, psi + sp.psi_len * eb, sp.d_psi_jobs, sp.d_psi_rows,
+                          (int)sp.psi_rows.size(), s));
   c->prof_mark();
-  SP_TRY(launch_tc_gemm(eb, true, sp.s1.d_maps, sp.s1.d_units, (int)sp.s1.units.size(),
-                        sp.s1.d_outs, sp.s1.d_segs, stb, stb + sp.store_len * eb, nullptr,
-                        (float*)c->sws.p, sp.s1.d_reds, (int)sp.s1.reds.size(), (int*)c->err.p,
-                        c->num_sms, s));
+  SP_TRY(launch_tc_gemm(eb, true, sp.s1.d_maps, sp.s1.d_units, sp.s1.d_cta_begin,
+                        (int)sp.s1.cta_begin.size() - 1, sp.s1.d_outs, sp.s1.d_segs, stb,
+                        stb + sp.store_len * eb, nullptr, (float*)c->sws.p, sp.s1.d_reds,
+                        sp.s1.d_redblk, (int)sp.s1.redblk.size(), (int*)c->err.p, s));
   c->prof_mark();
   if (!sp.s2.full_cover) SP_TRY(cudaMemsetAsync(out, 0, sizeof(double) * c->n, s));
-  SP_TRY(launch_tc_gemm(eb, false, sp.s2.d_maps, sp.s2.d_units, (int)sp.s2.units.size(),
-                        sp.s2.d_outs, sp.s2.d_segs, nullptr, nullptr, out, (float*)c->sws.p,
-                        sp.s2.d_reds, (int)sp.s2.reds.size(), (int*)c->err.p, c->num_sms, s));
+  SP_TRY(launch_tc_gemm(eb, false, sp.s2.d_maps, sp.s2.d_units, sp.s2.d_cta_begin,
+                        (int)sp.s2.cta_begin.size() - 1, sp.s2.d_outs, sp.s2.d_segs, nullptr,
+                        nullptr, out, (float*)c->sws.p, sp.s2.d_reds, sp.s2.d_redblk,
+                        (int)sp.s2.redblk.size(), (int*)c->err.p, s));
   c->prof_mark();
   return 0;
 }

@@ -56,7 +56,7 @@ constexpr int B_BYTES = 2 * TNMAX * ROWB;     // hi + lo: 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int SBO = 8 * ROWB;                 // 512 B between 8-row atoms
 constexpr uint32_t TMEM_COLS = 512;           // two 256-column accumulators
-constexpr long long WAIT_LIMIT = 1ll << 23;
+constexpr uint64_t WAIT_NS = 2000000000ull;  // a wait gives up after 2 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -75,12 +75,19 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// try_wait suspends in hardware until the phase completes or a short time
+// limit passes; the loop gives up after WAIT_NS of wall time.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (long long i = 0; i < WAIT_LIMIT; i++) {
-    if (mbar_try(bar, parity)) return true;
-    if (i > 32) __nanosleep(32);
-  }
-  return false;
+  if (mbar_try(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  while (!mbar_try(bar, parity))
+    if (globaltimer_ns() - t0 > WAIT_NS) return false;
+  return true;
 }
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
@@ -203,8 +210,9 @@ __device__ __forceinline__ void store16(const SOut& o, int row, int col0, const 
 
 template <int EB, bool OUT_SPLIT>
 __global__ void __launch_bounds__(THREADS, 1)
-tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ units, int nunits,
-                const SOut* __restrict__ outs, const SSeg2* __restrict__ segs,
+tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ units,
+                const int* __restrict__ cta_begin, const SOut* __restrict__ outs,
+                const SSeg2* __restrict__ segs,
                 uint8_t* __restrict__ c_hi, uint8_t* __restrict__ c_lo, double* __restrict__ c64,
                 float* __restrict__ ws, int* __restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
@@ -244,13 +252,14 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  const int ubeg = cta_begin[blockIdx.x], uend = cta_begin[blockIdx.x + 1];
 
   if (warp == 0) {
     // ------------------------------------------------------------ TMA producer
     if (lane == 0) {
       uint32_t g = 0;
       bool ok = true;
-      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+      for (int u = ubeg; u < uend && ok; u++) {
         const SUnit un = units[u];
         const SOut o = outs[un.out];
         // locate the unit's first k-tile
@@ -272,7 +281,7 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
           const uint32_t bar = smem_u32(&full[slot]);
           mbar_expect_tx(bar, (uint32_t)(A_BYTES + 2 * sg.brows * ROWB));
           tma_load_3d(st, maps + sg.amap, kin * BK, un.tm * TM, 0, bar);
-          tma_load_3d(st + A_BYTES, maps + sg.bmap, kin * BK, un.tn * TNMAX, 0, bar);
+          tma_load_3d(st + A_BYTES, maps + sg.bmap, kin * BK, un.tn * o.tnw, 0, bar);
           g++;
           if (++kin >= sg.nkt) {
             kin = 0;
@@ -286,11 +295,11 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
     if (lane == 0) {
       uint32_t g = 0, ua = 0;
       bool ok = true;
-      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+      for (int u = ubeg; u < uend && ok; u++) {
         const SUnit un = units[u];
         if (un.kt1 <= un.kt0) continue;
         const SOut o = outs[un.out];
-        const int ncols = min(TNMAX, o.n - un.tn * TNMAX);
+        const int ncols = min(o.tnw, o.n - un.tn * o.tnw);
         const int nmma = (ncols + 15) & ~15;
         const uint32_t idesc = instr_desc<EB>(nmma);
         const uint32_t acc = ua & 1;
@@ -346,12 +355,12 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
     const int row = q * 32 + lane;
     uint32_t ua = 0;
     bool ok = true;
-    for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+    for (int u = ubeg; u < uend && ok; u++) {
       const SUnit un = units[u];
       const SOut o = outs[un.out];
-      const int ncols = min(TNMAX, o.n - un.tn * TNMAX);
+      const int ncols = min(o.tnw, o.n - un.tn * o.tnw);
       const int nmma = (ncols + 15) & ~15;
-      const int m0 = un.tm * TM, n0 = un.tn * TNMAX;
+      const int m0 = un.tm * TM, n0 = un.tn * o.tnw;
       const bool has = un.kt1 > un.kt0;
       const uint32_t acc = ua & 1;
       if (has) {
@@ -398,36 +407,61 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
                  : "memory");
 }
 
-// Sum the K-split partials of one output tile in slot order and store them.
+// Final store of 4 consecutive columns of one row (cols [col0, col0+4)).
 template <int EB, bool OUT_SPLIT>
-__global__ void split_reduce(const SRed* __restrict__ reds, const SOut* __restrict__ outs,
-                             const float* __restrict__ ws, uint8_t* __restrict__ c_hi,
-                             uint8_t* __restrict__ c_lo, double* __restrict__ c64) {
-  const SRed rd = reds[blockIdx.x];
-  const SOut o = outs[rd.out];
-  const int m0 = rd.tm * TM, n0 = rd.tn * TNMAX;
-  const int rows = min(TM, o.m - m0);
-  const int ncols = min(TNMAX, o.n - n0);
-  const int nmma = (ncols + 15) & ~15;
-  const int groups = nmma / 16;
-  for (int e = threadIdx.x; e < rows * groups; e += blockDim.x) {
-    const int r = e / groups, cc = (e - r * groups) * 16;
-    float v[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = 0.f;
-    for (int s = 0; s < rd.nslots; s++) {
-      const float* p = ws + ((int64_t)(rd.slot0 + s) * TM + r) * TNMAX + cc;
-#pragma unroll
-      for (int i = 0; i < 16; i += 4) {
-        const float4 t = *reinterpret_cast<const float4*>(p + i);
-        v[i] += t.x;
-        v[i + 1] += t.y;
-        v[i + 2] += t.z;
-        v[i + 3] += t.w;
-      }
+__device__ __forceinline__ void store4(const SOut& o, int row, int col0, float4 v, uint8_t* c_hi,
+                                       uint8_t* c_lo, double* c64) {
+  const int64_t e = o.c_off + (int64_t)row * o.ldc + col0;
+  if (OUT_SPLIT) {
+    if (col0 >= o.ldc) return;  // ldc is a multiple of 4 elements
+    uint32_t h[4], l[4];
+    split_f32<EB>(v.x, h[0], l[0]);
+    split_f32<EB>(v.y, h[1], l[1]);
+    split_f32<EB>(v.z, h[2], l[2]);
+    split_f32<EB>(v.w, h[3], l[3]);
+    if (EB == 2) {
+      *reinterpret_cast<uint2*>(c_hi + e * 2) = make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
+      *reinterpret_cast<uint2*>(c_lo + e * 2) = make_uint2(l[0] | (l[1] << 16), l[2] | (l[3] << 16));
+    } else {
+      *reinterpret_cast<uint4*>(c_hi + e * 4) = make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4*>(c_lo + e * 4) = make_uint4(l[0], l[1], l[2], l[3]);
     }
-    store16<EB, OUT_SPLIT>(o, m0 + r, n0 + cc, v, c_hi, c_lo, c64);
+  } else {
+    if (col0 < o.n) c64[e] = (double)v.x;
+    if (col0 + 1 < o.n) c64[e + 1] = (double)v.y;
+    if (col0 + 2 < o.n) c64[e + 2] = (double)v.z;
+    if (col0 + 3 < o.n) c64[e + 3] = (double)v.w;
   }
+}
+
+constexpr int RED_ROWS = 4;  // rows of one K-split tile per reduction block
+
+// Sum the K-split partials of a tile in slot order (deterministic) and store
+// them; one thread per (row, 4 columns), 4 rows per block.
+template <int EB, bool OUT_SPLIT>
+__global__ void __launch_bounds__(256)
+split_reduce(const SRed* __restrict__ reds, const SRedBlk* __restrict__ blks,
+             const SOut* __restrict__ outs, const float* __restrict__ ws,
+             uint8_t* __restrict__ c_hi, uint8_t* __restrict__ c_lo, double* __restrict__ c64) {
+  const SRedBlk b = blks[blockIdx.x];
+  const SRed rd = reds[b.red];
+  const SOut o = outs[rd.out];
+  const int m0 = rd.tm * TM, n0 = rd.tn * o.tnw;
+  const int rows = min(TM, o.m - m0);
+  const int ncols = min(o.tnw, o.n - n0);
+  const int g4 = ((ncols + 15) & ~15) / 4;  // float4 groups per row
+  const int r = b.r0 + threadIdx.x / 64, g = threadIdx.x % 64;
+  if (r >= rows || r >= b.r0 + RED_ROWS || g >= g4) return;
+  const float* p = ws + ((int64_t)rd.slot0 * TM + r) * TNMAX + g * 4;
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int s = 0; s < rd.nslots; s++) {
+    const float4 t = *reinterpret_cast<const float4*>(p + (int64_t)s * TM * TNMAX);
+    acc.x += t.x;
+    acc.y += t.y;
+    acc.z += t.z;
+    acc.w += t.w;
+  }
+  store4<EB, OUT_SPLIT>(o, m0 + r, n0 + g * 4, acc, c_hi, c_lo, c64);
 }
 
 }  // namespace
@@ -438,23 +472,22 @@ int tc_tile_n() { return TNMAX; }
 int tc_ktile_bytes() { return ROWB; }
 
 cudaError_t launch_tc_gemm(int eb, bool out_split, const CUtensorMap* maps, const SUnit* units,
-                           int nunits, const SOut* outs, const SSeg2* segs, void* c_hi, void* c_lo,
-                           double* c64, float* ws, const SRed* reds, int nreds, int* err, int grid,
-                           cudaStream_t st) {
-  if (nunits <= 0) return cudaSuccess;
-  if (grid > nunits) grid = nunits;
+                           const int* cta_begin, int nctas, const SOut* outs, const SSeg2* segs,
+                           void* c_hi, void* c_lo, double* c64, float* ws, const SRed* reds,
+                           const SRedBlk* redblk, int nredblk, int* err, cudaStream_t st) {
+  if (nctas <= 0) return cudaSuccess;
   const int sm = tc_smem_bytes();
 #define DMRGX_TC_LAUNCH(EB, OS)                                                               \
   do {                                                                                        \
     cudaError_t e = cudaFuncSetAttribute(tc_grouped_gemm<EB, OS>,                             \
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, sm);    \
     if (e != cudaSuccess) return e;                                                           \
-    tc_grouped_gemm<EB, OS><<<grid, THREADS, sm, st>>>(maps, units, nunits, outs, segs,       \
-                                                      (uint8_t*)c_hi, (uint8_t*)c_lo, c64, ws, \
-                                                      err);                                   \
-    if (nreds > 0)                                                                            \
-      split_reduce<EB, OS><<<nreds, 256, 0, st>>>(reds, outs, ws, (uint8_t*)c_hi,             \
-                                                 (uint8_t*)c_lo, c64);                        \
+    tc_grouped_gemm<EB, OS><<<nctas, THREADS, sm, st>>>(maps, units, cta_begin, outs, segs,   \
+                                                       (uint8_t*)c_hi, (uint8_t*)c_lo, c64,   \
+                                                       ws, err);                              \
+    if (nredblk > 0)                                                                          \
+      split_reduce<EB, OS><<<nredblk, 256, 0, st>>>(reds, redblk, outs, ws, (uint8_t*)c_hi,   \
+                                                   (uint8_t*)c_lo, c64);                      \
   } while (0)
   if (eb == 2) {
     if (out_split) DMRGX_TC_LAUNCH(2, true);

@@ -37,6 +37,7 @@ SIGNATURES = {
     "dmrgx_av": (_i, [_vp, _vp, _vp, _i]),
     "dmrgx_av_noalloc": (_i, [_i, _i64, _i64, _ip, _i, _vp, _i64p, _i, _ip, _i, _vp, _i64p, _i,
                               _vp, _vp, _vp]),
+    "dmrgx_eigsolve": (_i, [_vp, _i, _i, C.c_double, _i, _vp, _dp, _vp, _i64p]),
     "dmrgx_profile": (_i, [_vp, _i]),
     "dmrgx_profile_read": (_i, [_vp, _dp, _i]),
     "dmrgx_stream": (_vp, [_vp]),
@@ -180,6 +181,24 @@ class Context:
     def av_device(self, x_ptr: int, y_ptr: int):
         """Device pointers (e.g. torch tensors' data_ptr()) on this context's stream."""
         _check(lib().dmrgx_av(self.ptr, C.c_void_p(x_ptr), C.c_void_p(y_ptr), MEM_DEVICE))
+
+    def eigsolve(self, nev=6, ncv=0, tol=1e-10, maxiter=0, v0=None):
+        """Lowest nev eigenvalues and the lowest eigenvector (device Lanczos).
+
+        Returns (evals, evec, info dict)."""
+        ev = np.zeros(max(nev, 1))
+        vec = np.zeros(self.n, self._np)
+        info = np.zeros(6, np.int64)
+        p0 = None
+        if v0 is not None:
+            v0 = np.ascontiguousarray(v0, self._np)
+            p0 = v0.ctypes.data
+        _check(lib().dmrgx_eigsolve(self.ptr, nev, ncv, tol, maxiter, p0,
+                                    ev.ctypes.data_as(_dp), vec.ctypes.data, _i64p(info)))
+        d = dict(matvecs=int(info[0]), matvecs_fp64=int(info[1]), cycles=int(info[2]),
+                 corrections=int(info[3]), converged=int(info[4]),
+                 residual=float(info[5:6].view(np.float64)[0]))
+        return ev[:nev], vec, d
 
     def profile(self, enable: bool):
         _check(lib().dmrgx_profile(self.ptr, 1 if enable else 0))

@@ -143,6 +143,22 @@ int dmrgx_av_noalloc(int dtype, int64_t n, int64_t d_store, const int* rmap, int
                      const int* lmap, int n_lmap, const void* lenv, const int64_t* lenv_sizes,
                      int n_lenv_blocks, const void* in, void* out, void* stream);
 
+/* The nev lowest eigenvalues of H_eff and the eigenvector of the lowest: the
+ * replacement of the reference's ARPACK wrapper znaupd(n, nev, Evals, Evecs,
+ * pass_val) (src/dsaupd.cpp:65-155, src/znaupd.cpp:78-197), run on the device.
+ * Thick-restart Lanczos with FP64 basis, inner products and reorthogonalisation;
+ * with a split-precision context the lowest Ritz pair is finished by defect
+ * correction against the FP64 matvec (residual measured in FP64).
+ *   ncv      basis size (<= 0: 4*nev real, 6*nev complex, as the reference)
+ *   tol      convergence |H v - theta v| <= tol |theta| (<= 0: 1e-10)
+ *   maxiter  restart cycles (<= 0: 3n)
+ *   v0       host start vector of n elements, or NULL for a fixed default
+ *   evals    host, nev values ascending; evec: host, n elements, unit norm
+ *   info     NULL or 6 slots: matvecs, FP64 matvecs, cycles, defect corrections,
+ *            converged Ritz values, final residual norm (a double's bits). */
+int dmrgx_eigsolve(dmrgx_ctx* ctx, int nev, int ncv, double tol, int maxiter, const void* v0,
+                   double* evals, void* evec, int64_t* info);
+
 /* Per-launch device timing of the matvec, for roofline measurements: CUDA
  * events recorded on the context's stream around each launch of every matvec
  * while enabled (enable=1 clears the totals and starts, 0 stops).
