@@ -18,7 +18,7 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libdmrgx.so")
 
-SOURCES = ["qmeta.cpp", "ctx.cu", "gemm_f64.cu", "noalloc.cu", "split.cu", "tc_gemm.cu", "split_plan.cu", "eig.cu"]
+SOURCES = ["qmeta.cpp", "ctx.cu", "gemm_f64.cu", "noalloc.cu", "split.cu", "tc_gemm.cu", "split_plan.cu", "eig.cu", "qtensor.cu", "dmrg.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -62,7 +62,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
     if force or not _newer(LIB, objs):
-        cmd = [nvcc(), "-shared", "-ccbin", host_cxx()] + ARCH + objs + ["-o", LIB]
+        cmd = [nvcc(), "-shared", "-ccbin", host_cxx()] + ARCH + objs + ["-o", LIB, "-ldl"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

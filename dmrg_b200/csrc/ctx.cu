@@ -9,6 +9,7 @@
 #include "../../include/dmrgx.h"
 #include "ctx.h"
 #include "kernels.h"
+#include "qtensor.h"
 #include "split.h"
 
 using namespace dmrgx;
@@ -81,8 +82,9 @@ namespace {
 // a block used only with alpha=-1 is stored negated, a block used with both
 // signs gets a negated copy appended.  plus/minus: real offsets per block.
 struct EnvImage {
-  std::vector<double> vals;
+  std::vector<double> vals;        // host values (empty when built on the device)
   std::vector<int64_t> plus, minus;
+  int64_t len = 0;                 // doubles
 };
 
 EnvImage make_image(const double* src, const std::vector<int64_t>& off,
@@ -95,19 +97,24 @@ EnvImage make_image(const double* src, const std::vector<int64_t>& off,
   int64_t extra = 0;
   for (size_t b = 0; b < nb; b++)
     if (use[b] == 3) extra += size[b];
-  im.vals.resize((size_t)(total + extra) * f);
-  std::memcpy(im.vals.data(), src, sizeof(double) * (size_t)total * f);
+  im.len = (total + extra) * f;
+  if (src) {
+    im.vals.resize((size_t)im.len);
+    std::memcpy(im.vals.data(), src, sizeof(double) * (size_t)total * f);
+  }
   im.plus.assign(nb, -1);
   im.minus.assign(nb, -1);
   int64_t tail = total * f;
   for (size_t b = 0; b < nb; b++) {
     const int64_t o = off[b] * f, s = size[b] * f;
     if (use[b] == 2) {
-      for (int64_t i = 0; i < s; i++) im.vals[o + i] = -im.vals[o + i];
+      if (src)
+        for (int64_t i = 0; i < s; i++) im.vals[o + i] = -im.vals[o + i];
       im.minus[b] = o;
     } else if (use[b] == 3) {
       im.plus[b] = o;
-      for (int64_t i = 0; i < s; i++) im.vals[tail + i] = -im.vals[o + i];
+      if (src)
+        for (int64_t i = 0; i < s; i++) im.vals[tail + i] = -im.vals[o + i];
       im.minus[b] = tail;
       tail += s;
     } else {
@@ -216,9 +223,44 @@ int upload_stage(Stage& st, cudaStream_t s) {
 
 // Common tail of both plan entry points: sign-folded env images, stage
 // descriptors, device uploads, scratch.
+// Device image of an environment with the signs folded in, gathered from a
+// device tensor (the site-step path: environments never leave the GPU).
+int device_image(dmrgx_ctx* c, const QTensor& T, const EnvImage& im, double* dst) {
+  const int f = c->f();
+  std::vector<GOut> go;
+  std::vector<GSrc> gs;
+  for (size_t b = 0; b < im.plus.size(); b++) {
+    const int64_t sz = T.bsize((int)b);
+    if (sz == 0) continue;
+    for (int sgn = 0; sgn < 2; sgn++) {
+      const int64_t at = sgn ? im.minus[b] : im.plus[b];
+      if (at < 0) continue;
+      GSrc g;
+      std::memset(&g, 0, sizeof(g));
+      g.src_off = T.off[b];
+      g.strides[0] = 1;
+      g.sign = sgn ? -1.0 : 1.0;
+      gs.push_back(g);
+      GOut o;
+      std::memset(&o, 0, sizeof(o));
+      o.dst_off = at / f;
+      o.size = sz;
+      o.rank = 1;
+      o.dims[0] = (int32_t)sz;
+      o.dst_strides[0] = 1;
+      o.src_begin = (int32_t)gs.size() - 1;
+      o.src_count = 1;
+      go.push_back(o);
+    }
+  }
+  CUDA_TRY(launch_gather(T.d, dst, go, gs, f == 2, c->stream));
+  return 0;
+}
+
 int finalize_plan(dmrgx_ctx* c, const double* renv_vals, const std::vector<int64_t>& roff,
                   const std::vector<int64_t>& rsize, const double* lenv_vals,
-                  const std::vector<int64_t>& loff, const std::vector<int64_t>& lsize) {
+                  const std::vector<int64_t>& loff, const std::vector<int64_t>& lsize,
+                  const QTensor* rdev = nullptr, const QTensor* ldev = nullptr) {
   const int f = c->f();
   c->has_plan = false;
   c->flops = 0;
@@ -233,11 +275,16 @@ int finalize_plan(dmrgx_ctx* c, const double* renv_vals, const std::vector<int64
   std::map<int64_t, int> so;
   for (auto& r : c->rmap) so[r.out_beg] = 1;
   c->n_store_blocks = (int)so.size();
-  c->st1.a_len = (int64_t)ri.vals.size();
-  c->st2.a_len = (int64_t)li.vals.size();
+  c->st1.a_len = ri.len;
+  c->st2.a_len = li.len;
   CUDA_TRY(cudaSetDevice(c->device));
-  CUDA_TRY(c->renv.ensure(sizeof(double) * std::max<size_t>(1, ri.vals.size())));
-  CUDA_TRY(c->lenv.ensure(sizeof(double) * std::max<size_t>(1, li.vals.size())));
+  CUDA_TRY(c->renv.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, ri.len)));
+  CUDA_TRY(c->lenv.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, li.len)));
+  if (rdev) {
+    int rc0 = device_image(c, *rdev, ri, (double*)c->renv.p);
+    if (!rc0) rc0 = device_image(c, *ldev, li, (double*)c->lenv.p);
+    if (rc0) return rc0;
+  }
   CUDA_TRY(c->store.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, c->d_store * f)));
   CUDA_TRY(c->din.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, c->n * f)));
   CUDA_TRY(c->dout.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, c->n * f)));
@@ -318,6 +365,34 @@ int run_matvec_fp64(dmrgx_ctx* c, const double* in, double* out) {
 }  // namespace
 
 namespace dmrgx {
+// Plan from device tensors (the site step): same bookkeeping as
+// dmrgx_plan_build, environment images gathered on the device.
+int plan_build_device(dmrgx_ctx* c, const QTensor& L, const QTensor& R, int l_num, int r_num,
+                      int sector, const Group& G) {
+  if (L.f != c->f() || R.f != c->f()) {
+    set_error("plan: tensor element type differs from the context's");
+    return DMRGX_E_ARG;
+  }
+  std::vector<std::vector<int>> dim, sym, dim_ret, sym_ret;
+  generate_dim_sym(G, L.m, l_num - 1, R.m, r_num, sector, dim, sym);
+  c->n = get_dimension(dim, sym);
+  std::string e = get_map(G, R.m, dim, sym, r_num, 0, false, dim_ret, sym_ret, c->rmap);
+  if (e.empty()) {
+    c->d_store = get_dimension(dim_ret, sym_ret);
+    e = get_map(G, L.m, dim_ret, sym_ret, l_num, 0, true, dim, sym, c->lmap);
+  }
+  if (!e.empty()) {
+    set_error("plan: " + e);
+    return DMRGX_E_ARG;
+  }
+  c->psi_dim = dim;
+  c->psi_sym = sym;
+  std::vector<int64_t> rsize(R.m.syms.size()), lsize(L.m.syms.size());
+  for (size_t b = 0; b < rsize.size(); b++) rsize[b] = R.bsize((int)b);
+  for (size_t b = 0; b < lsize.size(); b++) lsize[b] = L.bsize((int)b);
+  return finalize_plan(c, nullptr, R.off, rsize, nullptr, L.off, lsize, &R, &L);
+}
+
 // the context's matvec (fp64=false) or its FP64 form regardless of precision
 int run_matvec_any(dmrgx_ctx* c, const double* in, double* out, bool fp64) {
   return fp64 ? run_matvec_fp64(c, in, out) : run_matvec(c, in, out);

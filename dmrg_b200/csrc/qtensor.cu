@@ -1,0 +1,991 @@
+// Device block-sparse tensor operations of the DMRG site step (see qtensor.h).
+//
+// Each operation builds its plan on the host from the metadata, following the
+// reference's bookkeeping line by line (block order, labels, fermion signs),
+// and runs on the device as: gathers (permutes, slices, sub-block placement,
+// conjugation) through one grouped gather kernel, contractions through the
+// grouped FP64 tensor-core GEMM of the matvec (gemm_f64.cu), and per-sector
+// SVDs through cuSOLVER's Jacobi SVD (gesvdj), loaded at run time.
+#include <cuComplex.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+
+#include "kernels.h"
+#include "qtensor.h"
+
+namespace dmrgx {
+
+QTensor::~QTensor() {
+  if (d) cudaFree(d);
+}
+
+cudaError_t QTensor::alloc(cudaStream_t s) {
+  off.assign(m.syms.size() + 1, 0);
+  for (size_t b = 0; b < m.syms.size(); b++) off[b + 1] = off[b] + m.block_size((int)b);
+  if (d) cudaFree(d);
+  d = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(double) * std::max<int64_t>(1, total() * f));
+  if (e != cudaSuccess) return e;
+  return cudaMemsetAsync(d, 0, sizeof(double) * std::max<int64_t>(1, total() * f), s);
+}
+
+namespace {
+
+// ------------------------------------------------------------------ gather kernel
+struct DevGather {
+  GOut* outs = nullptr;
+  GSrc* srcs = nullptr;
+  ~DevGather() {
+    cudaFree(outs);
+    cudaFree(srcs);
+  }
+};
+
+template <bool CPLX>
+__global__ void gather_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                              const GOut* __restrict__ outs, const GSrc* __restrict__ srcs) {
+  const GOut o = outs[blockIdx.y];
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < o.size;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int idx[8];
+    int64_t r = e;
+    for (int k = o.rank - 1; k >= 0; k--) {
+      idx[k] = (int)(r % o.dims[k]);
+      r /= o.dims[k];
+    }
+    int64_t dpos = o.dst_off;
+    for (int k = 0; k < o.rank; k++) dpos += idx[k] * o.dst_strides[k];
+    double ar = 0.0, ai = 0.0;
+    for (int s = 0; s < o.src_count; s++) {
+      const GSrc g = srcs[o.src_begin + s];
+      int64_t p = g.src_off;
+      for (int k = 0; k < o.rank; k++) p += idx[k] * g.strides[k];
+      if (CPLX) {
+        ar += g.sign * src[2 * p];
+        ai += g.sign * (g.conj ? -src[2 * p + 1] : src[2 * p + 1]);
+      } else {
+        ar += g.sign * src[p];
+      }
+    }
+    if (CPLX) {
+      dst[2 * dpos] = ar;
+      dst[2 * dpos + 1] = ai;
+    } else {
+      dst[dpos] = ar;
+    }
+  }
+}
+
+int64_t prod(const std::vector<int>& v, int a, int b) {  // product of v[a..b)
+  int64_t p = 1;
+  for (int i = a; i < b; i++) p *= v[i];
+  return p;
+}
+
+std::vector<int> block_dims(const QMeta& m, int b) {
+  std::vector<int> d(m.nleg());
+  for (int l = 0; l < m.nleg(); l++) d[l] = m.dims[l][m.syms[b][l]];
+  return d;
+}
+
+std::vector<int64_t> row_major_strides(const std::vector<int>& d) {
+  std::vector<int64_t> s(d.size(), 1);
+  for (int i = (int)d.size() - 2; i >= 0; i--) s[i] = s[i + 1] * d[i + 1];
+  return s;
+}
+
+GOut make_out(int64_t dst_off, const std::vector<int>& dims, const std::vector<int64_t>& dstr,
+              int src_begin, int src_count) {
+  GOut o;
+  std::memset(&o, 0, sizeof(o));
+  o.dst_off = dst_off;
+  o.rank = (int)dims.size();
+  o.size = 1;
+  for (int k = 0; k < o.rank; k++) {
+    o.dims[k] = dims[k];
+    o.dst_strides[k] = dstr[k];
+    o.size *= dims[k];
+  }
+  o.src_begin = src_begin;
+  o.src_count = src_count;
+  return o;
+}
+
+GSrc make_src(int64_t off, const std::vector<int64_t>& strides, double sign, bool conj) {
+  GSrc g;
+  std::memset(&g, 0, sizeof(g));
+  g.src_off = off;
+  for (size_t k = 0; k < strides.size(); k++) g.strides[k] = strides[k];
+  g.sign = sign;
+  g.conj = conj ? 1 : 0;
+  return g;
+}
+
+int64_t label_key(const std::vector<int>& st, const std::vector<std::vector<int>>& dim) {
+  int64_t loc = 0;
+  for (size_t q = 0; q < dim.size(); q++) loc = loc * (int64_t)dim[q].size() + st[q];
+  return loc;
+}
+
+// grouped NT GEMM over (C_o = sum_s A_s B_s^T) descriptors, uploaded per call
+cudaError_t run_gemms(const Engine& E, const double* A, const double* B, double* C,
+                      std::vector<DOut>& outs, std::vector<DSeg>& segs) {
+  if (outs.empty()) return cudaSuccess;
+  const int BM = f64_tile_m(), BN = f64_tile_n();
+  std::vector<DTile> tiles;
+  for (size_t o = 0; o < outs.size(); o++)
+    for (int a = 0; a < (outs[o].m + BM - 1) / BM; a++)
+      for (int b = 0; b < (outs[o].n + BN - 1) / BN; b++) {
+        DTile t;
+        t.out = (int32_t)o;
+        t.tm = (int16_t)a;
+        t.tn = (int16_t)b;
+        tiles.push_back(t);
+      }
+  if (tiles.empty()) return cudaSuccess;
+  DOut* d_o = nullptr;
+  DSeg* d_s = nullptr;
+  DTile* d_t = nullptr;
+  cudaError_t e = cudaMalloc(&d_o, sizeof(DOut) * outs.size());
+  if (e == cudaSuccess) e = cudaMalloc(&d_s, sizeof(DSeg) * std::max<size_t>(1, segs.size()));
+  if (e == cudaSuccess) e = cudaMalloc(&d_t, sizeof(DTile) * tiles.size());
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_o, outs.data(), sizeof(DOut) * outs.size(), cudaMemcpyHostToDevice, E.stream);
+  if (e == cudaSuccess && !segs.empty())
+    e = cudaMemcpyAsync(d_s, segs.data(), sizeof(DSeg) * segs.size(), cudaMemcpyHostToDevice, E.stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_t, tiles.data(), sizeof(DTile) * tiles.size(), cudaMemcpyHostToDevice, E.stream);
+  if (e == cudaSuccess)
+    e = launch_grouped_f64(A, B, C, d_t, (int)tiles.size(), d_o, d_s, E.f == 2, E.num_sms * 3,
+                           E.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+  cudaFree(d_o);
+  cudaFree(d_s);
+  cudaFree(d_t);
+  return e;
+}
+
+// ------------------------------------------------------------------ cuSOLVER (run-time loaded)
+struct Solver {
+  bool tried = false, ok = false;
+  cusolverDnHandle_t h = nullptr;
+  gesvdjInfo_t info = nullptr;
+  decltype(&cusolverDnCreate) create;
+  decltype(&cusolverDnSetStream) set_stream;
+  decltype(&cusolverDnCreateGesvdjInfo) create_info;
+  decltype(&cusolverDnXgesvdjSetTolerance) set_tol;
+  decltype(&cusolverDnXgesvdjSetMaxSweeps) set_sweeps;
+  decltype(&cusolverDnDgesvdj_bufferSize) d_buf;
+  decltype(&cusolverDnDgesvdj) d_svd;
+  decltype(&cusolverDnZgesvdj_bufferSize) z_buf;
+  decltype(&cusolverDnZgesvdj) z_svd;
+};
+Solver g_sol;
+std::mutex g_sol_mu;
+
+bool load_solver(std::string& err) {
+  std::lock_guard<std::mutex> lk(g_sol_mu);
+  if (g_sol.tried) {
+    if (!g_sol.ok) err = "cuSOLVER could not be loaded";
+    return g_sol.ok;
+  }
+  g_sol.tried = true;
+  const char* names[] = {getenv("DMRGX_CUSOLVER"), "libcusolver.so.11",
+                         "/usr/local/cuda/lib64/libcusolver.so.11", "libcusolver.so"};
+  void* lib = nullptr;
+  for (const char* n : names)
+    if (n && (lib = dlopen(n, RTLD_NOW | RTLD_LOCAL))) break;
+  if (!lib) {
+    err = "cuSOLVER (libcusolver.so.11) not found";
+    return false;
+  }
+#define SYM(field, name)                                     \
+  g_sol.field = (decltype(g_sol.field))dlsym(lib, #name);    \
+  if (!g_sol.field) {                                        \
+    err = "cuSOLVER symbol missing: " #name;                 \
+    return false;                                            \
+  }
+  SYM(create, cusolverDnCreate);
+  SYM(set_stream, cusolverDnSetStream);
+  SYM(create_info, cusolverDnCreateGesvdjInfo);
+  SYM(set_tol, cusolverDnXgesvdjSetTolerance);
+  SYM(set_sweeps, cusolverDnXgesvdjSetMaxSweeps);
+  SYM(d_buf, cusolverDnDgesvdj_bufferSize);
+  SYM(d_svd, cusolverDnDgesvdj);
+  SYM(z_buf, cusolverDnZgesvdj_bufferSize);
+  SYM(z_svd, cusolverDnZgesvdj);
+#undef SYM
+  if (g_sol.create(&g_sol.h) != CUSOLVER_STATUS_SUCCESS ||
+      g_sol.create_info(&g_sol.info) != CUSOLVER_STATUS_SUCCESS) {
+    err = "cuSOLVER initialisation failed";
+    return false;
+  }
+  g_sol.set_tol(g_sol.info, 1e-15);
+  g_sol.set_sweeps(g_sol.info, 100);
+  g_sol.ok = true;
+  return true;
+}
+
+}  // namespace
+
+cudaError_t launch_gather(const double* src, double* dst, const std::vector<GOut>& outs,
+                          const std::vector<GSrc>& srcs, bool cplx, cudaStream_t st) {
+  if (outs.empty()) return cudaSuccess;
+  DevGather g;
+  cudaError_t e = cudaMalloc(&g.outs, sizeof(GOut) * outs.size());
+  if (e == cudaSuccess) e = cudaMalloc(&g.srcs, sizeof(GSrc) * std::max<size_t>(1, srcs.size()));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(g.outs, outs.data(), sizeof(GOut) * outs.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && !srcs.empty())
+    e = cudaMemcpyAsync(g.srcs, srcs.data(), sizeof(GSrc) * srcs.size(), cudaMemcpyHostToDevice, st);
+  int64_t mx = 1;
+  for (auto& o : outs) mx = std::max<int64_t>(mx, o.size);
+  for (size_t y0 = 0; e == cudaSuccess && y0 < outs.size(); y0 += 65535) {
+    dim3 grid((unsigned)std::min<int64_t>(1024, (mx + 255) / 256),
+              (unsigned)std::min<size_t>(65535, outs.size() - y0));
+    if (cplx)
+      gather_kernel<true><<<grid, 256, 0, st>>>(src, dst, g.outs + y0, g.srcs);
+    else
+      gather_kernel<false><<<grid, 256, 0, st>>>(src, dst, g.outs + y0, g.srcs);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e;
+}
+
+QTPtr qt_from_host(const Engine& E, const int* meta, const void* vals, std::string& err) {
+  auto T = std::make_shared<QTensor>();
+  err = T->m.parse(meta);
+  if (!err.empty()) return nullptr;
+  T->f = E.f;
+  if (T->alloc(E.stream) != cudaSuccess) {
+    err = "device allocation failed";
+    return nullptr;
+  }
+  if (T->total() && cudaMemcpyAsync(T->d, vals, sizeof(double) * T->total() * T->f,
+                                    cudaMemcpyHostToDevice, E.stream) != cudaSuccess) {
+    err = "upload failed";
+    return nullptr;
+  }
+  cudaStreamSynchronize(E.stream);
+  return T;
+}
+
+int qt_to_host(const QTensor& T, std::vector<int>& meta, std::vector<double>& vals,
+               cudaStream_t s) {
+  const QMeta& m = T.m;
+  meta.clear();
+  meta.push_back(m.nleg());
+  meta.push_back((int)m.syms.size());
+  for (auto& d : m.dims) meta.push_back((int)d.size());
+  for (auto& d : m.dims) meta.insert(meta.end(), d.begin(), d.end());
+  for (int l = 0; l < m.nleg(); l++) meta.push_back(l < (int)m.dirs.size() ? m.dirs[l] : 0);
+  for (auto& sy : m.syms) meta.insert(meta.end(), sy.begin(), sy.end());
+  vals.resize((size_t)T.total() * T.f);
+  if (T.total() &&
+      cudaMemcpyAsync(vals.data(), T.d, sizeof(double) * vals.size(), cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess)
+    return -1;
+  return cudaStreamSynchronize(s) == cudaSuccess ? 0 : -1;
+}
+
+QTPtr qt_copy(const Engine& E, const QTensor& A) {
+  auto T = std::make_shared<QTensor>();
+  T->m = A.m;
+  T->f = A.f;
+  if (T->alloc(E.stream) != cudaSuccess) return nullptr;
+  if (A.total())
+    cudaMemcpyAsync(T->d, A.d, sizeof(double) * A.total() * A.f, cudaMemcpyDeviceToDevice,
+                    E.stream);
+  return T;
+}
+
+// ------------------------------------------------------------------ contract(A, a, B, b)
+QTPtr qt_contract_legs(const Engine& E, const QTensor& A, int a, const QTensor& B, int b,
+                       bool change, int ex0, int ex1, std::string& err) {
+  const Group& G = E.G;
+  const int na = A.m.nleg(), nb = B.m.nleg();
+  if (a < 0 || a >= na || b < 0 || b >= nb || A.m.dims[a] != B.m.dims[b]) {
+    err = "contract: dimensions of the contracted legs differ";
+    return nullptr;
+  }
+  auto T = std::make_shared<QTensor>();
+  T->f = E.f;
+  QMeta& M = T->m;
+  // output legs: A[0..a), B[0..b), B(b..], A(a..]   (src/qtensor.cpp:917-929)
+  std::vector<int> legsrc;  // code: +i for A leg i, -(j+1) for B leg j
+  for (int i = 0; i < a; i++) legsrc.push_back(i);
+  for (int j = 0; j < b; j++) legsrc.push_back(-(j + 1));
+  for (int j = b + 1; j < nb; j++) legsrc.push_back(-(j + 1));
+  for (int i = a + 1; i < na; i++) legsrc.push_back(i);
+  for (int c : legsrc) {
+    M.dims.push_back(c >= 0 ? A.m.dims[c] : B.m.dims[-c - 1]);
+    M.dirs.push_back(c >= 0 ? A.m.dirs[c] : B.m.dirs[-c - 1]);
+  }
+  // pairs, output blocks in first-appearance order, fermion signs
+  struct Pair { int l, r, out; double sign; };
+  std::vector<Pair> pairs;
+  std::map<int64_t, int> key2out;
+  for (size_t l = 0; l < A.m.syms.size(); l++)
+    for (size_t r = 0; r < B.m.syms.size(); r++) {
+      const auto& sa = A.m.syms[l];
+      const auto& sb = B.m.syms[r];
+      if (sa[a] != sb[b]) continue;
+      std::vector<int> sym;
+      for (int c : legsrc) sym.push_back(c >= 0 ? sa[c] : sb[-c - 1]);
+      int sign = 1;
+      if (change) {
+        int d_a = 0, b_p = 0;
+        for (int i = 0; i < na; i++) d_a = G.ss(d_a, sa[i] * A.m.dirs[i]);
+        for (int i = 0; i < nb; i++)
+          if (B.m.dirs[i] == 1) b_p = G.ss(b_p, sb[i]);
+        sign = G.sign(d_a, b_p);
+      } else {
+        int d_b = 0, a_p = 0;
+        for (int i = 0; i < nb; i++) d_b = G.ss(d_b, sb[i] * B.m.dirs[i]);
+        for (int i = 0; i < na; i++)
+          if (A.m.dirs[i] == 1) a_p = G.ss(a_p, sa[i]);
+        sign = G.sign(d_b, a_p);
+      }
+      const int64_t key = label_key(sym, M.dims);
+      auto it = key2out.find(key);
+      int o;
+      if (it == key2out.end()) {
+        o = (int)M.syms.size();
+        key2out[key] = o;
+        M.syms.push_back(sym);
+      } else {
+        o = it->second;
+      }
+      pairs.push_back({(int)l, (int)r, o, (double)sign});
+    }
+  if (T->alloc(E.stream) != cudaSuccess) {
+    err = "contract: allocation failed";
+    return nullptr;
+  }
+  // stage: A' = [i1, i2, k], B' = [j1, j2, k] per pair, C' = A' B'^T per pair
+  const int f = E.f;
+  int64_t la = 0, lb = 0, lc = 0;
+  std::vector<int64_t> oa(pairs.size()), ob(pairs.size()), oc(pairs.size());
+  for (size_t p = 0; p < pairs.size(); p++) {
+    oa[p] = la;
+    ob[p] = lb;
+    oc[p] = lc;
+    const auto da = block_dims(A.m, pairs[p].l), db = block_dims(B.m, pairs[p].r);
+    const int64_t al = prod(da, 0, a), ar = prod(da, a + 1, na), mid = da[a];
+    const int64_t bl = prod(db, 0, b), br = prod(db, b + 1, nb);
+    la += al * ar * mid;
+    lb += bl * br * mid;
+    lc += al * ar * bl * br;
+  }
+  double *dA = nullptr, *dB = nullptr, *dC = nullptr;
+  cudaError_t e = cudaMalloc(&dA, sizeof(double) * std::max<int64_t>(1, la * f));
+  if (e == cudaSuccess) e = cudaMalloc(&dB, sizeof(double) * std::max<int64_t>(1, lb * f));
+  if (e == cudaSuccess) e = cudaMalloc(&dC, sizeof(double) * std::max<int64_t>(1, lc * f));
+  std::vector<GOut> go;
+  std::vector<GSrc> gs;
+  std::vector<DOut> douts;
+  std::vector<DSeg> dsegs;
+  if (e == cudaSuccess) {
+    // A' permutes
+    for (size_t p = 0; p < pairs.size(); p++) {
+      const auto da = block_dims(A.m, pairs[p].l);
+      const int64_t al = prod(da, 0, a), ar = prod(da, a + 1, na), mid = da[a];
+      gs.push_back(make_src(A.off[pairs[p].l], {mid * ar, 1, ar}, 1.0, false));
+      go.push_back(make_out(oa[p], {(int)al, (int)ar, (int)mid}, {ar * mid, mid, 1},
+                            (int)gs.size() - 1, 1));
+    }
+    e = launch_gather(A.d, dA, go, gs, f == 2, E.stream);
+  }
+  if (e == cudaSuccess) {
+    go.clear();
+    gs.clear();
+    for (size_t p = 0; p < pairs.size(); p++) {
+      const auto db = block_dims(B.m, pairs[p].r);
+      const int64_t bl = prod(db, 0, b), br = prod(db, b + 1, nb), mid = db[b];
+      gs.push_back(make_src(B.off[pairs[p].r], {mid * br, 1, br}, 1.0, false));
+      go.push_back(make_out(ob[p], {(int)bl, (int)br, (int)mid}, {br * mid, mid, 1},
+                            (int)gs.size() - 1, 1));
+    }
+    e = launch_gather(B.d, dB, go, gs, f == 2, E.stream);
+  }
+  if (e == cudaSuccess) {
+    for (size_t p = 0; p < pairs.size(); p++) {
+      const auto da = block_dims(A.m, pairs[p].l), db = block_dims(B.m, pairs[p].r);
+      const int64_t M_ = prod(da, 0, a) * prod(da, a + 1, na), K = da[a];
+      const int64_t N_ = prod(db, 0, b) * prod(db, b + 1, nb);
+      if (M_ == 0 || N_ == 0) continue;
+      DOut o;
+      o.c_off = oc[p] * f;
+      o.m = (int32_t)M_;
+      o.n = (int32_t)(N_ * f);
+      o.seg_begin = (int32_t)dsegs.size();
+      o.seg_count = K > 0 ? 1 : 0;
+      douts.push_back(o);
+      if (K > 0) {
+        DSeg s;
+        s.a_off = oa[p] * f;
+        s.b_off = ob[p] * f;
+        s.k = (int32_t)(K * f);
+        s.pad_ = 0;
+        dsegs.push_back(s);
+      }
+    }
+    e = run_gemms(E, dA, dB, dC, douts, dsegs);
+  }
+  if (e == cudaSuccess) {
+    // out[legs] = sum_pairs sign * C'[(i1, i2), (j1, j2)], then exchange(ex0, ex1)
+    const int no = (int)T->m.syms.size();
+    std::vector<std::vector<int>> by_out(no);
+    for (size_t p = 0; p < pairs.size(); p++) by_out[pairs[p].out].push_back((int)p);
+    go.clear();
+    gs.clear();
+    const int nl = (int)legsrc.size();
+    std::vector<int> perm(nl);
+    for (int k = 0; k < nl; k++) perm[k] = k;
+    if (ex0 != ex1) std::swap(perm[ex0], perm[ex1]);
+    for (int o = 0; o < no; o++) {
+      std::vector<int> od = block_dims(T->m, o);   // pre-exchange output block dims
+      std::vector<int> fd(nl);                      // dims in the final leg order
+      for (int k = 0; k < nl; k++) fd[k] = od[perm[k]];
+      const auto fstr = row_major_strides(fd);
+      const int sb = (int)gs.size();
+      for (int p : by_out[o]) {
+        const auto da = block_dims(A.m, pairs[p].l), db = block_dims(B.m, pairs[p].r);
+        const int64_t ar = prod(da, a + 1, na), bl = prod(db, 0, b), br = prod(db, b + 1, nb);
+        // stride of every pre-exchange output leg inside C'
+        std::vector<int64_t> cs(nl);
+        int k = 0;
+        for (int i = 0; i < a; i++, k++) cs[k] = prod(da, i + 1, a) * ar * bl * br;
+        for (int j = 0; j < b; j++, k++) cs[k] = prod(db, j + 1, b) * br;
+        for (int j = b + 1; j < nb; j++, k++) cs[k] = prod(db, j + 1, nb);
+        for (int i = a + 1; i < na; i++, k++) cs[k] = prod(da, i + 1, na) * bl * br;
+        std::vector<int64_t> fs(nl);
+        for (int q = 0; q < nl; q++) fs[q] = cs[perm[q]];
+        gs.push_back(make_src(oc[p], fs, pairs[p].sign, false));
+      }
+      go.push_back(make_out(T->off[o], fd, fstr, sb, (int)gs.size() - sb));
+    }
+    e = launch_gather(dC, T->d, go, gs, f == 2, E.stream);
+  }
+  cudaFree(dA);
+  cudaFree(dB);
+  cudaFree(dC);
+  if (e != cudaSuccess) {
+    err = std::string("contract: ") + cudaGetErrorString(e);
+    return nullptr;
+  }
+  if (ex0 != ex1) {  // exchange the metadata (src/qtensor.cpp:361-371)
+    std::swap(M.dims[ex0], M.dims[ex1]);
+    std::swap(M.dirs[ex0], M.dirs[ex1]);
+    for (auto& s : M.syms) std::swap(s[ex0], s[ex1]);
+  }
+  return T;
+}
+
+QTPtr qt_exchange(const Engine& E, const QTensor& A, int a, int b, std::string& err) {
+  const int nl = A.m.nleg();
+  if (a < 0 || b < 0 || a >= nl || b >= nl) {
+    err = "exchange: leg out of range";
+    return nullptr;
+  }
+  auto T = std::make_shared<QTensor>();
+  T->f = A.f;
+  T->m = A.m;
+  std::swap(T->m.dims[a], T->m.dims[b]);
+  std::swap(T->m.dirs[a], T->m.dirs[b]);
+  for (auto& s : T->m.syms) std::swap(s[a], s[b]);
+  if (T->alloc(E.stream) != cudaSuccess) {
+    err = "exchange: allocation failed";
+    return nullptr;
+  }
+  std::vector<GOut> go;
+  std::vector<GSrc> gs;
+  for (size_t blk = 0; blk < A.m.syms.size(); blk++) {
+    const auto d = block_dims(A.m, (int)blk);
+    const auto s = row_major_strides(d);
+    std::vector<int> fd = d;
+    std::swap(fd[a], fd[b]);
+    std::vector<int64_t> fs = s;
+    std::swap(fs[a], fs[b]);
+    gs.push_back(make_src(A.off[blk], fs, 1.0, false));
+    go.push_back(make_out(T->off[blk], fd, row_major_strides(fd), (int)gs.size() - 1, 1));
+  }
+  cudaError_t e = launch_gather(A.d, T->d, go, gs, A.f == 2, E.stream);
+  if (e != cudaSuccess) {
+    err = std::string("exchange: ") + cudaGetErrorString(e);
+    return nullptr;
+  }
+  return T;
+}
+
+// ------------------------------------------------------------------ contract(A, B, ta, tb, num)
+QTPtr qt_contract_mat(const Engine& E, const QTensor& A, const QTensor& B, char ta, char tb,
+                      int num, std::string& err) {
+  const int na = A.m.nleg(), nb = B.m.nleg();
+  const bool an = ta == 'N' || ta == 'n', bn = tb == 'N' || tb == 'n';
+  const int ia = an ? na - num : 0;   // first contracted leg of A
+  const int ib = bn ? 0 : nb - num;   // first contracted leg of B
+  if (num <= 0 || ia < 0 || ib < 0) {
+    err = "contract: bad number of contracted legs";
+    return nullptr;
+  }
+  for (int i = 0; i < num; i++)
+    if (A.m.dims[ia + i] != B.m.dims[ib + i]) {
+      err = "contract: the dimensions are not the same";
+      return nullptr;
+    }
+  auto T = std::make_shared<QTensor>();
+  T->f = E.f;
+  QMeta& M = T->m;
+  for (int i = 0; i < na; i++)
+    if (i < ia || i >= ia + num) {
+      M.dims.push_back(A.m.dims[i]);
+      M.dirs.push_back(A.m.dirs[i]);
+    }
+  for (int i = 0; i < nb; i++)
+    if (i < ib || i >= ib + num) {
+      M.dims.push_back(B.m.dims[i]);
+      M.dirs.push_back(B.m.dirs[i]);
+    }
+  struct Pair { int l, r, out; };
+  std::vector<Pair> pairs;
+  std::map<int64_t, int> key2out;
+  for (size_t i = 0; i < A.m.syms.size(); i++)
+    for (size_t j = 0; j < B.m.syms.size(); j++) {
+      bool ok = true;
+      for (int k = 0; k < num; k++)
+        if (A.m.syms[i][ia + k] != B.m.syms[j][ib + k]) ok = false;
+      if (!ok) continue;
+      std::vector<int> sym;
+      for (int k = 0; k < na; k++)
+        if (k < ia || k >= ia + num) sym.push_back(A.m.syms[i][k]);
+      for (int k = 0; k < nb; k++)
+        if (k < ib || k >= ib + num) sym.push_back(B.m.syms[j][k]);
+      const int64_t key = label_key(sym, M.dims);
+      auto it = key2out.find(key);
+      int o;
+      if (it == key2out.end()) {
+        o = (int)M.syms.size();
+        key2out[key] = o;
+        M.syms.push_back(sym);
+      } else {
+        o = it->second;
+      }
+      pairs.push_back({(int)i, (int)j, o});
+    }
+  if (T->alloc(E.stream) != cudaSuccess) {
+    err = "contract: allocation failed";
+    return nullptr;
+  }
+  const int f = E.f;
+  // operands as [free, contracted]: transpose A when ta='T', B when tb='N'
+  auto need_t = [](bool transpose) { return transpose; };
+  int64_t la = 0, lb = 0;
+  std::map<int, int64_t> a_at, b_at;  // block -> offset in the staging buffer
+  std::vector<GOut> goa, gob;
+  std::vector<GSrc> gsa, gsb;
+  for (auto& p : pairs) {
+    if (need_t(!an) && !a_at.count(p.l)) {
+      const auto d = block_dims(A.m, p.l);
+      const int64_t K = prod(d, 0, num), Mx = prod(d, num, na);
+      a_at[p.l] = la;
+      gsa.push_back(make_src(A.off[p.l], {1, Mx}, 1.0, false));
+      goa.push_back(make_out(la, {(int)Mx, (int)K}, {K, 1}, (int)gsa.size() - 1, 1));
+      la += Mx * K;
+    }
+    if (need_t(bn) && !b_at.count(p.r)) {
+      const auto d = block_dims(B.m, p.r);
+      const int64_t K = prod(d, 0, num), Nx = prod(d, num, nb);
+      b_at[p.r] = lb;
+      gsb.push_back(make_src(B.off[p.r], {1, Nx}, 1.0, false));
+      gob.push_back(make_out(lb, {(int)Nx, (int)K}, {K, 1}, (int)gsb.size() - 1, 1));
+      lb += Nx * K;
+    }
+  }
+  double *dA = nullptr, *dB = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (la) e = cudaMalloc(&dA, sizeof(double) * la * f);
+  if (e == cudaSuccess && lb) e = cudaMalloc(&dB, sizeof(double) * lb * f);
+  if (e == cudaSuccess && la) e = launch_gather(A.d, dA, goa, gsa, f == 2, E.stream);
+  if (e == cudaSuccess && lb) e = launch_gather(B.d, dB, gob, gsb, f == 2, E.stream);
+  // both staged operands live in one buffer pair: A side and B side
+  const double* Abase = an ? A.d : dA;
+  const double* Bbase = bn ? dB : B.d;
+  std::vector<DOut> douts;
+  std::vector<DSeg> dsegs;
+  if (e == cudaSuccess) {
+    std::vector<std::vector<int>> by_out(M.syms.size());
+    for (size_t p = 0; p < pairs.size(); p++) by_out[pairs[p].out].push_back((int)p);
+    for (size_t o = 0; o < by_out.size(); o++) {
+      const auto od = block_dims(M, (int)o);
+      const int64_t Mo = prod(od, 0, na - num), No = prod(od, na - num, (int)od.size());
+      if (Mo == 0 || No == 0) continue;
+      DOut dout;
+      dout.c_off = T->off[o] * f;
+      dout.m = (int32_t)Mo;
+      dout.n = (int32_t)(No * f);
+      dout.seg_begin = (int32_t)dsegs.size();
+      dout.seg_count = 0;
+      for (int p : by_out[o]) {
+        const auto da = block_dims(A.m, pairs[p].l);
+        const int64_t K = an ? prod(da, na - num, na) : prod(da, 0, num);
+        if (K == 0) continue;
+        DSeg s;
+        s.a_off = (an ? A.off[pairs[p].l] : a_at[pairs[p].l]) * f;
+        s.b_off = (bn ? b_at[pairs[p].r] : B.off[pairs[p].r]) * f;
+        s.k = (int32_t)(K * f);
+        s.pad_ = 0;
+        dsegs.push_back(s);
+        dout.seg_count++;
+      }
+      douts.push_back(dout);
+    }
+    // the GEMM kernel takes one A and one B base: both operands may be staged
+    e = run_gemms(E, Abase, Bbase, T->d, douts, dsegs);
+  }
+  cudaFree(dA);
+  cudaFree(dB);
+  if (e != cudaSuccess) {
+    err = std::string("contract: ") + cudaGetErrorString(e);
+    return nullptr;
+  }
+  return T;
+}
+
+int qt_conjugate(const Engine& E, QTensor& A) {
+  for (auto& d : A.m.dirs) d = -d;
+  if (A.f != 2 || A.total() == 0) return 0;
+  std::vector<GOut> go;
+  std::vector<GSrc> gs;
+  gs.push_back(make_src(0, {1}, 1.0, true));
+  go.push_back(make_out(0, {(int)A.total()}, {1}, 0, 1));
+  return launch_gather(A.d, A.d, go, gs, true, E.stream) == cudaSuccess ? 0 : -1;
+}
+
+// ------------------------------------------------------------------ svd
+namespace {
+// combine legs [lo, hi] of label tuples into one leg (src/qtensor.cpp:466-585):
+// for every tuple of the legs (lexicographic), its summed label and its offset in
+// the combined sector.  Returns the combined sector sizes.
+std::vector<int> combine_layout(const Group& G, const std::vector<std::vector<int>>& dims, int lo,
+                                int hi, std::vector<std::vector<int>>& tuples,
+                                std::vector<int>& tsum, std::vector<int64_t>& tbeg,
+                                std::vector<int64_t>& tsize) {
+  std::vector<int> radix;
+  for (int i = lo; i <= hi; i++) radix.push_back((int)dims[i].size());
+  tuples.clear();
+  std::vector<int> cur(radix.size(), 0);
+  int64_t total = 1;
+  for (int r : radix) total *= r;
+  for (int64_t t = 0; t < total; t++) {
+    tuples.push_back(cur);
+    for (int p = (int)radix.size() - 1; p >= 0; p--) {
+      if (++cur[p] < radix[p]) break;
+      cur[p] = 0;
+    }
+  }
+  int maxs = 0;
+  tsum.resize(tuples.size());
+  tsize.resize(tuples.size());
+  for (size_t t = 0; t < tuples.size(); t++) {
+    int s = 0;
+    int64_t sz = 1;
+    for (int i = lo; i <= hi; i++) {
+      s = G.ss(s, tuples[t][i - lo]);
+      sz *= dims[i][tuples[t][i - lo]];
+    }
+    tsum[t] = s;
+    tsize[t] = sz;
+    maxs = std::max(maxs, s);
+  }
+  std::vector<int> secsize(maxs + 1, 0);
+  tbeg.resize(tuples.size());
+  std::vector<int64_t> run(maxs + 1, 0);
+  for (size_t t = 0; t < tuples.size(); t++) {
+    tbeg[t] = run[tsum[t]];
+    run[tsum[t]] += tsize[t];
+  }
+  for (int s = 0; s <= maxs; s++) secsize[s] = (int)run[s];
+  return secsize;
+}
+}  // namespace
+
+int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTPtr& V,
+           std::vector<double>& s, std::string& err) {
+  const Group& G = E.G;
+  const int nl = A.m.nleg();
+  if (num <= 0 || num >= nl) {
+    err = "svd: the number of left legs should be 1.." + std::to_string(nl - 1);
+    return -1;
+  }
+  const int f = E.f;
+  std::vector<std::vector<int>> lt, rt;
+  std::vector<int> lsum, rsum;
+  std::vector<int64_t> lbeg, lsz, rbeg, rsz;
+  const std::vector<int> L = combine_layout(G, A.m.dims, 0, num - 1, lt, lsum, lbeg, lsz);
+  const std::vector<int> R = combine_layout(G, A.m.dims, num, nl - 1, rt, rsum, rbeg, rsz);
+  // sector blocks (c0, c1) in lexicographic order, as the two combines produce them
+  std::map<std::pair<int, int>, int> sec;
+  for (auto& sy : A.m.syms) {
+    int c0 = 0, c1 = 0;
+    for (int i = 0; i < num; i++) c0 = G.ss(c0, sy[i]);
+    for (int i = num; i < nl; i++) c1 = G.ss(c1, sy[i]);
+    sec[{c0, c1}] = 0;
+  }
+  std::vector<std::pair<int, int>> secs;
+  for (auto& kv : sec) secs.push_back(kv.first);
+  {
+    const int tot = G.ss(secs[0].first, secs[0].second);
+    for (auto& p : secs)
+      if (G.ss(p.first, p.second) != tot) {
+        err = "svd: symmetry sectors do not have a constraint";
+        return -1;
+      }
+  }
+  const int ns = (int)secs.size();
+  std::vector<int64_t> Rr(ns), Cc(ns), moff(ns + 1, 0);
+  for (int i = 0; i < ns; i++) {
+    Rr[i] = secs[i].first < (int)L.size() ? L[secs[i].first] : 0;
+    Cc[i] = secs[i].second < (int)R.size() ? R[secs[i].second] : 0;
+    moff[i + 1] = moff[i] + Rr[i] * Cc[i];
+  }
+  // tuple index lookups
+  auto tuple_index = [](const std::vector<std::vector<int>>& tl, const std::vector<int>& v) {
+    for (size_t t = 0; t < tl.size(); t++)
+      if (tl[t] == v) return (int)t;
+    return -1;
+  };
+  // place every block into its sector matrix (row-major R x C)
+  double* dM = nullptr;
+  cudaError_t e = cudaMalloc(&dM, sizeof(double) * std::max<int64_t>(1, moff[ns] * f));
+  if (e == cudaSuccess) e = cudaMemsetAsync(dM, 0, sizeof(double) * std::max<int64_t>(1, moff[ns] * f), E.stream);
+  std::vector<GOut> go;
+  std::vector<GSrc> gs;
+  for (size_t b = 0; b < A.m.syms.size(); b++) {
+    const auto& sy = A.m.syms[b];
+    std::vector<int> lv(sy.begin(), sy.begin() + num), rv(sy.begin() + num, sy.end());
+    const int ti = tuple_index(lt, lv), tj = tuple_index(rt, rv);
+    int c0 = lsum[ti], c1 = rsum[tj];
+    const int si = (int)std::distance(secs.begin(), std::find(secs.begin(), secs.end(), std::make_pair(c0, c1)));
+    const int64_t rows = lsz[ti], cols = rsz[tj];
+    if (rows == 0 || cols == 0) continue;
+    gs.push_back(make_src(A.off[b], {cols, 1}, 1.0, false));
+    go.push_back(make_out(moff[si] + lbeg[ti] * Cc[si] + rbeg[tj], {(int)rows, (int)cols},
+                          {Cc[si], 1}, (int)gs.size() - 1, 1));
+  }
+  if (e == cudaSuccess) e = launch_gather(A.d, dM, go, gs, f == 2, E.stream);
+  if (e != cudaSuccess) {
+    cudaFree(dM);
+    err = std::string("svd: ") + cudaGetErrorString(e);
+    return -1;
+  }
+  if (!load_solver(err)) {
+    cudaFree(dM);
+    return -1;
+  }
+  // per-sector SVD of X = A^T (column-major C x R view of the row-major block)
+  std::vector<std::vector<double>> S(ns);
+  std::vector<double*> Ux(ns, nullptr), Vx(ns, nullptr);
+  int* dinfo = nullptr;
+  cudaMalloc(&dinfo, sizeof(int));
+  bool fail = false;
+  std::lock_guard<std::mutex> lk(g_sol_mu);
+  g_sol.set_stream(g_sol.h, E.stream);
+  for (int i = 0; i < ns && !fail; i++) {
+    const int m = (int)Cc[i], n = (int)Rr[i];
+    const int mn = std::min(m, n);
+    S[i].assign(mn, 0.0);
+    if (mn == 0) continue;
+    double *dS = nullptr, *work = nullptr;
+    cudaMalloc(&Ux[i], sizeof(double) * (size_t)m * m * f);
+    cudaMalloc(&Vx[i], sizeof(double) * (size_t)n * n * f);
+    cudaMalloc(&dS, sizeof(double) * mn);
+    int lwork = 0;
+    cusolverStatus_t st;
+    double* X = dM + moff[i] * f;
+    // gesvdj overwrites its input: the sector matrices are not needed afterwards
+    if (f == 1)
+      st = g_sol.d_buf(g_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, X, m, dS, Ux[i], m, Vx[i], n,
+                       &lwork, g_sol.info);
+    else
+      st = g_sol.z_buf(g_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, (cuDoubleComplex*)X, m, dS,
+                       (cuDoubleComplex*)Ux[i], m, (cuDoubleComplex*)Vx[i], n, &lwork, g_sol.info);
+    if (st == CUSOLVER_STATUS_SUCCESS) cudaMalloc(&work, sizeof(double) * (size_t)std::max(1, lwork) * f);
+    if (st == CUSOLVER_STATUS_SUCCESS) {
+      if (f == 1)
+        st = g_sol.d_svd(g_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, X, m, dS, Ux[i], m, Vx[i], n,
+                         work, lwork, dinfo, g_sol.info);
+      else
+        st = g_sol.z_svd(g_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, (cuDoubleComplex*)X, m, dS,
+                         (cuDoubleComplex*)Ux[i], m, (cuDoubleComplex*)Vx[i], n,
+                         (cuDoubleComplex*)work, lwork, dinfo, g_sol.info);
+    }
+    int hinfo = 0;
+    if (st == CUSOLVER_STATUS_SUCCESS) {
+      cudaMemcpyAsync(S[i].data(), dS, sizeof(double) * mn, cudaMemcpyDeviceToHost, E.stream);
+      cudaMemcpyAsync(&hinfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost, E.stream);
+      cudaStreamSynchronize(E.stream);
+    }
+    cudaFree(dS);
+    cudaFree(work);
+    if (st != CUSOLVER_STATUS_SUCCESS || hinfo != 0) {
+      err = "svd: cuSOLVER gesvdj failed (status " + std::to_string((int)st) + ", info " +
+            std::to_string(hinfo) + ")";
+      fail = true;
+    }
+    for (int q = 1; q < mn && !fail; q++)
+      if (S[i][q] > S[i][q - 1]) {
+        err = "svd: singular values not in descending order";
+        fail = true;
+      }
+  }
+  cudaFree(dinfo);
+  cudaFree(dM);
+  auto free_all = [&]() {
+    for (auto p : Ux) cudaFree(p);
+    for (auto p : Vx) cudaFree(p);
+  };
+  if (fail) {
+    free_all();
+    return -1;
+  }
+  // ---- global merge and truncation (src/qtensor.cpp:1178-1252)
+  int64_t sum = 0;
+  for (auto& v : S) sum += (int64_t)v.size();
+  s.assign(sum, 0.0);
+  int64_t keep = sum;
+  if (cutoff != 0 && cutoff < sum) keep = cutoff;
+  std::vector<int64_t> un(ns, 0);
+  for (int64_t t = 0; t < sum; t++) {
+    double mx = -1;
+    int loc = -1;
+    for (int i = 0; i < ns; i++)
+      if (un[i] < (int64_t)S[i].size() && mx < S[i][un[i]]) {
+        mx = S[i][un[i]];
+        loc = i;
+      }
+    s[t] = mx;
+    un[loc] += 1;
+    if (t + 1 == keep) {
+      // remember the counts of the kept values
+      std::vector<int64_t> kept = un;
+      for (int64_t t2 = t + 1; t2 < sum; t2++) {
+        double m2 = -1;
+        int l2 = -1;
+        for (int i = 0; i < ns; i++)
+          if (un[i] < (int64_t)S[i].size() && m2 < S[i][un[i]]) {
+            m2 = S[i][un[i]];
+            l2 = i;
+          }
+        s[t2] = m2;
+        un[l2] += 1;
+      }
+      un = kept;
+      break;
+    }
+  }
+  std::vector<int64_t> vn = un;
+  if (cutoff == 0) {
+    // no truncation: full U and V
+    for (int i = 0; i < ns; i++) {
+      un[i] = Rr[i];
+      vn[i] = Cc[i];
+    }
+  } else {
+    // pad with complement vectors up to min(dim, cutoff); the sector lists are
+    // indexed by block position, as in the reference
+    auto pad = [&](std::vector<int64_t>& cnt, int64_t total_dim, const std::vector<int>& secsz) {
+      int64_t diff = std::min<int64_t>(total_dim, cutoff) - keep;
+      while (diff > 0) {
+        bool moved = false;
+        for (int i = 0; i < ns && diff > 0; i++) {
+          const int64_t lim = i < (int)secsz.size() ? secsz[i] : 0;
+          if (cnt[i] < lim) {
+            cnt[i]++;
+            diff--;
+            moved = true;
+          }
+        }
+        if (!moved) break;
+      }
+    };
+    int64_t Ltot = 0, Rtot = 0;
+    for (int v : L) Ltot += v;
+    for (int v : R) Rtot += v;
+    pad(un, Ltot, L);
+    pad(vn, Rtot, R);
+  }
+  // ---- U: leg 0 split back into the first `num` legs, leg 1 = kept columns
+  U = std::make_shared<QTensor>();
+  V = std::make_shared<QTensor>();
+  U->f = V->f = f;
+  for (int i = 0; i < num; i++) U->m.dims.push_back(A.m.dims[i]);
+  // labels without a block keep the combined size (src/qtensor.cpp:1153-1157)
+  std::vector<int> usz = L, vsz = R;
+  for (int i = 0; i < ns; i++) {
+    usz[secs[i].first] = (int)un[i];
+    vsz[secs[i].second] = (int)vn[i];
+  }
+  U->m.dims.push_back(usz);
+  V->m.dims.push_back(vsz);
+  for (int i = num; i < nl; i++) V->m.dims.push_back(A.m.dims[i]);
+  U->m.dirs.assign(num + 1, 1);
+  V->m.dirs.assign(nl - num + 1, 1);
+  struct Piece { int sector, tuple; };
+  std::vector<Piece> up, vp;
+  for (int i = 0; i < ns; i++)
+    for (size_t t = 0; t < lt.size(); t++)
+      if (lsum[t] == secs[i].first && lsz[t] > 0 && un[i] > 0) {
+        std::vector<int> sy = lt[t];
+        sy.push_back(secs[i].first);
+        U->m.syms.push_back(sy);
+        up.push_back({i, (int)t});
+      }
+  for (int i = 0; i < ns; i++)
+    for (size_t t = 0; t < rt.size(); t++)
+      if (rsum[t] == secs[i].second && rsz[t] > 0 && vn[i] > 0) {
+        std::vector<int> sy(1, secs[i].second);
+        sy.insert(sy.end(), rt[t].begin(), rt[t].end());
+        V->m.syms.push_back(sy);
+        vp.push_back({i, (int)t});
+      }
+  if (U->alloc(E.stream) != cudaSuccess || V->alloc(E.stream) != cudaSuccess) {
+    free_all();
+    err = "svd: allocation failed";
+    return -1;
+  }
+  // U block (rows of the tuple, kept columns j < un): U[r][j] = conj(Vx[(lbeg + r) + j*R])
+  for (size_t p = 0; p < up.size() && e == cudaSuccess; p++) {
+    const int i = up[p].sector, t = up[p].tuple;
+    const int64_t rows = lsz[t], cols = std::min<int64_t>(un[i], Rr[i]);
+    if (cols <= 0) continue;
+    go.assign(1, make_out(U->off[p], {(int)rows, (int)cols}, {un[i], 1}, 0, 1));
+    gs.assign(1, make_src(lbeg[t], {1, Rr[i]}, 1.0, f == 2));
+    e = launch_gather(Vx[i], U->d, go, gs, f == 2, E.stream);
+  }
+  // V block (kept rows j < vn, columns of the tuple): V[j][c] = Ux[(rbeg + c) + j*C]
+  for (size_t p = 0; p < vp.size() && e == cudaSuccess; p++) {
+    const int i = vp[p].sector, t = vp[p].tuple;
+    const int64_t rows = std::min<int64_t>(vn[i], Cc[i]), cols = rsz[t];
+    if (rows <= 0) continue;
+    go.assign(1, make_out(V->off[p], {(int)rows, (int)cols}, {cols, 1}, 0, 1));
+    gs.assign(1, make_src(rbeg[t], {Cc[i], 1}, 1.0, false));
+    e = launch_gather(Ux[i], V->d, go, gs, f == 2, E.stream);
+  }
+  free_all();
+  if (e != cudaSuccess) {
+    err = std::string("svd: ") + cudaGetErrorString(e);
+    return -1;
+  }
+  return 0;
+}
+
+}  // namespace dmrgx

@@ -38,6 +38,8 @@ SIGNATURES = {
     "dmrgx_av_noalloc": (_i, [_i, _i64, _i64, _ip, _i, _vp, _i64p, _i, _ip, _i, _vp, _i64p, _i,
                               _vp, _vp, _vp]),
     "dmrgx_eigsolve": (_i, [_vp, _i, _i, C.c_double, _i, _vp, _dp, _vp, _i64p]),
+    "dmrgx_dmrg": (_i, [_vp, _i, _i, _i, _i, _i, _dp, _i, _dp, _dp, _ip, _i64p, _i64, _i64p,
+                        _dp]),
     "dmrgx_profile": (_i, [_vp, _i]),
     "dmrgx_profile_read": (_i, [_vp, _dp, _i]),
     "dmrgx_stream": (_vp, [_vp]),
@@ -199,6 +201,25 @@ class Context:
                  corrections=int(info[3]), converged=int(info[4]),
                  residual=float(info[5:6].view(np.float64)[0]))
         return ev[:nev], vec, d
+
+    def dmrg(self, model, L, m, sweeps, params, sector=0, cap=100000):
+        """Run the reference dmrg() schedule on the GPU.  model: 'kitaev' (F64
+        context), 'xyz' or 'potts' (C128 context).  Returns a dict of per-step
+        arrays (lr, energies[:, 6], trunc, matvecs) and timings."""
+        code = {"kitaev": 0, "xyz": 1, "potts": 2, "xyz_real": 3}[model]
+        par = np.ascontiguousarray(params, np.float64)
+        en = np.zeros((cap, 6))
+        tr = np.zeros(cap)
+        lr = np.zeros((cap, 2), np.int32)
+        mv = np.zeros(cap, np.int64)
+        ns = np.zeros(1, np.int64)
+        sec = np.zeros(5)
+        _check(lib().dmrgx_dmrg(self.ptr, code, L, m, sweeps, sector, par.ctypes.data_as(_dp),
+                                par.size, en.ctypes.data_as(_dp), tr.ctypes.data_as(_dp),
+                                _ip(lr), _i64p(mv), cap, _i64p(ns), sec.ctypes.data_as(_dp)))
+        k = int(ns[0])
+        return dict(lr=lr[:k], energies=en[:k], trunc=tr[:k], matvecs=mv[:k],
+                    seconds=dict(total=sec[0], eig=sec[1], svd=sec[2], env=sec[3], fuse=sec[4]))
 
     def profile(self, enable: bool):
         _check(lib().dmrgx_profile(self.ptr, 1 if enable else 0))

@@ -159,6 +159,21 @@ int dmrgx_av_noalloc(int dtype, int64_t n, int64_t d_store, const int* rmap, int
 int dmrgx_eigsolve(dmrgx_ctx* ctx, int nev, int ncv, double tol, int maxiter, const void* v0,
                    double* evals, void* evec, int64_t* info);
 
+/* The reference's dmrg() schedule (src/functions.cpp:157-227) with every site
+ * step on the GPU: env (x) MPO fusion, the device eigensolver (with this
+ * context's matvec precision), block SVD truncation and environment update.
+ * model: 0 Kitaev(t, p, u) on an F64 context, 1 XYZ(jx, jy, jz) and 2 Potts3
+ * (f, j, p, t) on C128 contexts, built as the reference's drivers build them
+ * (kitaev.cpp, xyz.cpp, potts.cpp; src/operators.cpp); 3 the same XYZ chain with
+ * a real MPO (sigma_y sigma_y = -(i sigma_y)(i sigma_y)) on an F64 context.  m: bond dimension, sweeps:
+ * the reference's n.  Per step (up to cap steps): energies[6*i..] the six lowest
+ * values, trunc[i] the truncation error, steps_lr[2*i..] the (l, r) sites,
+ * matvecs[i] the matvec count; nsteps: steps done.  seconds (5 slots, may be
+ * NULL): total, eigensolver, SVD, environment update, env (x) MPO fusion. */
+int dmrgx_dmrg(dmrgx_ctx* ctx, int model, int L, int m, int sweeps, int sector,
+               const double* params, int nparams, double* energies, double* trunc, int* steps_lr,
+               int64_t* matvecs, int64_t cap, int64_t* nsteps, double* seconds);
+
 /* Per-launch device timing of the matvec, for roofline measurements: CUDA
  * events recorded on the context's stream around each launch of every matvec
  * while enabled (enable=1 clears the totals and starts, 0 stops).

@@ -1,0 +1,62 @@
+"""The full dmrg() schedule on the GPU against the reference.
+
+Small chains where the bond dimension keeps the state exact: every step's
+lowest energy must equal the reference's step energy (the reference prints 10
+decimals, global.h ACC) and the final energy the exact value (BdG / ED) to
+1e-10 relative; truncation errors match the reference's to 1e-9."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from dmrg_b200 import native
+from oracle import exact
+
+pytestmark = pytest.mark.gpu
+
+with open(os.path.join(GOLDEN, "energies.json")) as fh:
+    GOLD = json.load(fh)
+
+CASES = [("kitaev", "kitaev", native.F64), ("xyz", "xyz", native.C128),
+         ("xyz", "xyz_real", native.F64), ("potts", "potts", native.C128)]
+
+
+@pytest.mark.parametrize("gold,model,dtype", CASES)
+def test_dmrg_small_chain_matches_reference_steps(gold, model, dtype):
+    g = GOLD[gold]
+    a = g["args"]
+    ctx = native.Context(dtype)
+    r = ctx.dmrg(model, a["L"], a["m"], a["n"], a["params"])
+    ref = np.array(g["energy_rows"])
+    assert len(r["energies"]) == len(ref)
+    assert np.array_equal(r["lr"], ref[:, :2].astype(int))
+    # reference energies are printed with 10 decimals
+    assert np.abs(r["energies"][:, 0] - ref[:, 2]).max() < 2e-10 * np.abs(ref[:, 2]).max() + 6e-11
+    assert abs(r["energies"][-1, 0] - g["exact"]) < 1e-10 * abs(g["exact"])
+    tr = np.array(g["trunc_err_rows"])
+    assert np.abs(r["trunc"] - tr[:, 2]).max() < 1e-9
+    print(model, r["seconds"], r["energies"][-1, 0])
+
+
+def test_kitaev_L32_m64_matches_bdg():
+    """Config 1: Kitaev chain L=32, t=Delta=1, mu=0.5 (u=0.25), m=64, 6 sweeps."""
+    ctx = native.Context(native.F64)
+    r = ctx.dmrg("kitaev", 32, 64, 6, [1.0, 1.0, 0.25])
+    e = r["energies"][-1, 0]
+    ex = exact.kitaev_bdg(32, 1.0, 1.0, 0.25)
+    print("kitaev L32 m64", e, ex, r["seconds"], len(r["trunc"]))
+    assert abs(e - ex) < 1e-9 * abs(ex)
+
+
+@pytest.mark.parametrize("prec", [native.PREC_BF16X3, native.PREC_TF32X3])
+def test_dmrg_split_precision_energy(prec):
+    """Split-precision matvecs + FP64 defect correction reach the FP64 energy."""
+    c64 = native.Context(native.F64)
+    r64 = c64.dmrg("xyz_real", 16, 32, 2, [1.0, 0.8, 0.5])
+    ctx = native.Context(native.F64)
+    ctx.set_precision(prec)
+    r = ctx.dmrg("xyz_real", 16, 32, 2, [1.0, 0.8, 0.5])
+    print(prec, r["energies"][-1, 0], r64["energies"][-1, 0], r["seconds"])
+    assert abs(r["energies"][-1, 0] - r64["energies"][-1, 0]) <= 1e-9 * abs(r64["energies"][-1, 0])
