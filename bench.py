@@ -41,6 +41,11 @@ def parse():
     p.add_argument("--prec", default="bf16x3", choices=["fp64", "bf16x3", "tf32x3"])
     p.add_argument("--impl", default="dmrgx", choices=["dmrgx", "reference"])
     p.add_argument("--cpu-sample-s", type=float, default=12.0)
+    p.add_argument("--sweep", type=int, default=1,
+                   help="also time a DMRG sweep schedule (XYZ real, L=32, m=128, 1 sweep)")
+    p.add_argument("--sweep-L", type=int, default=32)
+    p.add_argument("--sweep-m", type=int, default=128)
+    p.add_argument("--sweep-n", type=int, default=1)
     return p.parse_args()
 
 
@@ -183,6 +188,36 @@ def cpu_reference_rate(sample_s: float, w=None):
                 sample=f"{cnt} numpy-port matvecs on the m=1024 microbench in {el:.1f} s")
 
 
+def sweep_compare(native, args):
+    """The reference dmrg() schedule on the GPU for the XYZ chain (jx=1, jy=0.8,
+    jz=0.5, real MPO) with the FP64 matvec and with the headline precision:
+    wall seconds of the whole schedule, seconds per full sweep (2(L-2) steps at
+    the average step cost) and the final energies."""
+    prec = {"fp64": native.PREC_FP64, "bf16x3": native.PREC_BF16X3,
+            "tf32x3": native.PREC_TF32X3}[args.prec]
+    out = {"workload": f"XYZ chain L={args.sweep_L}, m={args.sweep_m}, {args.sweep_n} sweep(s), "
+                       "reference dmrg() schedule, real MPO", "runs": {}}
+    for name, p in (("fp64", native.PREC_FP64), (args.prec, prec)):
+        if name in out["runs"]:
+            continue
+        c = native.Context(native.F64)
+        c.set_precision(p)
+        r = c.dmrg("xyz_real", args.sweep_L, args.sweep_m, args.sweep_n, [1.0, 0.8, 0.5])
+        ns = len(r["trunc"])
+        tot = float(r["seconds"]["total"])
+        out["runs"][name] = {"schedule_s": tot, "steps": ns,
+                             "sweep_s": tot * 2 * (args.sweep_L - 2) / ns,
+                             "energy": float(r["energies"][-1, 0]),
+                             "matvecs": int(r["matvecs"].sum()),
+                             "split_s": {k: float(v) for k, v in r["seconds"].items()}}
+        c.close()
+    if args.prec != "fp64":
+        a, b = out["runs"]["fp64"], out["runs"][args.prec]
+        out["speedup"] = a["schedule_s"] / b["schedule_s"]
+        out["dE_rel"] = abs(a["energy"] - b["energy"]) / abs(a["energy"])
+    return out
+
+
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
@@ -295,10 +330,8 @@ def main():
     clocks.start()
     dev_s, _ = time_matvecs(torch, ctx, stream, xs, ys, flush, args.steps, args.warmup)
     ck = clocks.stop()
-    if world > 1:
-        t = torch.tensor([dev_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_s = float(t.item())
+    from dmrg_b200 import replicas
+    dev_s = replicas.max_over_ranks(dev_s, dev)
     per = dev_s / args.steps
     value = world * args.steps / dev_s
     y_main = ys.cpu().numpy()
@@ -328,11 +361,7 @@ def main():
     t0 = time.perf_counter()
     for _ in range(args.steps):
         yh = ctx.av(xh)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dev)
 
     if rank == 0:
         peaks, src = measured_peaks()
@@ -351,6 +380,7 @@ def main():
             peak_note = f"half the bf16_tflops of MEASURED_PEAKS.json ({src}): TF32 runs at half the BF16 rate"
             kernel = "grouped_split_tc<tf32> (stage 1 + stage 2 launches)"
         cpu = cpu_reference_rate(args.cpu_sample_s, w)
+        sweep = sweep_compare(native, args) if args.sweep else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
@@ -373,6 +403,8 @@ def main():
             "gpu_launches": (2 if args.prec == "fp64" else 3) * args.steps,
             "clocks": ck,
         }
+        if sweep is not None:
+            line["sweep"] = sweep
         if fp64 is not None:
             line["fp64_path"] = fp64
             line["split_vs_fp64"] = value / fp64["value"]

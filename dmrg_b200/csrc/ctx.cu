@@ -661,16 +661,14 @@ int dmrgx_av(dmrgx_ctx* c, const void* in, void* out, int mem) {
   const size_t bytes = sizeof(double) * (size_t)c->n * c->f();
   if (mem == DMRGX_MEM_DEVICE) return run_matvec(c, (const double*)in, (double*)out);
   ARG_CHECK(mem == DMRGX_MEM_HOST, "av: mem must be DMRGX_MEM_HOST or DMRGX_MEM_DEVICE");
-  std::memcpy(c->h_in, in, bytes);
-  CUDA_TRY(cudaMemcpyAsync(c->din.p, c->h_in, bytes, cudaMemcpyHostToDevice, c->stream));
+  // host arrays: the driver stages pageable copies itself (pipelined), which
+  // beats a serial memcpy through our own pinned buffers
+  CUDA_TRY(cudaMemcpyAsync(c->din.p, in, bytes, cudaMemcpyHostToDevice, c->stream));
   int rc = run_matvec(c, (const double*)c->din.p, (double*)c->dout.p);
   if (rc) return rc;
-  CUDA_TRY(cudaMemcpyAsync(c->h_out, c->dout.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(out, c->dout.p, bytes, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
-  rc = check_device_error(c);
-  if (rc) return rc;
-  std::memcpy(out, c->h_out, bytes);
-  return 0;
+  return check_device_error(c);
 }
 
 int dmrgx_profile(dmrgx_ctx* c, int enable) {

@@ -235,6 +235,11 @@ bool load_solver(std::string& err) {
 
 }  // namespace
 
+cudaError_t qt_grouped_gemm(const Engine& E, const double* A, const double* B, double* C,
+                            std::vector<DOut>& outs, std::vector<DSeg>& segs) {
+  return run_gemms(E, A, B, C, outs, segs);
+}
+
 cudaError_t launch_gather(const double* src, double* dst, const std::vector<GOut>& outs,
                           const std::vector<GSrc>& srcs, bool cplx, cudaStream_t st) {
   if (outs.empty()) return cudaSuccess;
@@ -308,6 +313,46 @@ QTPtr qt_copy(const Engine& E, const QTensor& A) {
 }
 
 // ------------------------------------------------------------------ contract(A, a, B, b)
+// Block pairs of contract(A, a, B, b, change, fermion) with their fermion signs
+// (src/qtensor.cpp:930-968): A block l meets B block r when the labels of the
+// contracted legs agree; output labels in the leg order A[0..a), B[0..b),
+// B(b..], A(a..].
+std::vector<FusePair> fuse_pairs(const Group& G, const QMeta& A, int a, const QMeta& B, int b,
+                                 bool change) {
+  const int na = A.nleg(), nb = B.nleg();
+  std::vector<FusePair> out;
+  for (size_t l = 0; l < A.syms.size(); l++)
+    for (size_t r = 0; r < B.syms.size(); r++) {
+      const auto& sa = A.syms[l];
+      const auto& sb = B.syms[r];
+      if (sa[a] != sb[b]) continue;
+      FusePair p;
+      p.l = (int)l;
+      p.r = (int)r;
+      for (int i = 0; i < a; i++) p.sym.push_back(sa[i]);
+      for (int j = 0; j < b; j++) p.sym.push_back(sb[j]);
+      for (int j = b + 1; j < nb; j++) p.sym.push_back(sb[j]);
+      for (int i = a + 1; i < na; i++) p.sym.push_back(sa[i]);
+      int sign = 1;
+      if (change) {
+        int d_a = 0, b_p = 0;
+        for (int i = 0; i < na; i++) d_a = G.ss(d_a, sa[i] * A.dirs[i]);
+        for (int i = 0; i < nb; i++)
+          if (B.dirs[i] == 1) b_p = G.ss(b_p, sb[i]);
+        sign = G.sign(d_a, b_p);
+      } else {
+        int d_b = 0, a_p = 0;
+        for (int i = 0; i < nb; i++) d_b = G.ss(d_b, sb[i] * B.dirs[i]);
+        for (int i = 0; i < na; i++)
+          if (A.dirs[i] == 1) a_p = G.ss(a_p, sa[i]);
+        sign = G.sign(d_b, a_p);
+      }
+      p.sign = (double)sign;
+      out.push_back(std::move(p));
+    }
+  return out;
+}
+
 QTPtr qt_contract_legs(const Engine& E, const QTensor& A, int a, const QTensor& B, int b,
                        bool change, int ex0, int ex1, std::string& err) {
   const Group& G = E.G;
@@ -333,39 +378,19 @@ QTPtr qt_contract_legs(const Engine& E, const QTensor& A, int a, const QTensor& 
   struct Pair { int l, r, out; double sign; };
   std::vector<Pair> pairs;
   std::map<int64_t, int> key2out;
-  for (size_t l = 0; l < A.m.syms.size(); l++)
-    for (size_t r = 0; r < B.m.syms.size(); r++) {
-      const auto& sa = A.m.syms[l];
-      const auto& sb = B.m.syms[r];
-      if (sa[a] != sb[b]) continue;
-      std::vector<int> sym;
-      for (int c : legsrc) sym.push_back(c >= 0 ? sa[c] : sb[-c - 1]);
-      int sign = 1;
-      if (change) {
-        int d_a = 0, b_p = 0;
-        for (int i = 0; i < na; i++) d_a = G.ss(d_a, sa[i] * A.m.dirs[i]);
-        for (int i = 0; i < nb; i++)
-          if (B.m.dirs[i] == 1) b_p = G.ss(b_p, sb[i]);
-        sign = G.sign(d_a, b_p);
-      } else {
-        int d_b = 0, a_p = 0;
-        for (int i = 0; i < nb; i++) d_b = G.ss(d_b, sb[i] * B.m.dirs[i]);
-        for (int i = 0; i < na; i++)
-          if (A.m.dirs[i] == 1) a_p = G.ss(a_p, sa[i]);
-        sign = G.sign(d_b, a_p);
-      }
-      const int64_t key = label_key(sym, M.dims);
-      auto it = key2out.find(key);
-      int o;
-      if (it == key2out.end()) {
-        o = (int)M.syms.size();
-        key2out[key] = o;
-        M.syms.push_back(sym);
-      } else {
-        o = it->second;
-      }
-      pairs.push_back({(int)l, (int)r, o, (double)sign});
+  for (auto& fp : fuse_pairs(G, A.m, a, B.m, b, change)) {
+    const int64_t key = label_key(fp.sym, M.dims);
+    auto it = key2out.find(key);
+    int o;
+    if (it == key2out.end()) {
+      o = (int)M.syms.size();
+      key2out[key] = o;
+      M.syms.push_back(fp.sym);
+    } else {
+      o = it->second;
     }
+    pairs.push_back({fp.l, fp.r, o, fp.sign});
+  }
   if (T->alloc(E.stream) != cudaSuccess) {
     err = "contract: allocation failed";
     return nullptr;

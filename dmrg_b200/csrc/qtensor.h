@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 
+#include "grouped.h"
 #include "qmeta.h"
 
 namespace dmrgx {
@@ -60,6 +61,22 @@ struct Engine {
   Group G;
   int f = 1;
 };
+
+// Block pairs of the reference's contract(A, a, B, b, change, fermion)
+// (src/qtensor.cpp:902-983) with their fermion signs; sym = output labels before
+// any exchange (legs A[0..a), B[0..b), B(b..], A(a..]).
+struct FusePair {
+  int l, r;
+  double sign;
+  std::vector<int> sym;
+};
+std::vector<FusePair> fuse_pairs(const Group& G, const QMeta& A, int a, const QMeta& B, int b,
+                                 bool change);
+
+// C_o = sum_s A_s B_s^T over grouped descriptors (FP64 / complex, see grouped.h);
+// synchronous on E.stream
+cudaError_t qt_grouped_gemm(const Engine& E, const double* A, const double* B, double* C,
+                            std::vector<DOut>& outs, std::vector<DSeg>& segs);
 
 QTPtr qt_from_host(const Engine& E, const int* meta, const void* vals, std::string& err);
 int qt_to_host(const QTensor& T, std::vector<int>& meta, std::vector<double>& vals,
