@@ -365,6 +365,14 @@ int run_matvec_fp64(dmrgx_ctx* c, const double* in, double* out) {
 }  // namespace
 
 namespace dmrgx {
+int matvec_fp64(dmrgx_ctx* c, const double* in, double* out) {
+  if (!c->has_plan) {
+    set_error("matvec: no plan");
+    return DMRGX_E_STATE;
+  }
+  return run_matvec_fp64(c, in, out);
+}
+
 // Plan from device tensors (the site step): same bookkeeping as
 // dmrgx_plan_build, environment images gathered on the device.
 int plan_build_device(dmrgx_ctx* c, const QTensor& L, const QTensor& R, int l_num, int r_num,
@@ -436,6 +444,8 @@ void dmrgx_ctx_destroy(dmrgx_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  if (c->run_free) c->run_free(c->run);
+  c->run = nullptr;
   c->st1.free_device();
   c->st2.free_device();
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);

@@ -95,5 +95,8 @@ struct dmrgx_ctx {
   double* h_out = nullptr;
   size_t h_cap = 0;
 
+  void* run = nullptr;                          // state of the last dmrgx_dmrg (MPS, centre)
+  void (*run_free)(void*) = nullptr;
+
   int f() const { return dtype == 1 ? 2 : 1; }  // doubles per element
 };

@@ -12,10 +12,12 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
 #include "../../include/dmrgx.h"
+#include "adjoint.h"
 #include "ctx.h"
 #include "qtensor.h"
 
@@ -115,6 +117,9 @@ HostQT exchange(const HostQT& A, int a, int b) {
 //        3 XYZ(jx, jy, jz) with a real MPO: sigma_y (x) sigma_y = -(i sigma_y) (x)
 //          (i sigma_y) and i sigma_y = [[0, 1], [-1, 0]] is real, so the reference's
 //          complex XYZ MPO becomes real with the same spectrum
+// XYZ (1 and 3) take an optional fourth parameter h, a field h sum_i sigma^z_i in
+// the on-site slot W[D-1, s, 0, s]; the reference has no field, and at h = 0 the
+// MPO is the reference's entry for entry.
 bool build_mpo(int model, const double* par, HostQT& W) {
   W = HostQT();
   const cplx I(0, 1);
@@ -133,31 +138,35 @@ bool build_mpo(int model, const double* par, HostQT& W) {
     return true;
   }
   if (model == 1) {
-    const double jx = par[0], jy = par[1], jz = par[2];
+    const double jx = par[0], jy = par[1], jz = par[2], h = par[3];
     W.m.dims = {{5}, {1, 1}, {5}, {1, 1}};
     W.m.dirs = {0, 0, 0, 0};
     W.add_block({0, 0, 0, 0}, {5, 1, 5, 1});
     W.set(5, 0, 0, 1); W.set(5, 3, 0, 1); W.set(5, 4, 3, jz); W.set(5, 4, 4, 1);
+    W.set(5, 4, 0, h);
     W.add_block({0, 0, 0, 1}, {5, 1, 5, 1});
     W.set(5, 1, 0, 1); W.set(5, 2, 0, -I); W.set(5, 4, 1, jx); W.set(5, 4, 2, -I * jy);
     W.add_block({0, 1, 0, 0}, {5, 1, 5, 1});
     W.set(5, 1, 0, 1); W.set(5, 2, 0, I); W.set(5, 4, 1, jx); W.set(5, 4, 2, I * jy);
     W.add_block({0, 1, 0, 1}, {5, 1, 5, 1});
     W.set(5, 0, 0, 1); W.set(5, 3, 0, -1); W.set(5, 4, 3, -jz); W.set(5, 4, 4, 1);
+    W.set(5, 4, 0, -h);
     return true;
   }
   if (model == 3) {
-    const double jx = par[0], jy = par[1], jz = par[2];
+    const double jx = par[0], jy = par[1], jz = par[2], h = par[3];
     W.m.dims = {{5}, {1, 1}, {5}, {1, 1}};
     W.m.dirs = {0, 0, 0, 0};
     W.add_block({0, 0, 0, 0}, {5, 1, 5, 1});
     W.set(5, 0, 0, 1); W.set(5, 3, 0, 1); W.set(5, 4, 3, jz); W.set(5, 4, 4, 1);
+    W.set(5, 4, 0, h);
     W.add_block({0, 0, 0, 1}, {5, 1, 5, 1});
     W.set(5, 1, 0, 1); W.set(5, 2, 0, 1); W.set(5, 4, 1, jx); W.set(5, 4, 2, -jy);
     W.add_block({0, 1, 0, 0}, {5, 1, 5, 1});
     W.set(5, 1, 0, 1); W.set(5, 2, 0, -1); W.set(5, 4, 1, jx); W.set(5, 4, 2, jy);
     W.add_block({0, 1, 0, 1}, {5, 1, 5, 1});
     W.set(5, 0, 0, 1); W.set(5, 3, 0, -1); W.set(5, 4, 3, -jz); W.set(5, 4, 4, 1);
+    W.set(5, 4, 0, -h);
     return true;
   }
   if (model == 2) {
@@ -213,7 +222,15 @@ struct Run {
   int L;
   QTPtr bulk, ledge, redge;  // mpo[i], mpo[0], mpo[L-1]
   std::vector<QTPtr> env;    // mps(i): block environments
+  std::vector<QTPtr> site;   // mps[i]: U (left of the centre) or V (right of it)
   int sector;
+  int m_cut = 0;             // bond cutoff of the sweeps
+  // one-site centre of the state after the last step: psi[b_{c-1}, s_c, b_{c+1}]
+  // (left legs absent at c = 0, right ones at c = L-1)
+  int center = -1;
+  QTPtr cpsi;
+  int model = 0;
+  std::vector<double> par;   // model parameters of the MPO in use
   // per-step records
   std::vector<int> lr;
   std::vector<double> energies, trunc;
@@ -326,6 +343,9 @@ struct Run {
     if ((rc = svd(*psi, 1, cutoff, U, V))) return rc;
     env[l] = left_update(le, *U, 1);
     env[r] = right_update(re, *V, 1);
+    site[l] = U;
+    site[r] = V;
+    center = -1;
     return env[l] && env[r] ? 0 : DMRGX_E_CUDA;
   }
   // src/core.cpp:182-283
@@ -339,6 +359,9 @@ struct Run {
     if ((rc = svd(*psi, 2, cutoff, U, V))) return rc;
     env[l] = left_update(*le, *U, 2);
     env[r] = right_update(*re, *V, 2);
+    site[l] = U;
+    site[r] = V;
+    center = -1;
     return env[l] && env[r] ? 0 : DMRGX_E_CUDA;
   }
   // src/core.cpp:293-378
@@ -351,6 +374,9 @@ struct Run {
     if ((rc = solve(l, r, psi))) return rc;
     if ((rc = svd(*psi, 2, cutoff, U, V))) return rc;
     env[l] = left_update(*le, *U, 2);
+    site[l] = U;
+    center = l;  // psi[a_{l-1}, s_l, b_r]: centre at l, right block from r = l + 1
+    cpsi = psi;
     return env[l] ? 0 : DMRGX_E_CUDA;
   }
   // src/core.cpp:388-474
@@ -363,11 +389,295 @@ struct Run {
     if ((rc = solve(l, r, psi))) return rc;
     if ((rc = svd(*psi, 1, cutoff, U, V))) return rc;
     env[r] = right_update(*re, *V, 2);
+    site[r] = V;
+    center = r;  // psi[b_l, s_r, a_{r+1}]: centre at r, left block through l = r - 1
+    cpsi = psi;
     return env[r] ? 0 : DMRGX_E_CUDA;
   }
   int fail(int rc) {
     err = std::string("plan: ") + dmrgx_last_error();
     return rc;
+  }
+
+  // ------------------------------------------------------------ state after the sweeps
+  QTPtr fuse_left_of(const QTensor& e, const QTensor& W) {
+    return qt_contract_legs(E, e, 1, W, 0, false, 3, 4, err);
+  }
+  QTPtr fuse_right_of(const QTensor& e, const QTensor& W) {
+    QTPtr ope = qt_exchange(E, W, 0, 2, err);
+    if (!ope) return nullptr;
+    return qt_contract_legs(E, e, 1, *ope, 0, true, 0, 1, err);
+  }
+
+  // Plan operands of the one-site centre c: the move2right form
+  // (L~_c or the left edge, right block c+1) for c < L-1, and
+  // (left block L-2, right edge) at c = L-1.
+  struct Form {
+    QTPtr lop, rop;
+    int ln = 0, rn = 0;
+  };
+  int form_at(int cc, const QTPtr& W, const QTPtr& le, const QTPtr& re,
+              const std::vector<QTPtr>& ev, Form& F) {
+    if (cc < L - 1) {
+      F.lop = cc == 0 ? le : (ev[cc - 1] ? fuse_left_of(*ev[cc - 1], *W) : nullptr);
+      F.rop = ev[cc + 1];
+      F.ln = cc == 0 ? 2 : 3;
+      F.rn = 1;
+    } else {
+      F.lop = ev[L - 2];
+      F.rop = re;
+      F.ln = 2;
+      F.rn = 1;
+    }
+    if (!F.lop || !F.rop) {
+      if (err.empty()) err = "an environment of the centre is missing";
+      return DMRGX_E_STATE;
+    }
+    return 0;
+  }
+
+  // centre tensor (any block order) -> the current plan's packed psi layout
+  int to_plan(const QTensor& psi, double* dst) {
+    const int f = c->f();
+    if (psi.m.nleg() != (int)c->psi_dim.size()) {
+      err = "centre tensor and plan disagree on the number of legs";
+      return DMRGX_E_STATE;
+    }
+    std::map<std::vector<int>, int> at;
+    for (size_t b = 0; b < psi.m.syms.size(); b++) at[psi.m.syms[b]] = (int)b;
+    std::vector<GOut> go;
+    std::vector<GSrc> gs;
+    int64_t off = 0;
+    for (auto& sym : c->psi_sym) {
+      int64_t sz = 1;
+      for (size_t l = 0; l < sym.size(); l++) sz *= c->psi_dim[l][sym[l]];
+      auto it = at.find(sym);
+      if (it != at.end() && sz > 0) {
+        if (psi.bsize(it->second) != sz) {
+          err = "centre block size differs from the plan's";
+          return DMRGX_E_STATE;
+        }
+        GSrc g;
+        std::memset(&g, 0, sizeof(g));
+        g.src_off = psi.off[it->second];
+        g.strides[0] = 1;
+        g.sign = 1.0;
+        gs.push_back(g);
+        GOut o;
+        std::memset(&o, 0, sizeof(o));
+        o.dst_off = off;
+        o.size = sz;
+        o.rank = 1;
+        o.dims[0] = (int32_t)sz;
+        o.dst_strides[0] = 1;
+        o.src_begin = (int32_t)gs.size() - 1;
+        o.src_count = 1;
+        go.push_back(o);
+      }
+      off += sz;
+    }
+    if (off != c->n) {
+      err = "plan layout size mismatch";
+      return DMRGX_E_STATE;
+    }
+    if (cudaMemsetAsync(dst, 0, sizeof(double) * std::max<int64_t>(1, c->n * f), E.stream) !=
+            cudaSuccess ||
+        launch_gather(psi.d, dst, go, gs, f == 2, E.stream) != cudaSuccess) {
+      err = "centre relayout failed";
+      return DMRGX_E_CUDA;
+    }
+    return 0;
+  }
+
+  // <psi|H|psi> / <psi|psi> at the centre with the given operators, and the
+  // adjoints of the centre's Lop / Rop when asked
+  int eval_center(const QTPtr& W, const QTPtr& le, const QTPtr& re, const std::vector<QTPtr>& ev,
+                  bool want_l, bool want_r, Form& F, QTPtr& gl, QTPtr& gr, double& en,
+                  double& nn) {
+    int rc = form_at(center, W, le, re, ev, F);
+    if (rc) return rc;
+    rc = plan_build_device(c, *F.lop, *F.rop, F.ln, F.rn, sector, E.G);
+    if (rc) return fail(rc);
+    double* d = nullptr;
+    if (cudaMalloc(&d, sizeof(double) * std::max<int64_t>(1, c->n * c->f())) != cudaSuccess) {
+      err = "centre allocation failed";
+      return DMRGX_E_CUDA;
+    }
+    rc = to_plan(*cpsi, d);
+    if (!rc) rc = heff_adjoint(c, E, *F.lop, *F.rop, d, want_l, want_r, gl, gr, en, nn, err);
+    cudaFree(d);
+    return rc;
+  }
+
+  // SVD of the centre that drops no weight above the sweeps' cutoff
+  int center_svd(int num, QTPtr& U, QTPtr& V, double& disc) {
+    std::vector<double> s;
+    if (qt_svd(E, *cpsi, num, m_cut, U, V, s, err)) return DMRGX_E_CUDA;
+    disc = 0;
+    for (size_t i = (size_t)std::min<int64_t>(m_cut, (int64_t)s.size()); i < s.size(); i++)
+      disc += s[i] * s[i];
+    return 0;
+  }
+
+  // move the one-site centre without changing the state: psi = U S V,
+  // new site tensor, environment update, psi' = A_{c-1} (psi V^+)  or  (U^+ psi) B_{c+1}
+  int move_left(double& disc) {
+    const int c0 = center;
+    const int nr = c0 == L - 1 ? 1 : 2;
+    QTPtr U, V;
+    int rc = center_svd(1, U, V, disc);
+    if (rc) return rc;
+    QTPtr rt = c0 == L - 1 ? redge : fuse_right_of(*env[c0 + 1], *bulk);
+    if (!rt) return DMRGX_E_CUDA;
+    env[c0] = right_update(*rt, *V, nr);
+    site[c0] = V;
+    auto Vc = qt_copy(E, *V);
+    if (!Vc || qt_conjugate(E, *Vc)) return DMRGX_E_CUDA;
+    QTPtr us = qt_contract_mat(E, *cpsi, *Vc, 'N', 'T', nr, err);
+    if (!us || !env[c0]) return DMRGX_E_CUDA;
+    QTPtr nxt = qt_contract_mat(E, *site[c0 - 1], *us, 'N', 'N', 1, err);
+    if (!nxt) return DMRGX_E_CUDA;
+    nxt->m.dirs.assign(nxt->m.nleg(), 0);
+    cpsi = nxt;
+    center = c0 - 1;
+    return 0;
+  }
+  int move_right(double& disc, QTPtr lt) {
+    const int c0 = center;
+    const int nl = c0 == 0 ? 1 : 2;
+    QTPtr U, V;
+    int rc = center_svd(nl, U, V, disc);
+    if (rc) return rc;
+    if (!lt) lt = c0 == 0 ? ledge : fuse_left_of(*env[c0 - 1], *bulk);
+    if (!lt) return DMRGX_E_CUDA;
+    env[c0] = left_update(*lt, *U, nl);
+    site[c0] = U;
+    auto Uc = qt_copy(E, *U);
+    if (!Uc || qt_conjugate(E, *Uc)) return DMRGX_E_CUDA;
+    QTPtr sv = qt_contract_mat(E, *Uc, *cpsi, 'T', 'N', nl, err);
+    if (!sv || !env[c0]) return DMRGX_E_CUDA;
+    QTPtr nxt = qt_contract_mat(E, *sv, *site[c0 + 1], 'N', 'N', 1, err);
+    if (!nxt) return DMRGX_E_CUDA;
+    nxt->m.dirs.assign(nxt->m.nleg(), 0);
+    cpsi = nxt;
+    center = c0 + 1;
+    return 0;
+  }
+
+  // environments of the centre rebuilt from the site tensors alone (the MPS),
+  // for the MPO (W, le, re): left blocks 0..c-1, right blocks c+1..L-1
+  int rebuild(const QTPtr& W, const QTPtr& le, const QTPtr& re, std::vector<QTPtr>& ev) {
+    ev.assign(L, nullptr);
+    const int cc = center;
+    for (int k = 0; k < cc; k++) {
+      if (!site[k]) {
+        err = "site tensor missing";
+        return DMRGX_E_STATE;
+      }
+      if (k == 0) {
+        ev[0] = left_update(*le, *site[0], 1);
+      } else {
+        QTPtr lt = fuse_left_of(*ev[k - 1], *W);
+        if (!lt) return DMRGX_E_CUDA;
+        ev[k] = left_update(*lt, *site[k], 2);
+      }
+      if (!ev[k]) return DMRGX_E_CUDA;
+    }
+    for (int k = L - 1; k > cc; k--) {
+      if (!site[k]) {
+        err = "site tensor missing";
+        return DMRGX_E_STATE;
+      }
+      if (k == L - 1) {
+        ev[k] = right_update(*re, *site[k], 1);
+      } else {
+        QTPtr rt = fuse_right_of(*ev[k + 1], *W);
+        if (!rt) return DMRGX_E_CUDA;
+        ev[k] = right_update(*rt, *site[k], 2);
+      }
+      if (!ev[k]) return DMRGX_E_CUDA;
+    }
+    return 0;
+  }
+
+  // dE/dW_k for every site k by the adjoint of the centre's H_eff contraction:
+  // the centre walks to the left edge, then across the chain; at each site the
+  // MPO tensor sits in the centre's Lop (left edge, fused L~) or Rop (right edge).
+  // gw[k]: the bulk MPO layout (edge gradients land in row D-1 / column 0).
+  // checks: [0] final eigenvalue E0, [1] max |<psi|H|psi> - E0| over the centres,
+  // [2] max_k |<dE/dW_k, W_k> - E0| (E is linear in each W_k), [3] max discarded weight.
+  int adjoint(bool recompute, const std::vector<double>& w_host,
+              std::vector<std::vector<double>>& gw, double* checks) {
+    if (center < 0 || !cpsi) {
+      err = "adjoint: the last step left no one-site centre (the schedule must end with a move)";
+      return DMRGX_E_STATE;
+    }
+    const int f = c->f();
+    const double e0 = energies.empty() ? 0.0 : energies[energies.size() - 6];
+    double edev = 0, wdev = 0, disc = 0;
+    int rc;
+    if (recompute) {
+      std::vector<QTPtr> ev;
+      for (auto& e : env) e.reset();  // drop the stored environments first
+      if ((rc = rebuild(bulk, ledge, redge, ev))) return rc;
+      env = ev;
+    }
+    gw.assign(L, std::vector<double>((size_t)(bulk->total() * f), 0.0));
+    Form F;
+    QTPtr gl, gr;
+    double en = 0, nn = 1, d = 0;
+    if ((rc = eval_center(bulk, ledge, redge, env, false, false, F, gl, gr, en, nn))) return rc;
+    edev = std::fabs(en - e0);
+    while (center > 0) {
+      if ((rc = move_left(d))) return rc;
+      disc = std::max(disc, d);
+      if (center > 0) {
+        if ((rc = eval_center(bulk, ledge, redge, env, false, false, F, gl, gr, en, nn))) return rc;
+        edev = std::max(edev, std::fabs(en - e0));
+      }
+    }
+    for (;;) {
+      const int cc = center;
+      const bool last = cc == L - 1;
+      if ((rc = eval_center(bulk, ledge, redge, env, !last, last, F, gl, gr, en, nn))) return rc;
+      edev = std::max(edev, std::fabs(en - e0));
+      if (last) rc = edge_adjoint(*gr, *bulk, true, gw[cc], E.stream, err);
+      else if (cc == 0) rc = edge_adjoint(*gl, *bulk, false, gw[cc], E.stream, err);
+      else rc = fusion_adjoint(E, *env[cc - 1], *bulk, *gl, false, gw[cc], err);
+      if (rc) return rc;
+      for (auto& v : gw[cc]) v /= nn;
+      // <dE/dW_k, W_k> = E
+      double sr = 0;
+      for (size_t w = 0; w < w_host.size() / f; w++)
+        sr += f == 2 ? gw[cc][2 * w] * w_host[2 * w] - gw[cc][2 * w + 1] * w_host[2 * w + 1]
+                     : gw[cc][w] * w_host[w];
+      wdev = std::max(wdev, std::fabs(sr - e0));
+      if (last) break;
+      if ((rc = move_right(d, cc == 0 ? ledge : F.lop))) return rc;
+      disc = std::max(disc, d);
+    }
+    if (checks) {
+      checks[0] = e0;
+      checks[1] = edev;
+      checks[2] = wdev;
+      checks[3] = disc;
+    }
+    return 0;
+  }
+
+  // <Psi|H(W)|Psi> of the current state for another MPO of the same shape
+  int expect(const QTPtr& W, const QTPtr& le, const QTPtr& re, double& value) {
+    if (center < 0 || !cpsi) {
+      err = "expect: no state (run dmrg first)";
+      return DMRGX_E_STATE;
+    }
+    std::vector<QTPtr> ev;
+    int rc = rebuild(W, le, re, ev);
+    if (rc) return rc;
+    Form F;
+    QTPtr gl, gr;
+    double nn = 1;
+    return eval_center(W, le, re, ev, false, false, F, gl, gr, value, nn);
   }
 
   // the reference schedule dmrg() (src/functions.cpp:157-227)
@@ -402,6 +712,37 @@ struct Run {
   }
 };
 
+int model_nparams(int model) { return model == 0 ? 3 : 4; }
+
+std::vector<double> flatten(const HostQT& W, int f) {
+  std::vector<double> v;
+  for (auto& b : W.blocks)
+    for (auto& x : b) {
+      v.push_back(x.real());
+      if (f == 2) v.push_back(x.imag());
+    }
+  return v;
+}
+
+// the three device MPO tensors of a parameter set: bulk, left edge, right edge
+// (left() = take(0, D-1), right() = take(2, 0).exchange(0, 1), src/qtensor.cpp:449-463)
+bool mpo_set(int model, const double* par, int f, cudaStream_t st, QTPtr& bulk, QTPtr& le,
+             QTPtr& re, HostQT* host, std::string& err) {
+  HostQT W;
+  if (!build_mpo(model, par, W)) {
+    err = "unknown model";
+    return false;
+  }
+  const int D = W.m.dims[0][0];
+  bulk = upload(W, f, st, err);
+  le = upload(take(W, 0, D - 1), f, st, err);
+  re = upload(exchange(take(W, 2, 0), 0, 1), f, st, err);
+  if (host) *host = W;
+  return bulk && le && re;
+}
+
+void free_run(void* p) { delete static_cast<Run*>(p); }
+
 }  // namespace
 }  // namespace dmrgx
 
@@ -415,18 +756,7 @@ extern "C" int dmrgx_dmrg(dmrgx_ctx* c, int model, int L, int m, int sweeps, int
     set_error("dmrg: bad arguments (need a context, parameters and L >= 4)");
     return DMRGX_E_ARG;
   }
-  Run R;
-  R.c = c;
-  R.L = L;
-  R.sector = sector;
-  R.E.stream = c->stream;
-  R.E.device = c->device;
-  R.E.num_sms = c->num_sms;
-  R.E.f = c->f();
-  double par[8] = {0};
-  for (int i = 0; i < nparams && i < 8; i++) par[i] = params[i];
-  HostQT W;
-  if (!build_mpo(model, par, W)) {
+  if (model < 0 || model > 3) {
     set_error("dmrg: unknown model");
     return DMRGX_E_ARG;
   }
@@ -435,47 +765,156 @@ extern "C" int dmrgx_dmrg(dmrgx_ctx* c, int model, int L, int m, int sweeps, int
     set_error("dmrg: Kitaev and real XYZ run on F64 contexts, XYZ and Potts on C128");
     return DMRGX_E_ARG;
   }
-  R.E.G.n = model == 2 ? 3 : 2;
-  R.E.G.fermion = model == 0;
-  // edges: left() = take(0, D-1), right() = take(2, 0).exchange(0, 1) (src/qtensor.cpp:449-463)
-  const int D = W.m.dims[0][0];
-  HostQT le = take(W, 0, D - 1);
-  HostQT re = exchange(take(W, 2, 0), 0, 1);
+  if (c->run_free) c->run_free(c->run);
+  c->run = nullptr;
+  c->run_free = nullptr;
+  Run* R = new Run;
+  R->c = c;
+  R->L = L;
+  R->sector = sector;
+  R->m_cut = m;
+  R->model = model;
+  R->E.stream = c->stream;
+  R->E.device = c->device;
+  R->E.num_sms = c->num_sms;
+  R->E.f = c->f();
+  R->par.assign(8, 0.0);
+  for (int i = 0; i < nparams && i < 8; i++) R->par[i] = params[i];
+  R->E.G.n = model == 2 ? 3 : 2;
+  R->E.G.fermion = model == 0;
   std::string err;
   cudaSetDevice(c->device);
-  R.bulk = upload(W, c->f(), c->stream, err);
-  R.ledge = upload(le, c->f(), c->stream, err);
-  R.redge = upload(re, c->f(), c->stream, err);
-  if (!R.bulk || !R.ledge || !R.redge) {
+  if (!mpo_set(model, R->par.data(), c->f(), c->stream, R->bulk, R->ledge, R->redge, nullptr,
+               err)) {
+    delete R;
     set_error("dmrg: " + err);
     return DMRGX_E_CUDA;
   }
-  R.env.assign(L, nullptr);
+  R->env.assign(L, nullptr);
+  R->site.assign(L, nullptr);
   const double t0 = Run::now();
-  int rc = R.dmrg(m, sweeps);
+  int rc = R->dmrg(m, sweeps);
   const double t1 = Run::now();
   if (rc) {
-    set_error("dmrg: " + R.err);
+    set_error("dmrg: " + R->err);
+    delete R;
     return rc;
   }
-  const int64_t ns = (int64_t)R.trunc.size();
+  const int64_t ns = (int64_t)R->trunc.size();
   *nsteps = ns;
   for (int64_t i = 0; i < ns && i < cap; i++) {
     if (energies)
-      for (int q = 0; q < 6; q++) energies[6 * i + q] = R.energies[6 * i + q];
-    if (trunc) trunc[i] = R.trunc[i];
+      for (int q = 0; q < 6; q++) energies[6 * i + q] = R->energies[6 * i + q];
+    if (trunc) trunc[i] = R->trunc[i];
     if (steps_lr) {
-      steps_lr[2 * i] = R.lr[2 * i];
-      steps_lr[2 * i + 1] = R.lr[2 * i + 1];
+      steps_lr[2 * i] = R->lr[2 * i];
+      steps_lr[2 * i + 1] = R->lr[2 * i + 1];
     }
-    if (matvecs) matvecs[i] = R.matvecs[i];
+    if (matvecs) matvecs[i] = R->matvecs[i];
   }
   if (seconds) {
     seconds[0] = t1 - t0;
-    seconds[1] = R.t_eig;
-    seconds[2] = R.t_svd;
-    seconds[3] = R.t_env;
-    seconds[4] = R.t_fuse;
+    seconds[1] = R->t_eig;
+    seconds[2] = R->t_svd;
+    seconds[3] = R->t_env;
+    seconds[4] = R->t_fuse;
+  }
+  c->run = R;  // the final state stays for dmrgx_adjoint / dmrgx_expect
+  c->run_free = free_run;
+  return 0;
+}
+
+extern "C" int dmrgx_adjoint(dmrgx_ctx* c, int recompute, double* dE_dparams, int nparams,
+                             double* dE_dW, int64_t w_cap, int64_t* w_len, double* checks,
+                             double* seconds) {
+  if (!c || !c->run) {
+    set_error("adjoint: no state (run dmrgx_dmrg on this context first)");
+    return DMRGX_E_STATE;
+  }
+  Run* R = static_cast<Run*>(c->run);
+  const int f = c->f();
+  const int np = model_nparams(R->model);
+  if (nparams < 0 || nparams > np) {
+    set_error("adjoint: the model has fewer parameters than asked for");
+    return DMRGX_E_ARG;
+  }
+  const int64_t wl = R->bulk->total() * f;
+  if (w_len) *w_len = wl;
+  if (dE_dW && w_cap < (int64_t)R->L * wl) {
+    set_error("adjoint: dE_dW needs L * w_len doubles");
+    return DMRGX_E_ARG;
+  }
+  cudaSetDevice(c->device);
+  HostQT W0;
+  std::string err;
+  build_mpo(R->model, R->par.data(), W0);
+  const std::vector<double> w0 = flatten(W0, f);
+  const int prec = c->prec;
+  c->prec = DMRGX_PREC_FP64;  // the adjoint runs on the FP64 plan only
+  std::vector<std::vector<double>> gw;
+  const double t0 = Run::now();
+  R->err.clear();
+  int rc = R->adjoint(recompute != 0, w0, gw, checks);
+  const double t1 = Run::now();
+  c->prec = prec;
+  if (rc) {
+    set_error("adjoint: " + R->err);
+    return rc;
+  }
+  if (dE_dW)
+    for (int k = 0; k < R->L; k++) std::copy(gw[k].begin(), gw[k].end(), dE_dW + (int64_t)k * wl);
+  // dE/dp = sum_k <dE/dW_k, dW/dp>; W is affine in every parameter but the Potts
+  // angles, which take a central difference of the MPO entries (step 1e-5)
+  for (int p = 0; p < nparams; p++) {
+    const bool affine = !(R->model == 2 && p >= 2);
+    const double h = affine ? 1.0 : 1e-5;
+    std::vector<double> pp = R->par, pm = R->par;
+    pp[p] += h;
+    if (!affine) pm[p] -= h;
+    HostQT Wp, Wm;
+    build_mpo(R->model, pp.data(), Wp);
+    build_mpo(R->model, pm.data(), Wm);
+    const std::vector<double> vp = flatten(Wp, f), vm = flatten(Wm, f);
+    const double den = affine ? h : 2 * h;
+    double acc = 0;
+    for (int k = 0; k < R->L; k++)
+      for (size_t w = 0; w < vp.size() / f; w++) {
+        if (f == 2) {
+          const double dr = (vp[2 * w] - vm[2 * w]) / den, di = (vp[2 * w + 1] - vm[2 * w + 1]) / den;
+          acc += gw[k][2 * w] * dr - gw[k][2 * w + 1] * di;
+        } else {
+          acc += gw[k][w] * (vp[w] - vm[w]) / den;
+        }
+      }
+    dE_dparams[p] = acc;
+  }
+  if (seconds) seconds[0] = t1 - t0;
+  return 0;
+}
+
+extern "C" int dmrgx_expect(dmrgx_ctx* c, const double* params, int nparams, double* value) {
+  if (!c || !c->run || !params || !value) {
+    set_error("expect: bad arguments or no state (run dmrgx_dmrg first)");
+    return DMRGX_E_ARG;
+  }
+  Run* R = static_cast<Run*>(c->run);
+  std::vector<double> par(8, 0.0);
+  for (int i = 0; i < nparams && i < 8; i++) par[i] = params[i];
+  cudaSetDevice(c->device);
+  QTPtr W, le, re;
+  std::string err;
+  if (!mpo_set(R->model, par.data(), c->f(), c->stream, W, le, re, nullptr, err)) {
+    set_error("expect: " + err);
+    return DMRGX_E_CUDA;
+  }
+  const int prec = c->prec;
+  c->prec = DMRGX_PREC_FP64;
+  R->err.clear();
+  int rc = R->expect(W, le, re, *value);
+  c->prec = prec;
+  if (rc) {
+    set_error("expect: " + R->err);
+    return rc;
   }
   return 0;
 }

@@ -391,6 +391,13 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
   int kkeep = 0, cycles = 0, corrections = 0, nconv = 0;
   double resid = 0.0;
   bool have_vec = false;  // lowest Ritz vector sits in V2[:, 0]
+  // Split precision: the Krylov operator carries the split rounding (relative
+  // ~1e-6..1e-5), so the first solve stops at that floor for all nev values and
+  // each defect-correction cycle then converges the lowest pair only, to a
+  // fraction of the current FP64 residual.  FP64: the reference's criterion.
+  const double split_floor = 1e-6;
+  double tol_cur = split ? std::max(tol, split_floor) : tol;
+  int nev_cur = nev;
 
   for (;;) {
     int mm = m;  // basis size reached this cycle
@@ -412,16 +419,17 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
       for (int b = 0; b < mm; b++) A[(size_t)a * mm + b] = Th[(size_t)a * td + b];
     jacobi_eig(A, mm, th, Z);
     const double beta_m = mm < m ? 0.0 : Th[(size_t)(m - 1) * td + m];
-    const int kev = std::min(nev, mm);
+    const int kev = std::min(nev_cur, mm);
     nconv = 0;
     for (int q = 0; q < kev; q++) {
       const double r = std::fabs(beta_m * Z[(size_t)(mm - 1) * mm + q]);
-      if (r <= tol * std::max(std::fabs(th[q]), 1e-30)) nconv++;
+      if (r <= tol_cur * std::max(std::fabs(th[q]), 1e-30)) nconv++;
       else break;
     }
     const bool stop = nconv >= kev || cycles >= maxiter || mm < m;
     if (stop) {
-      ritz.assign(th.begin(), th.begin() + kev);
+      if (corrections == 0) ritz.assign(th.begin(), th.begin() + kev);
+      else ritz[0] = th[0];
       std::vector<double> Yh(mm);
       for (int a = 0; a < mm; a++) Yh[a] = Z[(size_t)a * mm + 0];
       EIG_TRY(cudaMemcpyAsync(L.Y, Yh.data(), sizeof(double) * mm, cudaMemcpyHostToDevice, L.s));
@@ -447,6 +455,8 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
       resid = rnorm;
       if (rnorm <= tol * std::max(std::fabs(theta), 1e-30) || corrections >= 20) break;
       corrections++;
+      nev_cur = 1;
+      tol_cur = std::max(tol, 0.02 * rnorm / std::max(std::fabs(theta), 1e-30));
       // restart basis [v, r/|r|] with the exact coupling
       vscale<<<L.grid, RB, 0, L.s>>>(v, nullptr, 1.0 / std::sqrt(vv), L.V, L.len);
       vscale<<<L.grid, RB, 0, L.s>>>(L.w, nullptr, 1.0 / (rnorm * std::sqrt(vv)), L.col(L.V, 1),

@@ -175,8 +175,6 @@ cudaError_t run_gemms(const Engine& E, const double* A, const double* B, double*
 // ------------------------------------------------------------------ cuSOLVER (run-time loaded)
 struct Solver {
   bool tried = false, ok = false;
-  cusolverDnHandle_t h = nullptr;
-  gesvdjInfo_t info = nullptr;
   decltype(&cusolverDnCreate) create;
   decltype(&cusolverDnSetStream) set_stream;
   decltype(&cusolverDnCreateGesvdjInfo) create_info;
@@ -222,14 +220,28 @@ bool load_solver(std::string& err) {
   SYM(z_buf, cusolverDnZgesvdj_bufferSize);
   SYM(z_svd, cusolverDnZgesvdj);
 #undef SYM
-  if (g_sol.create(&g_sol.h) != CUSOLVER_STATUS_SUCCESS ||
-      g_sol.create_info(&g_sol.info) != CUSOLVER_STATUS_SUCCESS) {
+  g_sol.ok = true;
+  return true;
+}
+
+// one cuSOLVER handle per host thread, so contexts driven from several threads
+// run their SVDs concurrently
+struct SolverHandle {
+  cusolverDnHandle_t h = nullptr;
+  gesvdjInfo_t info = nullptr;
+};
+thread_local SolverHandle t_sol;
+
+bool thread_handle(std::string& err) {
+  if (t_sol.h) return true;
+  if (g_sol.create(&t_sol.h) != CUSOLVER_STATUS_SUCCESS ||
+      g_sol.create_info(&t_sol.info) != CUSOLVER_STATUS_SUCCESS) {
     err = "cuSOLVER initialisation failed";
+    t_sol.h = nullptr;
     return false;
   }
-  g_sol.set_tol(g_sol.info, 1e-15);
-  g_sol.set_sweeps(g_sol.info, 100);
-  g_sol.ok = true;
+  g_sol.set_tol(t_sol.info, 1e-15);
+  g_sol.set_sweeps(t_sol.info, 100);
   return true;
 }
 
@@ -812,7 +824,7 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
     err = std::string("svd: ") + cudaGetErrorString(e);
     return -1;
   }
-  if (!load_solver(err)) {
+  if (!load_solver(err) || !thread_handle(err)) {
     cudaFree(dM);
     return -1;
   }
@@ -822,8 +834,7 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
   int* dinfo = nullptr;
   cudaMalloc(&dinfo, sizeof(int));
   bool fail = false;
-  std::lock_guard<std::mutex> lk(g_sol_mu);
-  g_sol.set_stream(g_sol.h, E.stream);
+  g_sol.set_stream(t_sol.h, E.stream);
   for (int i = 0; i < ns && !fail; i++) {
     const int m = (int)Cc[i], n = (int)Rr[i];
     const int mn = std::min(m, n);
@@ -838,20 +849,20 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
     double* X = dM + moff[i] * f;
     // gesvdj overwrites its input: the sector matrices are not needed afterwards
     if (f == 1)
-      st = g_sol.d_buf(g_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, X, m, dS, Ux[i], m, Vx[i], n,
-                       &lwork, g_sol.info);
+      st = g_sol.d_buf(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, X, m, dS, Ux[i], m, Vx[i], n,
+                       &lwork, t_sol.info);
     else
-      st = g_sol.z_buf(g_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, (cuDoubleComplex*)X, m, dS,
-                       (cuDoubleComplex*)Ux[i], m, (cuDoubleComplex*)Vx[i], n, &lwork, g_sol.info);
+      st = g_sol.z_buf(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, (cuDoubleComplex*)X, m, dS,
+                       (cuDoubleComplex*)Ux[i], m, (cuDoubleComplex*)Vx[i], n, &lwork, t_sol.info);
     if (st == CUSOLVER_STATUS_SUCCESS) cudaMalloc(&work, sizeof(double) * (size_t)std::max(1, lwork) * f);
     if (st == CUSOLVER_STATUS_SUCCESS) {
       if (f == 1)
-        st = g_sol.d_svd(g_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, X, m, dS, Ux[i], m, Vx[i], n,
-                         work, lwork, dinfo, g_sol.info);
+        st = g_sol.d_svd(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, X, m, dS, Ux[i], m, Vx[i], n,
+                         work, lwork, dinfo, t_sol.info);
       else
-        st = g_sol.z_svd(g_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, (cuDoubleComplex*)X, m, dS,
+        st = g_sol.z_svd(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, (cuDoubleComplex*)X, m, dS,
                          (cuDoubleComplex*)Ux[i], m, (cuDoubleComplex*)Vx[i], n,
-                         (cuDoubleComplex*)work, lwork, dinfo, g_sol.info);
+                         (cuDoubleComplex*)work, lwork, dinfo, t_sol.info);
     }
     int hinfo = 0;
     if (st == CUSOLVER_STATUS_SUCCESS) {

@@ -66,15 +66,16 @@ namespace {
 int64_t rup(int64_t x, int64_t p) { return (x + p - 1) / p * p; }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (!fn) {
+  // resolved once, thread-safe (function-local static)
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
             cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-  }
+      return (PFN_cuTensorMapEncodeTiled_v12000)p;
+    return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+  }();
   return fn;
 }
 

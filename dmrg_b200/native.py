@@ -40,6 +40,8 @@ SIGNATURES = {
     "dmrgx_eigsolve": (_i, [_vp, _i, _i, C.c_double, _i, _vp, _dp, _vp, _i64p]),
     "dmrgx_dmrg": (_i, [_vp, _i, _i, _i, _i, _i, _dp, _i, _dp, _dp, _ip, _i64p, _i64, _i64p,
                         _dp]),
+    "dmrgx_adjoint": (_i, [_vp, _i, _dp, _i, _dp, _i64, _i64p, _dp, _dp]),
+    "dmrgx_expect": (_i, [_vp, _dp, _i, _dp]),
     "dmrgx_profile": (_i, [_vp, _i]),
     "dmrgx_profile_read": (_i, [_vp, _dp, _i]),
     "dmrgx_stream": (_vp, [_vp]),
@@ -218,8 +220,40 @@ class Context:
                                 par.size, en.ctypes.data_as(_dp), tr.ctypes.data_as(_dp),
                                 _ip(lr), _i64p(mv), cap, _i64p(ns), sec.ctypes.data_as(_dp)))
         k = int(ns[0])
+        self._L = L
+        self._nparams = 3 if code == 0 else min(4, max(3, par.size))
         return dict(lr=lr[:k], energies=en[:k], trunc=tr[:k], matvecs=mv[:k],
                     seconds=dict(total=sec[0], eig=sec[1], svd=sec[2], env=sec[3], fuse=sec[4]))
+
+    def adjoint(self, nparams=None, recompute=False, want_w=False):
+        """Gradient of the last dmrg() ground-state energy: dict with dE_dparams
+        (model parameter order), checks (E0, centre energy spread, max
+        |<dE/dW_k, W_k> - E0|, dropped weight), seconds and, with want_w, the
+        per-site dE/dW_k (L x w_len doubles, bulk MPO block layout)."""
+        npar = nparams if nparams is not None else self._nparams
+        g = np.zeros(max(1, npar))
+        chk = np.zeros(4)
+        sec = np.zeros(1)
+        wl = np.zeros(1, np.int64)
+        _check(lib().dmrgx_adjoint(self.ptr, 1 if recompute else 0, g.ctypes.data_as(_dp), npar,
+                                   None, 0, _i64p(wl), chk.ctypes.data_as(_dp),
+                                   sec.ctypes.data_as(_dp)))
+        out = dict(dE_dparams=g[:npar].copy(), checks=chk, seconds=float(sec[0]))
+        if want_w:
+            # a second sweep with the tensor output (the centre ends at the right edge)
+            w = np.zeros((self._L, int(wl[0])))
+            _check(lib().dmrgx_adjoint(self.ptr, 0, g.ctypes.data_as(_dp), npar,
+                                       w.ctypes.data_as(_dp), w.size, _i64p(wl), None, None))
+            out["dE_dW"] = w
+        return out
+
+    def expect(self, params):
+        """<Psi|H(params)|Psi> of the last dmrg() state for the same model."""
+        par = np.ascontiguousarray(params, np.float64)
+        v = np.zeros(1)
+        _check(lib().dmrgx_expect(self.ptr, par.ctypes.data_as(_dp), par.size,
+                                  v.ctypes.data_as(_dp)))
+        return float(v[0])
 
     def profile(self, enable: bool):
         _check(lib().dmrgx_profile(self.ptr, 1 if enable else 0))

@@ -173,6 +173,41 @@ int dmrgx_eigsolve(dmrgx_ctx* ctx, int nev, int ncv, double tol, int maxiter, co
 int dmrgx_dmrg(dmrgx_ctx* ctx, int model, int L, int m, int sweeps, int sector,
                const double* params, int nparams, double* energies, double* trunc, int* steps_lr,
                int64_t* matvecs, int64_t cap, int64_t* nsteps, double* seconds);
+/* XYZ (models 1 and 3) accept a fourth parameter h: a field h sum_i sigma^z_i,
+ * absent from the reference (nparams = 3, or h = 0, is the reference's MPO).
+ * The final state of dmrgx_dmrg (MPS site tensors, environments and the one-site
+ * centre of the last step) stays in the context for the two calls below. */
+
+/* Gradient of the ground-state energy of the last dmrgx_dmrg with respect to the
+ * MPO tensors and the model parameters, by adjoint contractions of the
+ * effective Hamiltonian.  New work: the reference has no derivatives; it
+ * replaces the finite differences a reference user would take over whole runs
+ * (src/functions.cpp:157-227 per parameter value).  The centre walks to the left
+ * edge and across the chain without changing the state; at each site k
+ *   dE/dW_k = adjoint of <psi| Lop (x) (Rop (x) psi)> w.r.t. the operator that
+ *             holds W_k, pulled back through the env (x) MPO fusion
+ *             (src/core.cpp:188-192) with the reference's fermion signs.
+ * FP64 throughout.  recompute=1 drops the stored environments and rebuilds them
+ * from the MPS site tensors first.
+ *   dE_dparams  nparams values (model parameter order of dmrgx_dmrg, nparams <=
+ *               3 Kitaev, 4 XYZ (jx, jy, jz, h) and Potts)
+ *   dE_dW       NULL or L * w_len doubles: per site, dE/dW_k in the bulk MPO's
+ *               block layout (edge sites land in row D-1 / column 0)
+ *   w_len       NULL or: doubles per site (MPO elements x 1 real / 2 complex)
+ *   checks      NULL or 4 slots: E0 of the last step, max |<psi|H|psi> - E0| over
+ *               the centres visited, max_k |<dE/dW_k, W_k> - E0| (E is linear in
+ *               each W_k), max weight dropped by the centre moves
+ *   seconds     NULL or 1 slot: wall time of the adjoint sweep */
+int dmrgx_adjoint(dmrgx_ctx* ctx, int recompute, double* dE_dparams, int nparams,
+                  double* dE_dW, int64_t w_cap, int64_t* w_len, double* checks,
+                  double* seconds);
+
+/* <Psi|H(params)|Psi> of the current state of the last dmrgx_dmrg for the same
+ * model with other parameters (the reference's calc(mps, mpo),
+ * src/functions.cpp:469-511, on the device): environments rebuilt from the MPS
+ * site tensors with the new MPO, closed at the centre.  For a Hamiltonian linear
+ * in its couplings, params = e_p gives the Hellmann-Feynman value dE/dp. */
+int dmrgx_expect(dmrgx_ctx* ctx, const double* params, int nparams, double* value);
 
 /* Per-launch device timing of the matvec, for roofline measurements: CUDA
  * events recorded on the context's stream around each launch of every matvec
