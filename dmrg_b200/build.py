@@ -18,7 +18,7 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libdmrgx.so")
 
-SOURCES = ["qmeta.cpp", "ctx.cu", "gemm_f64.cu", "noalloc.cu", "split.cu", "tc_gemm.cu", "split_plan.cu", "eig.cu", "qtensor.cu", "adjoint.cu", "dmrg.cu"]
+SOURCES = ["qmeta.cpp", "ctx.cu", "gemm_f64.cu", "noalloc.cu", "split.cu", "tc_gemm.cu", "split_plan.cu", "eig.cu", "qtensor.cu", "adjoint.cu", "plain.cu", "dmrg.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

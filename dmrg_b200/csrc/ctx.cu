@@ -18,6 +18,8 @@ namespace dmrgx {
 
 int build_split_plan(dmrgx_ctx* c, int eb);
 int run_matvec_split(dmrgx_ctx* c, const double* in, double* out);
+int run_matvec_plain(dmrgx_ctx* c, const double* in, double* out);
+void plain_release(dmrgx_ctx* c);
 
 static thread_local std::string g_err;
 void set_error(const std::string& msg) { g_err = msg; }
@@ -130,6 +132,7 @@ std::string build_stage(const std::vector<MapRow>& rows, const std::vector<int64
   st.outs.clear();
   st.segs.clear();
   st.tiles.clear();
+  st.rows.clear();
   std::map<int64_t, int> by_off;  // output offset -> out index
   std::vector<std::vector<DSeg>> per_out;
   for (auto& r : rows) {
@@ -165,6 +168,9 @@ std::string build_stage(const std::vector<MapRow>& rows, const std::vector<int64
     }
     DSeg sg;
     sg.a_off = r.alpha >= 0 ? im.plus[r.blk] : im.minus[r.blk];
+    // the image holds the block with the row's sign applied, so alpha is +1
+    st.rows.push_back({sg.a_off, r.in_beg * f, r.out_beg * f, (int32_t)M, (int32_t)N,
+                       (int32_t)K, 1});
     sg.b_off = r.in_beg * f;
     sg.k = (int32_t)(K * f);
     sg.pad_ = 0;
@@ -324,6 +330,7 @@ int run_matvec_fp64(dmrgx_ctx* c, const double* in, double* out);
 
 int run_matvec(dmrgx_ctx* c, const double* in, double* out) {
   if (c->prec != DMRGX_PREC_FP64) return run_matvec_split(c, in, out);
+  if (c->per_block) return run_matvec_plain(c, in, out);
   return run_matvec_fp64(c, in, out);
 }
 
@@ -403,6 +410,7 @@ int plan_build_device(dmrgx_ctx* c, const QTensor& L, const QTensor& R, int l_nu
 
 // the context's matvec (fp64=false) or its FP64 form regardless of precision
 int run_matvec_any(dmrgx_ctx* c, const double* in, double* out, bool fp64) {
+  if (fp64 && c->per_block) return run_matvec_plain(c, in, out);
   return fp64 ? run_matvec_fp64(c, in, out) : run_matvec(c, in, out);
 }
 }  // namespace dmrgx
@@ -446,6 +454,7 @@ void dmrgx_ctx_destroy(dmrgx_ctx* c) {
   cudaStreamSynchronize(c->stream);
   if (c->run_free) c->run_free(c->run);
   c->run = nullptr;
+  plain_release(c);
   c->st1.free_device();
   c->st2.free_device();
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
@@ -470,6 +479,8 @@ int dmrgx_set_precision(dmrgx_ctx* c, int prec) {
   ARG_CHECK(prec == DMRGX_PREC_FP64 || c->dtype == DMRGX_F64,
             "set_precision: split precision is available for F64 contexts");
   if (prec == c->prec) return 0;
+  ARG_CHECK(prec == DMRGX_PREC_FP64 || !c->per_block,
+            "set_precision: the per-block schedule is FP64 only");
   c->prec = prec;
   c->sp.free_device();
   c->sp = SplitPlan();
@@ -481,6 +492,16 @@ int dmrgx_set_precision(dmrgx_ctx* c, int prec) {
       return rc;
     }
   }
+  return 0;
+}
+
+int dmrgx_set_schedule(dmrgx_ctx* c, int schedule) {
+  ARG_CHECK(c, "null context");
+  ARG_CHECK(schedule == DMRGX_SCHED_GROUPED || schedule == DMRGX_SCHED_PER_BLOCK,
+            "set_schedule: unknown schedule");
+  ARG_CHECK(schedule == DMRGX_SCHED_GROUPED || c->prec == DMRGX_PREC_FP64,
+            "set_schedule: the per-block schedule is FP64 only");
+  c->per_block = schedule == DMRGX_SCHED_PER_BLOCK;
   return 0;
 }
 

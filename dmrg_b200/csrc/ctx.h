@@ -15,8 +15,16 @@ namespace dmrgx {
 
 void set_error(const std::string& msg);
 
+// one task row as a plain GEMM: C[M x N] += sign A[M x K] B[N x K]^T, offsets in
+// doubles (A in the environment image, which already carries the row's sign)
+struct PlainRow {
+  int64_t a_off, b_off, c_off;
+  int32_t M, N, K, sign;
+};
+
 // one stage of the matvec on the device
 struct Stage {
+  std::vector<PlainRow> rows;  // the same work as one GEMM per task row
   std::vector<DOut> outs;
   std::vector<DSeg> segs;
   std::vector<DTile> tiles;
@@ -95,6 +103,8 @@ struct dmrgx_ctx {
   double* h_out = nullptr;
   size_t h_cap = 0;
 
+  bool per_block = false;                       // DMRGX_SCHED_PER_BLOCK: one GEMM per task row
+  void* blas = nullptr;                         // cuBLAS handle of the per-block schedule
   void* run = nullptr;                          // state of the last dmrgx_dmrg (MPS, centre)
   void (*run_free)(void*) = nullptr;
 

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(PKG, "libdmrgx.so")
 
 F64, C128 = 0, 1
 PREC_FP64, PREC_BF16X3, PREC_TF32X3 = 0, 1, 2
+SCHED_GROUPED, SCHED_PER_BLOCK = 0, 1
 MEM_HOST, MEM_DEVICE = 0, 1
 
 # every entry point declared in include/dmrgx.h, with (restype, argtypes)
@@ -40,6 +41,7 @@ SIGNATURES = {
     "dmrgx_eigsolve": (_i, [_vp, _i, _i, C.c_double, _i, _vp, _dp, _vp, _i64p]),
     "dmrgx_dmrg": (_i, [_vp, _i, _i, _i, _i, _i, _dp, _i, _dp, _dp, _ip, _i64p, _i64, _i64p,
                         _dp]),
+    "dmrgx_set_schedule": (_i, [_vp, _i]),
     "dmrgx_adjoint": (_i, [_vp, _i, _dp, _i, _dp, _i64, _i64p, _dp, _dp]),
     "dmrgx_expect": (_i, [_vp, _dp, _i, _dp]),
     "dmrgx_profile": (_i, [_vp, _i]),
@@ -137,6 +139,10 @@ class Context:
 
     def set_precision(self, prec):
         _check(lib().dmrgx_set_precision(self.ptr, prec))
+
+    def set_schedule(self, schedule):
+        """SCHED_GROUPED (default) or SCHED_PER_BLOCK (one cuBLAS GEMM per task row)."""
+        _check(lib().dmrgx_set_schedule(self.ptr, schedule))
 
     def plan_build(self, lenv, renv, l_num, r_num, sector, group_n, fermion=0):
         """lenv/renv: (meta int array, packed values) pairs."""

@@ -51,6 +51,14 @@ enum {
   DMRGX_PREC_TF32X3 = 2, /* split precision in TF32, FP32 accumulate */
 };
 
+/* how the block GEMMs of one matvec are launched */
+enum {
+  DMRGX_SCHED_GROUPED = 0,   /* one grouped persistent kernel per stage (default) */
+  DMRGX_SCHED_PER_BLOCK = 1, /* one cuBLAS GEMM per task row: the reference's own av()
+                                loop (src/qtensor.cpp:986-994 -> src/tensor.cpp:698-718)
+                                moved to the GPU as-is; FP64 only */
+};
+
 enum { DMRGX_MEM_HOST = 0, DMRGX_MEM_DEVICE = 1 };
 
 typedef struct dmrgx_ctx dmrgx_ctx;
@@ -64,6 +72,11 @@ void dmrgx_ctx_destroy(dmrgx_ctx* ctx);
 
 /* Select the matvec arithmetic (DMRGX_PREC_*).  Default FP64. */
 int dmrgx_set_precision(dmrgx_ctx* ctx, int prec);
+
+/* Select the launch schedule of the matvec (DMRGX_SCHED_*).  Default grouped.
+ * The per-block schedule is the plain FP64 GPU path: same plan, same
+ * eigensolver, one library GEMM per task row with the row's sign as alpha. */
+int dmrgx_set_schedule(dmrgx_ctx* ctx, int schedule);
 
 /* Build a matvec plan from two block-sparse environments, the way the
  * reference step functions do before calling the eigensolver

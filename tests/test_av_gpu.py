@@ -122,3 +122,25 @@ def test_av_device_pointers():
     ctx.av_device(x.data_ptr(), y.data_ptr())
     ctx.sync()
     assert close(y.cpu().numpy(), mb["ax"])
+
+
+@pytest.mark.parametrize("model", MODELS)
+def test_av_per_block_schedule_matches_reference(model):
+    """The plain FP64 path (one cuBLAS GEMM per task row) on the same plans."""
+    for st in load_steps(model):
+        ctx = native.Context(native.C128 if st["complex"] else native.F64)
+        ctx.set_schedule(native.SCHED_PER_BLOCK)
+        ctx.plan_build(st["lenv"], st["renv"], st["l_num"], st["r_num"], st["sector"],
+                       st["group_n"], st["fermion"])
+        assert close(ctx.av(st["x"]), st["ax"])
+        ctx.close()
+
+
+def test_av_per_block_microbench_m64():
+    mb = load_microbench_m64()
+    ctx = native.Context(native.F64)
+    ctx.set_schedule(native.SCHED_PER_BLOCK)
+    ctx.plan_build(mb["lenv"], mb["renv"], 3, 2, mb["sector"], mb["group_n"], 0)
+    assert close(ctx.av(mb["x"]), mb["ax"])
+    with pytest.raises(native.DmrgxError):
+        ctx.set_precision(native.PREC_BF16X3)  # the per-block schedule is FP64 only
