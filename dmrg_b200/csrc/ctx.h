@@ -64,12 +64,12 @@ struct SplitStage {
   void free_device();
 };
 
-// Split-precision plan: (hi, lo) operand images (hi at [0, len), lo at
-// [len, 2 len) of one buffer each) and the two stages.
+// Split-precision plan: (hi, lo) operand images in the pair layout of split.h
+// (one buffer each) and the two stages.
 struct SplitPlan {
   int eb = 0;                      // element bytes of the pairs: 2 BF16, 4 TF32 (0 = none)
   SplitStage s1, s2;
-  int64_t a1_len = 0, a2_len = 0, psi_len = 0, store_len = 0;   // elements per half
+  int64_t a1_len = 0, a2_len = 0, psi_len = 0, store_len = 0;   // elements (hi and lo)
   std::vector<PadJob> psi_jobs;    // per-matvec FP64 psi -> (hi, lo)
   std::vector<PadRow> psi_rows;
   PadJob* d_psi_jobs = nullptr;

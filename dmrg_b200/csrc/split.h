@@ -10,15 +10,27 @@
 
 namespace dmrgx {
 
+// Pair layout of the split operands.  A row of logical length kq (a multiple of
+// CH = 64 / element-bytes) is kq / CH chunks of 128 bytes, chunk c holding the hi
+// parts of elements [c*CH, (c+1)*CH) followed by their lo parts; the row stride
+// is 2*kq elements.  One TMA box of one 128-byte row per k-tile brings both halves.
+__host__ __device__ inline int64_t pair_off(int64_t k, int ch) {
+  return (k / ch) * 2 * ch + (k % ch);
+}
+
 // Output block of the split path.  Offsets/extents in elements of the arrays
-// the kernel writes: the padded (hi, lo) intermediate for stage 1, the packed FP64
+// the kernel writes: the pair-layout intermediate for stage 1, the packed FP64
 // psi for stage 2.
 struct SOut {
   int64_t c_off;
   int32_t m, n;      // rows, columns
-  int32_t ldc;       // row stride of C (>= n)
+  int32_t ldc;       // stage 2: row stride of C.  stage 1: padded columns per row
+                     // (n1p); row r, column j lands at logical k = (r % grp) * n1p + j
+                     // of pair-layout row r / grp
   int32_t seg_begin, seg_count;
   int32_t tnw;       // tile width (columns per tile, <= 256, a multiple of 16)
+  int32_t grp;       // stage 1: output rows per pair-layout row (MPO channels)
+  int32_t rstride;   // stage 1: elements per pair-layout row (2 * kq)
 };
 
 // One segment of an output block: tensor-map indices of its A block (m x kp) and
@@ -56,11 +68,14 @@ struct PadRow {
   int32_t job, row;
 };
 
-// FP64 -> (hi, lo) conversion job: rows x (groups x cols) source elements,
-// destination rows of groups x colsp elements (colsp >= cols, zero padding).
+// FP64 -> (hi, lo) conversion job: rows x (groups x cols) source elements;
+// source element (g, j) of a row goes to logical k = g * colsp + j of a
+// pair-layout destination row of kq elements (colsp >= cols, kq >= groups * colsp;
+// the gaps stay zero).
 struct PadJob {
   int64_t src, dst;
   int32_t rows, groups, cols, colsp;
+  int32_t kq, pad_;
 };
 
 int tc_smem_bytes();
@@ -68,8 +83,8 @@ int tc_tile_m();
 int tc_tile_n();
 int tc_ktile_bytes();
 
-// Convert the rows listed in `rows` (one thread block each).
-cudaError_t launch_pad_split(int eb, const double* src, void* hi, void* lo, const PadJob* jobs,
+// Convert the rows listed in `rows` (one thread block each) into pair layout.
+cudaError_t launch_pad_split(int eb, const double* src, void* dst, const PadJob* jobs,
                              const PadRow* rows, int nrows, cudaStream_t st);
 
 // One stage: the warp-specialized TMA/tcgen05 kernel over `units`, then the
@@ -78,7 +93,7 @@ cudaError_t launch_pad_split(int eb, const double* src, void* hi, void* lo, cons
 // [cta_begin[c], cta_begin[c+1]) in order, then the reduction of K-split tiles.
 cudaError_t launch_tc_gemm(int eb, bool out_split, const CUtensorMap* maps, const SUnit* units,
                            const int* cta_begin, int nctas, const SOut* outs, const SSeg2* segs,
-                           void* c_hi, void* c_lo, double* c64, float* ws, const SRed* reds,
+                           void* c_pair, double* c64, float* ws, const SRed* reds,
                            const SRedBlk* redblk, int nredblk, int* err, cudaStream_t st);
 
 }  // namespace dmrgx

@@ -1,15 +1,18 @@
 // Split-precision form of a matvec plan, derived from the FP64 plan of the same
-// context: padded (hi, lo) operand images, one TMA tensor map per operand block,
-// and K-split work units for the warp-specialized tcgen05 kernel (tc_gemm.cu).
+// context: (hi, lo) operand images in the pair layout of split.h, one TMA tensor
+// map per operand block, and K-split work units for the warp-specialized tcgen05
+// kernel (tc_gemm.cu).
 //
 // Stage 1 (store = renv (x) psi):
-//   A1 = renv blocks, M1 x K1 -> rows padded to K1p (a multiple of 16 bytes)
-//   B1 = psi blocks as stage 1 views them, N1 x K1 -> N1 x K1p, split every matvec
-//   C1 = the intermediate, M1 x N1 -> written as (hi, lo) with row stride N1p
+//   A1 = renv blocks, M1 x K1 -> pair rows of kq = K1 rounded up to a k-tile
+//   B1 = psi blocks as stage 1 views them, N1 x K1 -> pair rows, split every matvec
+//   C1 = the intermediate, M1 x N1, written by the epilogue as (hi, lo) pairs
 // Stage 2 (out = lenv (x) store):
-//   the intermediate block (M1 x N1p) read as N2 x (D x N1p) with D = M1 / N2
-//   (its rows are the stage-2 rows times the MPO channel, src/core.cpp:188-192),
-//   A2 = lenv blocks M2 x (D x N1) -> M2 x (D x N1p), zeros in each slice's padding
+//   the intermediate block (M1 x N1) is read as N2 x (D x N1p) with D = M1 / N2
+//   (its rows are the stage-2 rows times the MPO channel, src/core.cpp:188-192);
+//   N1p = N1 rounded up to 16 bytes, each stage-2 row one pair row of
+//   kq2 = D x N1p rounded up to a k-tile
+//   A2 = lenv blocks M2 x (D x N1) -> pair rows of kq2, zeros in each slice's padding
 //   C2 = packed FP64 psi.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -79,22 +82,22 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// Tensor map of one padded block: dims (K elements, rows, hi|lo), box (one k-tile
-// row of 64 bytes, box_rows, 2), 64-byte swizzle.
-bool make_map(CUtensorMap* m, int eb, void* base, int64_t kp, int64_t rows, int64_t half_elems,
-              int box_rows, std::string& why) {
+// Tensor map of one pair-layout block: dims (2 kq elements, rows), box (one
+// 128-byte chunk per row, box_rows), 128-byte swizzle.
+bool make_map(CUtensorMap* m, int eb, void* base, int64_t kq, int64_t rows, int box_rows,
+              std::string& why) {
   auto fn = encode_fn();
   if (!fn) {
     why = "cuTensorMapEncodeTiled is not available from the driver";
     return false;
   }
-  const cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)rows, 2};
-  const cuuint64_t strides[2] = {(cuuint64_t)(kp * eb), (cuuint64_t)(half_elems * eb)};
-  const cuuint32_t box[3] = {(cuuint32_t)(tc_ktile_bytes() / eb), (cuuint32_t)box_rows, 2};
-  const cuuint32_t es[3] = {1, 1, 1};
+  const cuuint64_t dims[2] = {(cuuint64_t)(2 * kq), (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)(2 * kq * eb)};
+  const cuuint32_t box[2] = {(cuuint32_t)(tc_ktile_bytes() / eb), (cuuint32_t)box_rows};
+  const cuuint32_t es[2] = {1, 1};
   CUresult r = fn(m, eb == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                  3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                  CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     why = "cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) + ")";
@@ -120,7 +123,7 @@ int tile_width(int n, bool halve_wide) {
 // least-loaded CTA.
 void make_units(SplitStage& st, int num_sms) {
   const int TM = tc_tile_m();
-  const int A_B = 2 * TM * tc_ktile_bytes();
+  const int A_B = TM * tc_ktile_bytes();
   struct T { int out, tm, tn, kt; double per_kt; };
   std::vector<T> tiles;
   double total = 0;
@@ -134,7 +137,7 @@ void make_units(SplitStage& st, int num_sms) {
       for (int b = 0; b < tn; b++) {
         const int ncols = std::min(so.tnw, so.n - b * so.tnw);
         const int nmma = (int)rup(ncols, 16);
-        const double per = std::max(3.0 * nmma, (A_B + 2.0 * brows * tc_ktile_bytes()) / 48.0);
+        const double per = std::max(3.0 * nmma, (A_B + 1.0 * brows * tc_ktile_bytes()) / 48.0);
         tiles.push_back({(int)o, a, b, kt, per});
         total += kt * per + 800;
       }
@@ -219,7 +222,7 @@ std::vector<PadRow> rows_of(const std::vector<PadJob>& jobs) {
   return r;
 }
 
-int run_jobs(int eb, const double* src, void* hi, void* lo, const std::vector<PadJob>& jobs,
+int run_jobs(int eb, const double* src, void* dst, const std::vector<PadJob>& jobs,
              cudaStream_t s) {
   if (jobs.empty()) return 0;
   PadJob* d = nullptr;
@@ -230,7 +233,7 @@ int run_jobs(int eb, const double* src, void* hi, void* lo, const std::vector<Pa
   SP_TRY(cudaMemcpyAsync(d, jobs.data(), sizeof(PadJob) * jobs.size(), cudaMemcpyHostToDevice, s));
   if (!rows.empty())
     SP_TRY(cudaMemcpyAsync(dr, rows.data(), sizeof(PadRow) * rows.size(), cudaMemcpyHostToDevice, s));
-  SP_TRY(launch_pad_split(eb, src, hi, lo, d, dr, (int)rows.size(), s));
+  SP_TRY(launch_pad_split(eb, src, dst, d, dr, (int)rows.size(), s));
   SP_TRY(cudaStreamSynchronize(s));
   cudaFree(d);
   cudaFree(dr);
@@ -247,55 +250,91 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
     set_error("split precision is available for F64 contexts");
     return DMRGX_E_ARG;
   }
-  const int64_t P = 16 / eb;                     // padding granularity (elements)
-  const int64_t BK = tc_ktile_bytes() / eb;      // elements per k-tile row
+  const int64_t P = 16 / eb;   // padding of stage-1 output rows (16 bytes)
+  const int64_t CH = 64 / eb;  // elements per half-chunk of the pair layout = per k-tile
   const Stage& f1 = c->st1;
   const Stage& f2 = c->st2;
-  struct MapReq { int which; int64_t off, kp, rows; int box_rows; };  // which: 0 a1,1 psi,2 a2,3 store
+  struct MapReq { int which; int64_t off, kq, rows; int box_rows; };  // which: 0 a1,1 psi,2 a2,3 store
   std::vector<MapReq> req1, req2;
+
+  // MPO channels per stage-1 output block: stage 2 reads a store block
+  // [D*N2 x N1] as [N2 x D*N1]
+  std::map<int64_t, std::pair<int, int>> st_shape;  // FP64 store offset -> (M1, N1)
+  for (size_t o = 0; o < f1.outs.size(); o++) st_shape[f1.outs[o].c_off] = {f1.outs[o].m, f1.outs[o].n};
+  std::map<int64_t, int> st_grp;
+  for (size_t o = 0; o < f2.outs.size(); o++) {
+    const DOut& d = f2.outs[o];
+    for (int q = 0; q < d.seg_count; q++) {
+      const DSeg& g = f2.segs[d.seg_begin + q];
+      auto is = st_shape.find(g.b_off);
+      if (is == st_shape.end()) {
+        set_error("split plan: a stage-2 task reads no stage-1 output block");
+        return DMRGX_E_ARG;
+      }
+      const int M1 = is->second.first, N1 = is->second.second;
+      if (N1 <= 0 || g.k % N1 != 0 || (int64_t)(g.k / N1) * d.n != M1) {
+        set_error("split plan: stage-2 K does not factor as channels x stage-1 columns");
+        return DMRGX_E_ARG;
+      }
+      auto ig = st_grp.find(g.b_off);
+      if (ig != st_grp.end() && ig->second != g.k / N1) {
+        set_error("split plan: a store block is read with two channel counts");
+        return DMRGX_E_ARG;
+      }
+      st_grp[g.b_off] = g.k / N1;
+    }
+  }
 
   // ---- stage 1 layout
   std::map<int64_t, int> a1_map, psi_map;
-  std::map<int64_t, int64_t> st_off;
-  std::map<int64_t, std::pair<int, int>> st_shape;  // FP64 store offset -> (M1, N1)
+  std::map<int64_t, int64_t> st_off, st_kq;
   std::vector<PadJob> a1_jobs;
   int64_t a1_len = 0, psi_len = 0, st_len = 0;
   for (size_t o = 0; o < f1.outs.size(); o++) {
     const DOut& d = f1.outs[o];
     SOut so;
+    auto ig = st_grp.find(d.c_off);
+    const int D = ig == st_grp.end() ? 1 : ig->second;
+    if (d.m % D) {
+      set_error("split plan: stage-1 rows are not a multiple of the channel count");
+      return DMRGX_E_ARG;
+    }
+    const int64_t n1p = rup(d.n, P), kq2 = rup(D * n1p, CH);
     if (st_off.find(d.c_off) == st_off.end()) {
       st_off[d.c_off] = st_len;
-      st_shape[d.c_off] = {d.m, d.n};
-      st_len += (int64_t)d.m * rup(d.n, P);
+      st_kq[d.c_off] = kq2;
+      st_len += (int64_t)(d.m / D) * 2 * kq2;
     }
     so.c_off = st_off[d.c_off];
     so.m = d.m;
     so.n = d.n;
-    so.ldc = (int32_t)rup(d.n, P);
+    so.ldc = (int32_t)n1p;
+    so.grp = D;
+    so.rstride = (int32_t)(2 * kq2);
     so.seg_begin = (int32_t)sp.s1.segs.size();
     so.seg_count = d.seg_count;
     so.tnw = tile_width(d.n, true);
-    for (int s = 0; s < d.seg_count; s++) {
-      const DSeg& g = f1.segs[d.seg_begin + s];
-      const int64_t kp = rup(g.k, P);
+    for (int q = 0; q < d.seg_count; q++) {
+      const DSeg& g = f1.segs[d.seg_begin + q];
+      const int64_t kq = rup(g.k, CH);
       SSeg2 ss;
       auto ia = a1_map.find(g.a_off);
       if (ia == a1_map.end()) {
-        a1_jobs.push_back(PadJob{g.a_off, a1_len, d.m, 1, g.k, (int32_t)kp});
+        a1_jobs.push_back(PadJob{g.a_off, a1_len, d.m, 1, g.k, g.k, (int32_t)kq, 0});
         a1_map[g.a_off] = (int)req1.size();
-        req1.push_back({0, a1_len, kp, d.m, 128});
-        a1_len += (int64_t)d.m * kp;
+        req1.push_back({0, a1_len, kq, d.m, 128});
+        a1_len += (int64_t)d.m * 2 * kq;
       }
       ss.amap = a1_map[g.a_off];
       auto ib = psi_map.find(g.b_off);
       if (ib == psi_map.end()) {
-        sp.psi_jobs.push_back(PadJob{g.b_off, psi_len, d.n, 1, g.k, (int32_t)kp});
+        sp.psi_jobs.push_back(PadJob{g.b_off, psi_len, d.n, 1, g.k, g.k, (int32_t)kq, 0});
         psi_map[g.b_off] = (int)req1.size();
-        req1.push_back({1, psi_len, kp, d.n, tile_width(d.n, true)});
-        psi_len += (int64_t)d.n * kp;
+        req1.push_back({1, psi_len, kq, d.n, tile_width(d.n, true)});
+        psi_len += (int64_t)d.n * 2 * kq;
       }
       ss.bmap = psi_map[g.b_off];
-      ss.nkt = (int32_t)((kp + BK - 1) / BK);
+      ss.nkt = (int32_t)(kq / CH);
       ss.brows = req1[ss.bmap].box_rows;
       sp.s1.segs.push_back(ss);
     }
@@ -314,39 +353,32 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
     so.m = d.m;
     so.n = d.n;
     so.ldc = d.n;
+    so.grp = 1;
+    so.rstride = 0;
     so.seg_begin = (int32_t)sp.s2.segs.size();
     so.seg_count = d.seg_count;
     so.tnw = tile_width(d.n, false);
-    for (int s = 0; s < d.seg_count; s++) {
-      const DSeg& g = f2.segs[d.seg_begin + s];
-      auto is = st_shape.find(g.b_off);
-      if (is == st_shape.end()) {
-        set_error("split plan: a stage-2 task reads no stage-1 output block");
-        return DMRGX_E_ARG;
-      }
-      const int M1 = is->second.first, N1 = is->second.second;
-      if (g.k % N1 != 0 || (int64_t)(g.k / N1) * d.n != M1) {
-        set_error("split plan: stage-2 K does not factor as channels x stage-1 columns");
-        return DMRGX_E_ARG;
-      }
+    for (int q = 0; q < d.seg_count; q++) {
+      const DSeg& g = f2.segs[d.seg_begin + q];
+      const int N1 = st_shape[g.b_off].second;
       const int D = g.k / N1;
-      const int64_t n1p = rup(N1, P), kp = D * n1p;
+      const int64_t n1p = rup(N1, P), kq2 = st_kq[g.b_off];
       SSeg2 ss;
       auto ia = a2_map.find(g.a_off);
       if (ia == a2_map.end()) {
-        a2_jobs.push_back(PadJob{g.a_off, a2_len, d.m, D, N1, (int32_t)n1p});
+        a2_jobs.push_back(PadJob{g.a_off, a2_len, d.m, D, N1, (int32_t)n1p, (int32_t)kq2, 0});
         a2_map[g.a_off] = (int)req2.size();
-        req2.push_back({2, a2_len, kp, d.m, 128});
-        a2_len += (int64_t)d.m * kp;
+        req2.push_back({2, a2_len, kq2, d.m, 128});
+        a2_len += (int64_t)d.m * 2 * kq2;
       }
       ss.amap = a2_map[g.a_off];
       auto ib = stb_map.find(g.b_off);
       if (ib == stb_map.end()) {
         stb_map[g.b_off] = (int)req2.size();
-        req2.push_back({3, st_off[g.b_off], kp, d.n, tile_width(d.n, false)});
+        req2.push_back({3, st_off[g.b_off], kq2, d.n, tile_width(d.n, false)});
       }
       ss.bmap = stb_map[g.b_off];
-      ss.nkt = (int32_t)((kp + BK - 1) / BK);
+      ss.nkt = (int32_t)(kq2 / CH);
       ss.brows = req2[ss.bmap].box_rows;
       sp.s2.segs.push_back(ss);
     }
@@ -355,35 +387,34 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
   sp.s2.full_cover = f2.full_cover;
   make_units(sp.s1, c->num_sms);
   make_units(sp.s2, c->num_sms);
-  // halves rounded to 256 bytes so hi and lo both start aligned
-  auto half = [eb](int64_t n) { return rup(std::max<int64_t>(n, 1), 256 / eb); };
-  sp.a1_len = half(a1_len);
-  sp.a2_len = half(a2_len);
-  sp.psi_len = half(psi_len);
-  sp.store_len = half(st_len);
+  auto len = [eb](int64_t n) { return rup(std::max<int64_t>(n, 1), 256 / eb); };
+  sp.a1_len = len(a1_len);
+  sp.a2_len = len(a2_len);
+  sp.psi_len = len(psi_len);
+  sp.store_len = len(st_len);
   sp.psi_rows = rows_of(sp.psi_jobs);
 
   // ---- device buffers and images
   cudaStream_t s = c->stream;
-  SP_TRY(c->sa1.ensure(2 * sp.a1_len * eb));
-  SP_TRY(c->sa2.ensure(2 * sp.a2_len * eb));
-  SP_TRY(c->spsi.ensure(2 * sp.psi_len * eb));
-  SP_TRY(c->sstore.ensure(2 * sp.store_len * eb));
+  SP_TRY(c->sa1.ensure(sp.a1_len * eb));
+  SP_TRY(c->sa2.ensure(sp.a2_len * eb));
+  SP_TRY(c->spsi.ensure(sp.psi_len * eb));
+  SP_TRY(c->sstore.ensure(sp.store_len * eb));
   const int slots = std::max(1, std::max(sp.s1.nslots, sp.s2.nslots));
   SP_TRY(c->sws.ensure((size_t)slots * tc_tile_m() * tc_tile_n() * sizeof(float)));
   SP_TRY(c->err.ensure(16));
-  SP_TRY(cudaMemsetAsync(c->sa1.p, 0, 2 * sp.a1_len * eb, s));
-  SP_TRY(cudaMemsetAsync(c->sa2.p, 0, 2 * sp.a2_len * eb, s));
-  SP_TRY(cudaMemsetAsync(c->spsi.p, 0, 2 * sp.psi_len * eb, s));
-  SP_TRY(cudaMemsetAsync(c->sstore.p, 0, 2 * sp.store_len * eb, s));
+  SP_TRY(cudaMemsetAsync(c->sa1.p, 0, sp.a1_len * eb, s));
+  SP_TRY(cudaMemsetAsync(c->sa2.p, 0, sp.a2_len * eb, s));
+  SP_TRY(cudaMemsetAsync(c->spsi.p, 0, sp.psi_len * eb, s));
+  SP_TRY(cudaMemsetAsync(c->sstore.p, 0, sp.store_len * eb, s));
   SP_TRY(cudaMemsetAsync(c->err.p, 0, 16, s));
   uint8_t* a1 = (uint8_t*)c->sa1.p;
   uint8_t* a2 = (uint8_t*)c->sa2.p;
   uint8_t* psi = (uint8_t*)c->spsi.p;
   uint8_t* stb = (uint8_t*)c->sstore.p;
-  int rc = run_jobs(eb, (const double*)c->renv.p, a1, a1 + sp.a1_len * eb, a1_jobs, s);
+  int rc = run_jobs(eb, (const double*)c->renv.p, a1, a1_jobs, s);
   if (rc) return rc;
-  rc = run_jobs(eb, (const double*)c->lenv.p, a2, a2 + sp.a2_len * eb, a2_jobs, s);
+  rc = run_jobs(eb, (const double*)c->lenv.p, a2, a2_jobs, s);
   if (rc) return rc;
   // ---- tensor maps
   std::string why;
@@ -392,10 +423,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
     for (size_t i = 0; i < req.size(); i++) {
       const MapReq& r = req[i];
       uint8_t* base = r.which == 0 ? a1 : r.which == 1 ? psi : r.which == 2 ? a2 : stb;
-      const int64_t h = r.which == 0 ? sp.a1_len : r.which == 1 ? sp.psi_len
-                        : r.which == 2 ? sp.a2_len : sp.store_len;
-      if (!make_map(&out[i], eb, base + r.off * eb, r.kp, r.rows, h, r.box_rows, why))
-        return false;
+      if (!make_map(&out[i], eb, base + r.off * eb, r.kq, r.rows, r.box_rows, why)) return false;
     }
     return true;
   };
@@ -421,18 +449,18 @@ int run_matvec_split(dmrgx_ctx* c, const double* in, double* out) {
   uint8_t* psi = (uint8_t*)c->spsi.p;
   uint8_t* stb = (uint8_t*)c->sstore.p;
   c->prof_mark();
-  SP_TRY(launch_pad_split(eb, in, psi, psi + sp.psi_len * eb, sp.d_psi_jobs, sp.d_psi_rows,
-                          (int)sp.psi_rows.size(), s));
+  SP_TRY(launch_pad_split(eb, in, psi, sp.d_psi_jobs, sp.d_psi_rows, (int)sp.psi_rows.size(),
+                          s));
   c->prof_mark();
   SP_TRY(launch_tc_gemm(eb, true, sp.s1.d_maps, sp.s1.d_units, sp.s1.d_cta_begin,
-                        (int)sp.s1.cta_begin.size() - 1, sp.s1.d_outs, sp.s1.d_segs, stb,
-                        stb + sp.store_len * eb, nullptr, (float*)c->sws.p, sp.s1.d_reds,
-                        sp.s1.d_redblk, (int)sp.s1.redblk.size(), (int*)c->err.p, s));
+                        (int)sp.s1.cta_begin.size() - 1, sp.s1.d_outs, sp.s1.d_segs, stb, nullptr,
+                        (float*)c->sws.p, sp.s1.d_reds, sp.s1.d_redblk,
+                        (int)sp.s1.redblk.size(), (int*)c->err.p, s));
   c->prof_mark();
   if (!sp.s2.full_cover) SP_TRY(cudaMemsetAsync(out, 0, sizeof(double) * c->n, s));
   SP_TRY(launch_tc_gemm(eb, false, sp.s2.d_maps, sp.s2.d_units, sp.s2.d_cta_begin,
                         (int)sp.s2.cta_begin.size() - 1, sp.s2.d_outs, sp.s2.d_segs, nullptr,
-                        nullptr, out, (float*)c->sws.p, sp.s2.d_reds, sp.s2.d_redblk,
+                        out, (float*)c->sws.p, sp.s2.d_reds, sp.s2.d_redblk,
                         (int)sp.s2.redblk.size(), (int*)c->err.p, s));
   c->prof_mark();
   return 0;

@@ -7,12 +7,13 @@
 // Element types: BF16 pairs (kind::f16, K=16 per instruction) or TF32 pairs in
 // 32-bit containers (kind::tf32, K=8 per instruction).
 //
-// Operand blocks are row-major with K contiguous, rows padded to 16 bytes, the
-// lo array a fixed distance after the hi array.  One 3-D tensor map per block
-// (K, rows, hi|lo) with 64-byte swizzle brings a k-tile of 64 bytes per row for
-// both halves in one TMA instruction, straight into the UMMA canonical K-major
-// SW64 layout (8-row atoms of 512 B).  Rows and K past the block edge are
-// zero-filled by TMA.
+// Operand blocks are row-major with K contiguous in the pair layout of split.h:
+// each 128-byte chunk of a row holds 64 bytes of hi parts and the 64 bytes of
+// their lo parts.  One 2-D tensor map per block with 128-byte swizzle brings a
+// k-tile (one chunk per row, both halves) in one TMA instruction of 128-byte
+// rows, straight into the UMMA canonical K-major SW128 layout (8-row atoms of
+// 1 KB); the hi k-steps sit at byte 0 and 32 of each row, the lo k-steps at 64
+// and 96.  Rows past the block edge are zero-filled by TMA.
 //
 // Roles (192 threads):
 //   warp 0      TMA producer: walks the work unit's k-tiles over its segments,
@@ -50,11 +51,12 @@ constexpr int THREADS = 192;
 constexpr int TM = 128;
 constexpr int TNMAX = 256;
 constexpr int STAGES = 4;
-constexpr int ROWB = 64;                      // bytes per row of one k-tile
-constexpr int A_BYTES = 2 * TM * ROWB;        // hi + lo: 16 KB
-constexpr int B_BYTES = 2 * TNMAX * ROWB;     // hi + lo: 32 KB
+constexpr int ROWB = 128;                     // bytes per row of one k-tile (hi + lo)
+constexpr int HALF = 64;                      // byte offset of the lo parts in a row
+constexpr int A_BYTES = TM * ROWB;            // 16 KB
+constexpr int B_BYTES = TNMAX * ROWB;         // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-constexpr int SBO = 8 * ROWB;                 // 512 B between 8-row atoms
+constexpr int SBO = 8 * ROWB;                 // 1 KB between 8-row atoms
 constexpr uint32_t TMEM_COLS = 512;           // two 256-column accumulators
 constexpr uint64_t WAIT_NS = 2000000000ull;  // a wait gives up after 2 s
 
@@ -96,18 +98,18 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes)
                : "memory");
 }
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y,
-                                            int z, uint32_t bar) {
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint32_t bar) {
   asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-      "[%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
       : "memory");
 }
-__device__ __forceinline__ uint64_t sw64_desc(uint32_t addr) {
-  // K-major, 64-byte swizzle: LBO unused (1), SBO = 512 B, version 1, layout 4
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+  // K-major, 128-byte swizzle: LBO unused (1), SBO = 1 KB, version 1, layout 2
   return (uint64_t)((addr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(SBO >> 4) << 32) |
-         (1ull << 46) | (4ull << 61);
+         (1ull << 46) | (2ull << 61);
 }
 template <int EB>
 __device__ __forceinline__ uint32_t instr_desc(int n) {
@@ -174,12 +176,16 @@ __device__ __forceinline__ void split_f32(float v, uint32_t& hi, uint32_t& lo) {
 }
 
 // Final store of 16 consecutive columns of one row (cols [col0, col0+16)).
+// Stage 1 (OUT_SPLIT): (hi, lo) pairs in pair layout, 16 bytes of each per
+// group of 16 / EB columns (a group never crosses a chunk: n1p and col0 are
+// multiples of it).
 template <int EB, bool OUT_SPLIT>
 __device__ __forceinline__ void store16(const SOut& o, int row, int col0, const float* v,
-                                        uint8_t* c_hi, uint8_t* c_lo, double* c64) {
-  const int64_t rbase = o.c_off + (int64_t)row * o.ldc + col0;
+                                        uint8_t* c_pair, double* c64) {
   if (OUT_SPLIT) {
-    constexpr int EPC = 16 / EB;
+    constexpr int EPC = 16 / EB, CH = 64 / EB;
+    const int64_t rbase = o.c_off + (int64_t)(row / o.grp) * o.rstride;
+    const int64_t kb = (int64_t)(row % o.grp) * o.ldc;
 #pragma unroll
     for (int gq = 0; gq < 16 / EPC; gq++) {
       if (col0 + gq * EPC >= o.ldc) break;
@@ -197,11 +203,12 @@ __device__ __forceinline__ void store16(const SOut& o, int row, int col0, const 
 #pragma unroll
         for (int p = 0; p < 4; p++) split_f32<4>(v[gq * 4 + p], hw[p], lw[p]);
       }
-      const int64_t eoff = (rbase + gq * EPC) * EB;
-      *reinterpret_cast<uint4*>(c_hi + eoff) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-      *reinterpret_cast<uint4*>(c_lo + eoff) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+      const int64_t eoff = (rbase + pair_off(kb + col0 + gq * EPC, CH)) * EB;
+      *reinterpret_cast<uint4*>(c_pair + eoff) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+      *reinterpret_cast<uint4*>(c_pair + eoff + HALF) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
     }
   } else {
+    const int64_t rbase = o.c_off + (int64_t)row * o.ldc + col0;
 #pragma unroll
     for (int i = 0; i < 16; i++)
       if (col0 + i < o.n) c64[rbase + i] = (double)v[i];
@@ -212,9 +219,8 @@ template <int EB, bool OUT_SPLIT>
 __global__ void __launch_bounds__(THREADS, 1)
 tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ units,
                 const int* __restrict__ cta_begin, const SOut* __restrict__ outs,
-                const SSeg2* __restrict__ segs,
-                uint8_t* __restrict__ c_hi, uint8_t* __restrict__ c_lo, double* __restrict__ c64,
-                float* __restrict__ ws, int* __restrict__ err) {
+                const SSeg2* __restrict__ segs, uint8_t* __restrict__ c_pair,
+                double* __restrict__ c64, float* __restrict__ ws, int* __restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   // 1024-aligned ring (the swizzle pattern repeats every 512 B)
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
@@ -225,7 +231,7 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
   uint64_t* tempty = tfull + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
 
-  constexpr int BK = ROWB / EB;   // elements per k-tile row
+  constexpr int BK = HALF / EB;   // elements (of each half) per k-tile
   constexpr int NKS = BK / (32 / EB);  // MMA k-steps (32 bytes each) per k-tile
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t sbase = smem_u32(smem);
@@ -279,9 +285,9 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
           }
           const uint32_t st = sbase + slot * STAGE_BYTES;
           const uint32_t bar = smem_u32(&full[slot]);
-          mbar_expect_tx(bar, (uint32_t)(A_BYTES + 2 * sg.brows * ROWB));
-          tma_load_3d(st, maps + sg.amap, kin * BK, un.tm * TM, 0, bar);
-          tma_load_3d(st + A_BYTES, maps + sg.bmap, kin * BK, un.tn * o.tnw, 0, bar);
+          mbar_expect_tx(bar, (uint32_t)(A_BYTES + sg.brows * ROWB));
+          tma_load_2d(st, maps + sg.amap, kin * 2 * BK, un.tm * TM, bar);
+          tma_load_2d(st + A_BYTES, maps + sg.bmap, kin * 2 * BK, un.tn * o.tnw, bar);
           g++;
           if (++kin >= sg.nkt) {
             kin = 0;
@@ -326,13 +332,12 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
           }
           tc_fence_after();
           const uint32_t st = sbase + slot * STAGE_BYTES;
-          const uint32_t a_hi = st, a_lo = st + TM * ROWB;
-          const uint32_t b_hi = st + A_BYTES, b_lo = st + A_BYTES + sg.brows * ROWB;
+          const uint32_t a_t = st, b_t = st + A_BYTES;
 #pragma unroll
           for (int j = 0; j < NKS; j++) {
             const uint32_t ko = j * 32;
-            const uint64_t ah = sw64_desc(a_hi + ko), al = sw64_desc(a_lo + ko);
-            const uint64_t bh = sw64_desc(b_hi + ko), bl = sw64_desc(b_lo + ko);
+            const uint64_t ah = sw128_desc(a_t + ko), al = sw128_desc(a_t + HALF + ko);
+            const uint64_t bh = sw128_desc(b_t + ko), bl = sw128_desc(b_t + HALF + ko);
             mma<EB>(tacc, ah, bh, idesc, (kt > un.kt0 || j > 0) ? 1u : 0u);
             mma<EB>(tacc, ah, bl, idesc, 1u);
             mma<EB>(tacc, al, bh, idesc, 1u);
@@ -387,7 +392,7 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
           for (int i = 0; i < 16; i += 4)
             *reinterpret_cast<float4*>(p + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
         } else {
-          store16<EB, OUT_SPLIT>(o, m0 + row, n0 + cc, v, c_hi, c_lo, c64);
+          store16<EB, OUT_SPLIT>(o, m0 + row, n0 + cc, v, c_pair, c64);
         }
       }
       if (has) {
@@ -409,24 +414,27 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
 
 // Final store of 4 consecutive columns of one row (cols [col0, col0+4)).
 template <int EB, bool OUT_SPLIT>
-__device__ __forceinline__ void store4(const SOut& o, int row, int col0, float4 v, uint8_t* c_hi,
-                                       uint8_t* c_lo, double* c64) {
-  const int64_t e = o.c_off + (int64_t)row * o.ldc + col0;
+__device__ __forceinline__ void store4(const SOut& o, int row, int col0, float4 v,
+                                       uint8_t* c_pair, double* c64) {
   if (OUT_SPLIT) {
     if (col0 >= o.ldc) return;  // ldc is a multiple of 4 elements
+    constexpr int CH = 64 / EB;
+    const int64_t e = o.c_off + (int64_t)(row / o.grp) * o.rstride +
+                      pair_off((int64_t)(row % o.grp) * o.ldc + col0, CH);
     uint32_t h[4], l[4];
     split_f32<EB>(v.x, h[0], l[0]);
     split_f32<EB>(v.y, h[1], l[1]);
     split_f32<EB>(v.z, h[2], l[2]);
     split_f32<EB>(v.w, h[3], l[3]);
     if (EB == 2) {
-      *reinterpret_cast<uint2*>(c_hi + e * 2) = make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
-      *reinterpret_cast<uint2*>(c_lo + e * 2) = make_uint2(l[0] | (l[1] << 16), l[2] | (l[3] << 16));
+      *reinterpret_cast<uint2*>(c_pair + e * 2) = make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
+      *reinterpret_cast<uint2*>(c_pair + e * 2 + HALF) = make_uint2(l[0] | (l[1] << 16), l[2] | (l[3] << 16));
     } else {
-      *reinterpret_cast<uint4*>(c_hi + e * 4) = make_uint4(h[0], h[1], h[2], h[3]);
-      *reinterpret_cast<uint4*>(c_lo + e * 4) = make_uint4(l[0], l[1], l[2], l[3]);
+      *reinterpret_cast<uint4*>(c_pair + e * 4) = make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4*>(c_pair + e * 4 + HALF) = make_uint4(l[0], l[1], l[2], l[3]);
     }
   } else {
+    const int64_t e = o.c_off + (int64_t)row * o.ldc + col0;
     if (col0 < o.n) c64[e] = (double)v.x;
     if (col0 + 1 < o.n) c64[e + 1] = (double)v.y;
     if (col0 + 2 < o.n) c64[e + 2] = (double)v.z;
@@ -442,7 +450,7 @@ template <int EB, bool OUT_SPLIT>
 __global__ void __launch_bounds__(256)
 split_reduce(const SRed* __restrict__ reds, const SRedBlk* __restrict__ blks,
              const SOut* __restrict__ outs, const float* __restrict__ ws,
-             uint8_t* __restrict__ c_hi, uint8_t* __restrict__ c_lo, double* __restrict__ c64) {
+             uint8_t* __restrict__ c_pair, double* __restrict__ c64) {
   const SRedBlk b = blks[blockIdx.x];
   const SRed rd = reds[b.red];
   const SOut o = outs[rd.out];
@@ -461,7 +469,7 @@ split_reduce(const SRed* __restrict__ reds, const SRedBlk* __restrict__ blks,
     acc.z += t.z;
     acc.w += t.w;
   }
-  store4<EB, OUT_SPLIT>(o, m0 + r, n0 + g * 4, acc, c_hi, c_lo, c64);
+  store4<EB, OUT_SPLIT>(o, m0 + r, n0 + g * 4, acc, c_pair, c64);
 }
 
 }  // namespace
@@ -473,7 +481,7 @@ int tc_ktile_bytes() { return ROWB; }
 
 cudaError_t launch_tc_gemm(int eb, bool out_split, const CUtensorMap* maps, const SUnit* units,
                            const int* cta_begin, int nctas, const SOut* outs, const SSeg2* segs,
-                           void* c_hi, void* c_lo, double* c64, float* ws, const SRed* reds,
+                           void* c_pair, double* c64, float* ws, const SRed* reds,
                            const SRedBlk* redblk, int nredblk, int* err, cudaStream_t st) {
   if (nctas <= 0) return cudaSuccess;
   const int sm = tc_smem_bytes();
@@ -483,11 +491,10 @@ cudaError_t launch_tc_gemm(int eb, bool out_split, const CUtensorMap* maps, cons
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, sm);    \
     if (e != cudaSuccess) return e;                                                           \
     tc_grouped_gemm<EB, OS><<<nctas, THREADS, sm, st>>>(maps, units, cta_begin, outs, segs,   \
-                                                       (uint8_t*)c_hi, (uint8_t*)c_lo, c64,   \
-                                                       ws, err);                              \
+                                                       (uint8_t*)c_pair, c64, ws, err);       \
     if (nredblk > 0)                                                                          \
-      split_reduce<EB, OS><<<nredblk, 256, 0, st>>>(reds, redblk, outs, ws, (uint8_t*)c_hi,   \
-                                                   (uint8_t*)c_lo, c64);                      \
+      split_reduce<EB, OS><<<nredblk, 256, 0, st>>>(reds, redblk, outs, ws, (uint8_t*)c_pair, \
+                                                   c64);                                      \
   } while (0)
   if (eb == 2) {
     if (out_split) DMRGX_TC_LAUNCH(2, true);
