@@ -495,6 +495,19 @@ int dmrgx_set_precision(dmrgx_ctx* c, int prec) {
   return 0;
 }
 
+int dmrgx_split_tuning(dmrgx_ctx* c, int* out, int cap) {
+  ARG_CHECK(c && out && cap >= 8, "split_tuning: need a context and 8 slots");
+  ARG_CHECK(c->has_plan && c->sp.eb != 0, "split_tuning: no split-precision plan");
+  const SplitStage* st[2] = {&c->sp.s1, &c->sp.s2};
+  for (int i = 0; i < 2; i++) {
+    out[4 * i] = st[i]->cfg;
+    out[4 * i + 1] = st[i]->halve ? 1 : 0;
+    out[4 * i + 2] = (int)(st[i]->cap_scale * 100 + 0.5);
+    out[4 * i + 3] = st[i]->tuned ? 1 : 0;
+  }
+  return 0;
+}
+
 int dmrgx_set_schedule(dmrgx_ctx* c, int schedule) {
   ARG_CHECK(c, "null context");
   ARG_CHECK(schedule == DMRGX_SCHED_GROUPED || schedule == DMRGX_SCHED_PER_BLOCK,

@@ -61,6 +61,21 @@ struct SplitStage {
   CUtensorMap* d_maps = nullptr;
   int nslots = 0;
   bool full_cover = true;
+  // operand blocks of the stage's tensor maps: device address, logical padded
+  // K, rows, and whether it is a B operand (box rows = the tile width)
+  struct MapReq {
+    uint8_t* base;
+    int64_t kq, rows;
+    bool b_side;
+  };
+  std::vector<MapReq> req;
+  // tiling in use (chosen by the autotuner): kernel configuration, halving of
+  // blocks that fit one tile, scale of the K-split threshold
+  int cfg = 0;
+  bool halve = false;
+  double cap_scale = 1.0;
+  bool tuned = false;            // true: measured for this plan; false: from the cache / default
+  cudaStream_t st = nullptr;     // stream of the device arrays
   void free_device();
 };
 

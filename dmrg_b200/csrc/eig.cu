@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -399,12 +400,67 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
   double tol_cur = split ? std::max(tol, split_floor) : tol;
   int nev_cur = nev;
 
+  // One Lanczos cycle (steps kkeep..m-1: matvec, two classical Gram-Schmidt
+  // passes, normalisation) is captured once per (first step, basis buffer) into a
+  // CUDA graph and replayed; the per-block schedule and profiling run eagerly.
+  struct CycleGraph {
+    int first;
+    const double* V;
+    cudaGraphExec_t exec;
+  };
+  std::vector<CycleGraph> graphs;
+  struct GraphFree {
+    std::vector<CycleGraph>& g;
+    ~GraphFree() {
+      for (auto& x : g) cudaGraphExecDestroy(x.exec);
+    }
+  } graph_free{graphs};
+  const bool use_graph = !c->per_block && !c->prof && !getenv("DMRGX_NO_GRAPH");
+  auto run_cycle = [&](int first) -> int {
+    if (use_graph) {
+      for (auto& g : graphs)
+        if (g.first == first && g.V == L.V) {
+          L.matvecs += m - first;
+          EIG_TRY(cudaGraphLaunch(g.exec, L.s));
+          return 0;
+        }
+      cudaGraph_t gr = nullptr;
+      if (cudaStreamBeginCapture(L.s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        int r = 0;
+        for (int j = first; j < m && !r; j++) r = L.step(j);
+        const cudaError_t e = cudaStreamEndCapture(L.s, &gr);
+        cudaGraphExec_t ex = nullptr;
+        if (!r && e == cudaSuccess && gr && cudaGraphInstantiate(&ex, gr, 0) == cudaSuccess) {
+          cudaGraphDestroy(gr);
+          graphs.push_back({first, L.V, ex});
+          EIG_TRY(cudaGraphLaunch(ex, L.s));
+          return 0;
+        }
+        if (gr) cudaGraphDestroy(gr);
+        L.matvecs -= m - first;  // counted while capturing; run them eagerly below
+        cudaGetLastError();
+      }
+    }
+    for (int j = first; j < m; j++) {
+      const int r = L.step(j);
+      if (r) return r;
+    }
+    return 0;
+  };
+
   for (;;) {
     int mm = m;  // basis size reached this cycle
-    for (int j = kkeep; j < m; j++)
-      if ((rc = L.step(j))) return rc;
+    if ((rc = run_cycle(kkeep))) return rc;
     EIG_TRY(cudaMemcpyAsync(Th.data(), L.T, sizeof(double) * td * td, cudaMemcpyDeviceToHost, L.s));
+    int werr = 0;
+    if (split && c->err.p)
+      EIG_TRY(cudaMemcpyAsync(&werr, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, L.s));
     EIG_TRY(cudaStreamSynchronize(L.s));
+    if (werr) {
+      cudaMemsetAsync(c->err.p, 0, sizeof(int), L.s);
+      set_error("eigsolve: a bounded device wait timed out in the split-precision matvec");
+      return DMRGX_E_TIMEOUT;
+    }
     cycles++;
     // invariant subspace: a vanishing beta ends the basis early
     for (int j = kkeep; j < m; j++) {

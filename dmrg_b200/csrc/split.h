@@ -78,22 +78,31 @@ struct PadJob {
   int32_t kq, pad_;
 };
 
-int tc_smem_bytes();
+// Kernel configurations: cfg 0 tiles up to 256 columns with a 4-deep ring, cfg 1
+// up to 128 columns with a 7-deep ring.
+int tc_configs();
+int tc_cfg_tn(int cfg);
+int tc_cfg_stages(int cfg);
+int tc_smem_bytes(int cfg);
 int tc_tile_m();
-int tc_tile_n();
+int tc_tile_n();        // workspace row stride (floats): the widest tile of any cfg
 int tc_ktile_bytes();
 
 // Convert the rows listed in `rows` (one thread block each) into pair layout.
 cudaError_t launch_pad_split(int eb, const double* src, void* dst, const PadJob* jobs,
                              const PadRow* rows, int nrows, cudaStream_t st);
 
-// One stage: the warp-specialized TMA/tcgen05 kernel over `units`, then the
-// reduction of K-split tiles (if any).
-// One stage: the warp-specialized TMA/tcgen05 kernel, CTA c running units
-// [cta_begin[c], cta_begin[c+1]) in order, then the reduction of K-split tiles.
-cudaError_t launch_tc_gemm(int eb, bool out_split, const CUtensorMap* maps, const SUnit* units,
-                           const int* cta_begin, int nctas, const SOut* outs, const SSeg2* segs,
-                           void* c_pair, double* c64, float* ws, const SRed* reds,
-                           const SRedBlk* redblk, int nredblk, int* err, cudaStream_t st);
+// Shared-memory opt-in of the GEMM kernels on the current device; call before
+// launch_tc_gemm (not during a stream capture).
+cudaError_t prepare_tc_gemm();
+
+// One stage: the warp-specialized TMA/tcgen05 kernel of configuration cfg, CTA c
+// running units [cta_begin[c], cta_begin[c+1]) in order, then the reduction of
+// K-split tiles.
+cudaError_t launch_tc_gemm(int eb, bool out_split, int cfg, const CUtensorMap* maps,
+                           const SUnit* units, const int* cta_begin, int nctas, const SOut* outs,
+                           const SSeg2* segs, void* c_pair, double* c64, float* ws,
+                           const SRed* reds, const SRedBlk* redblk, int nredblk, int* err,
+                           cudaStream_t st);
 
 }  // namespace dmrgx

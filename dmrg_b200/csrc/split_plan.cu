@@ -20,23 +20,23 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <functional>
 #include <map>
+#include <mutex>
 #include <string>
 
 #include "../../include/dmrgx.h"
 #include "ctx.h"
+#include "devmem.h"
 #include "split.h"
 
 namespace dmrgx {
 
 void SplitStage::free_device() {
-  cudaFree(d_outs);
-  cudaFree(d_segs);
-  cudaFree(d_units);
-  cudaFree(d_cta_begin);
-  cudaFree(d_reds);
-  cudaFree(d_redblk);
-  cudaFree(d_maps);
+  for (void* p : {(void*)d_outs, (void*)d_segs, (void*)d_units, (void*)d_cta_begin, (void*)d_reds,
+                  (void*)d_redblk, (void*)d_maps})
+    dfree(p, st);
   d_outs = nullptr;
   d_segs = nullptr;
   d_units = nullptr;
@@ -49,8 +49,8 @@ void SplitStage::free_device() {
 void SplitPlan::free_device() {
   s1.free_device();
   s2.free_device();
-  cudaFree(d_psi_jobs);
-  cudaFree(d_psi_rows);
+  dfree(d_psi_jobs, s1.st);
+  dfree(d_psi_rows, s1.st);
   d_psi_jobs = nullptr;
   d_psi_rows = nullptr;
 }
@@ -106,22 +106,24 @@ bool make_map(CUtensorMap* m, int eb, void* base, int64_t kq, int64_t rows, int 
   return true;
 }
 
-// Tile width (columns of one work unit) of an output block with n columns.
-// Stage 1 halves wide blocks (more, smaller units, no partial sums); stage 2
-// keeps them whole and splits long K instead.
-int tile_width(int n, bool halve_wide) {
-  const int full = (int)std::min<int64_t>(256, rup(n, 16));
-  if (halve_wide && n > 128) return (int)rup((n + 1) / 2, 16);
-  return full;
+// Tile width (columns of one work unit) of an output block with n columns for a
+// kernel whose widest tile is tn: the fewest tiles that cover n, of equal width
+// rounded up to 16; `halve` cuts a block that fits one tile into two when it is
+// wider than 64 (more, smaller units).
+int tile_width(int n, int tn, bool halve) {
+  int k = (int)((n + tn - 1) / tn);
+  if (halve && k == 1 && n > 64) k = 2;
+  k = std::max(k, 1);
+  return (int)std::min<int64_t>(tn, rup((n + k - 1) / k, 16));
 }
 
 // Work units of one stage and their assignment to CTAs.
 // Cost of a unit (SM clock cycles, rough): the larger of its MMA issue time
 // (6 MMAs of N/2 cycles per k-tile) and its operand bytes at ~48 B/cycle, plus a
-// fixed 800.  Tiles costlier than half the mean CTA load are cut along K
-// (partials + fixed-order reduction).  Units go to CTAs longest-first onto the
-// least-loaded CTA.
-void make_units(SplitStage& st, int num_sms) {
+// fixed 800.  Tiles costlier than cap_scale x half the mean CTA load are cut
+// along K (partials + fixed-order reduction).  Units go to CTAs longest-first
+// onto the least-loaded CTA.
+void make_units(SplitStage& st, int num_sms, double cap_scale) {
   const int TM = tc_tile_m();
   const int A_B = TM * tc_ktile_bytes();
   struct T { int out, tm, tn, kt; double per_kt; };
@@ -130,7 +132,7 @@ void make_units(SplitStage& st, int num_sms) {
   for (size_t o = 0; o < st.outs.size(); o++) {
     const SOut& so = st.outs[o];
     int kt = 0;
-    for (int s = 0; s < so.seg_count; s++) kt += st.segs[so.seg_begin + s].nkt;
+    for (int q = 0; q < so.seg_count; q++) kt += st.segs[so.seg_begin + q].nkt;
     const int brows = so.seg_count ? st.segs[so.seg_begin].brows : so.tnw;
     const int tm = (so.m + TM - 1) / TM, tn = (so.n + so.tnw - 1) / so.tnw;
     for (int a = 0; a < tm; a++)
@@ -142,7 +144,7 @@ void make_units(SplitStage& st, int num_sms) {
         total += kt * per + 800;
       }
   }
-  const double cap = std::max(4000.0, 0.5 * total / std::max(1, num_sms));
+  const double cap = cap_scale * std::max(4000.0, 0.5 * total / std::max(1, num_sms));
   struct U { double cost; SUnit u; };
   std::vector<U> us;
   st.reds.clear();
@@ -197,14 +199,15 @@ void make_units(SplitStage& st, int num_sms) {
 
 template <class V, class P>
 int upload_vec(const std::vector<V>& v, P*& d, cudaStream_t s) {
-  cudaFree(d);
+  dfree(d, s);
   d = nullptr;
-  SP_TRY(cudaMalloc(&d, sizeof(V) * std::max<size_t>(1, v.size())));
+  SP_TRY(dalloc(&d, v.size(), s));
   if (!v.empty()) SP_TRY(cudaMemcpyAsync(d, v.data(), sizeof(V) * v.size(), cudaMemcpyHostToDevice, s));
   return 0;
 }
 
 int upload(SplitStage& st, cudaStream_t s) {
+  st.st = s;
   int rc = upload_vec(st.outs, st.d_outs, s);
   if (!rc) rc = upload_vec(st.segs, st.d_segs, s);
   if (!rc) rc = upload_vec(st.units, st.d_units, s);
@@ -228,19 +231,160 @@ int run_jobs(int eb, const double* src, void* dst, const std::vector<PadJob>& jo
   PadJob* d = nullptr;
   PadRow* dr = nullptr;
   const std::vector<PadRow> rows = rows_of(jobs);
-  SP_TRY(cudaMalloc(&d, sizeof(PadJob) * jobs.size()));
-  SP_TRY(cudaMalloc(&dr, sizeof(PadRow) * std::max<size_t>(1, rows.size())));
+  SP_TRY(dalloc(&d, jobs.size(), s));
+  SP_TRY(dalloc(&dr, rows.size(), s));
   SP_TRY(cudaMemcpyAsync(d, jobs.data(), sizeof(PadJob) * jobs.size(), cudaMemcpyHostToDevice, s));
   if (!rows.empty())
     SP_TRY(cudaMemcpyAsync(dr, rows.data(), sizeof(PadRow) * rows.size(), cudaMemcpyHostToDevice, s));
   SP_TRY(launch_pad_split(eb, src, dst, d, dr, (int)rows.size(), s));
-  SP_TRY(cudaStreamSynchronize(s));
-  cudaFree(d);
-  cudaFree(dr);
+  dfree(d, s);
+  dfree(dr, s);
   return 0;
 }
 
 }  // namespace
+
+// Apply one tiling to a stage: tile widths, B-box rows, tensor maps, work units,
+// workspace; uploads the descriptors.
+int configure_stage(dmrgx_ctx* c, SplitStage& st, int cfg, bool halve, double cap_scale) {
+  const int tn = tc_cfg_tn(cfg);
+  st.cfg = cfg;
+  st.halve = halve;
+  st.cap_scale = cap_scale;
+  for (auto& o : st.outs) o.tnw = tile_width(o.n, tn, halve);
+  st.maps.resize(st.req.size());
+  std::string why;
+  for (size_t i = 0; i < st.req.size(); i++) {
+    const auto& r = st.req[i];
+    const int box = r.b_side ? tile_width((int)r.rows, tn, halve) : tc_tile_m();
+    if (!make_map(&st.maps[i], c->sp.eb, r.base, r.kq, r.rows, box, why)) {
+      set_error("split plan: " + why);
+      return DMRGX_E_CUDA;
+    }
+  }
+  for (auto& g : st.segs) {
+    const auto& r = st.req[g.bmap];
+    g.brows = tile_width((int)r.rows, tn, halve);
+  }
+  make_units(st, c->num_sms, cap_scale);
+  const int slots = std::max(1, st.nslots);
+  SP_TRY(c->sws.ensure((size_t)slots * tc_tile_m() * tc_tile_n() * sizeof(float)));
+  return upload(st, c->stream);
+}
+
+namespace {
+
+// Autotuner of the split stages.  Key: the stage's block-shape histogram (the
+// multiset of output blocks' rows, columns and K-tile counts, rounded) and the
+// element type.  On a miss every candidate tiling -- kernel configuration
+// (256-column tiles / 4-deep ring or 128 / 7), halving of one-tile blocks,
+// K-split threshold x {0.5, 1, 2} -- is timed with CUDA events on the
+// context's stream (best of three launches after one warm-up, on the plan's own
+// buffers) and the fastest is kept for every later plan with the same histogram.
+struct TuneVal {
+  int cfg;
+  bool halve;
+  double cap_scale;
+};
+std::map<uint64_t, TuneVal> g_tune;
+std::mutex g_tune_mu;
+
+uint64_t stage_key(const SplitStage& st, int eb, int which) {
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&h](uint64_t v) { h ^= v + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2); };
+  mix((uint64_t)eb);
+  mix((uint64_t)which);
+  // shapes rounded (rows and columns to 64, K-tiles to 4) and sorted, so plans whose
+  // sector sizes differ a little share one entry
+  std::vector<uint64_t> shp;
+  for (const auto& o : st.outs) {
+    int kt = 0;
+    for (int q = 0; q < o.seg_count; q++) kt += st.segs[o.seg_begin + q].nkt;
+    shp.push_back(((uint64_t)rup(o.m, 64) << 40) | ((uint64_t)rup(o.n, 64) << 20) |
+                  (uint64_t)rup(kt, 4));
+  }
+  std::sort(shp.begin(), shp.end());
+  for (uint64_t v : shp) mix(v);
+  return h;
+}
+
+int launch_stage(dmrgx_ctx* c, int which) {
+  SplitPlan& sp = c->sp;
+  SplitStage& st = which == 1 ? sp.s1 : sp.s2;
+  uint8_t* stb = (uint8_t*)c->sstore.p;
+  SP_TRY(launch_tc_gemm(sp.eb, which == 1, st.cfg, st.d_maps, st.d_units, st.d_cta_begin,
+                        (int)st.cta_begin.size() - 1, st.d_outs, st.d_segs,
+                        which == 1 ? stb : nullptr, which == 1 ? nullptr : (double*)c->dout.p,
+                        (float*)c->sws.p, st.d_reds, st.d_redblk, (int)st.redblk.size(),
+                        (int*)c->err.p, c->stream));
+  return 0;
+}
+
+}  // namespace
+
+int tune_stage(dmrgx_ctx* c, int which) {
+  SplitPlan& sp = c->sp;
+  SplitStage& st = which == 1 ? sp.s1 : sp.s2;
+  const bool def_halve = which == 1;
+  const char* env = getenv("DMRGX_TUNE");
+  if (env && env[0] == '0') {
+    st.tuned = false;
+    return configure_stage(c, st, 0, def_halve, 1.0);
+  }
+  const uint64_t key = stage_key(st, sp.eb, which);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      st.tuned = false;
+      return configure_stage(c, st, it->second.cfg, it->second.halve, it->second.cap_scale);
+    }
+  }
+  cudaEvent_t e0, e1;
+  SP_TRY(cudaEventCreate(&e0));
+  SP_TRY(cudaEventCreate(&e1));
+  TuneVal best{0, def_halve, 1.0};
+  float best_ms = 1e30f;
+  int rc = 0;
+  for (int cfg = 0; cfg < tc_configs() && !rc; cfg++)
+    for (int hv = 0; hv < 2 && !rc; hv++)
+      for (double cs : {0.5, 1.0, 2.0}) {
+        rc = configure_stage(c, st, cfg, hv != 0, cs);
+        if (rc) break;
+        rc = launch_stage(c, which);  // warm-up
+        float ms = 1e30f;
+        for (int r = 0; r < 3 && !rc; r++) {
+          cudaEventRecord(e0, c->stream);
+          rc = launch_stage(c, which);
+          cudaEventRecord(e1, c->stream);
+          if (cudaEventSynchronize(e1) != cudaSuccess) rc = DMRGX_E_CUDA;
+          float t = 0;
+          cudaEventElapsedTime(&t, e0, e1);
+          ms = std::min(ms, t);
+        }
+        if (!rc && ms < best_ms) {
+          best_ms = ms;
+          best = TuneVal{cfg, hv != 0, cs};
+        }
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  int h = 0;
+  SP_TRY(cudaMemcpyAsync(&h, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  SP_TRY(cudaStreamSynchronize(c->stream));
+  if (h) {
+    set_error("split plan: a bounded device wait timed out while tuning");
+    return DMRGX_E_TIMEOUT;
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = best;
+  }
+  rc = configure_stage(c, st, best.cfg, best.halve, best.cap_scale);
+  st.tuned = true;
+  return rc;
+}
 
 int build_split_plan(dmrgx_ctx* c, int eb) {
   SplitPlan& sp = c->sp;
@@ -313,7 +457,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
     so.rstride = (int32_t)(2 * kq2);
     so.seg_begin = (int32_t)sp.s1.segs.size();
     so.seg_count = d.seg_count;
-    so.tnw = tile_width(d.n, true);
+    so.tnw = 0;  // set by configure_stage
     for (int q = 0; q < d.seg_count; q++) {
       const DSeg& g = f1.segs[d.seg_begin + q];
       const int64_t kq = rup(g.k, CH);
@@ -330,12 +474,12 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
       if (ib == psi_map.end()) {
         sp.psi_jobs.push_back(PadJob{g.b_off, psi_len, d.n, 1, g.k, g.k, (int32_t)kq, 0});
         psi_map[g.b_off] = (int)req1.size();
-        req1.push_back({1, psi_len, kq, d.n, tile_width(d.n, true)});
+        req1.push_back({1, psi_len, kq, d.n, 0});
         psi_len += (int64_t)d.n * 2 * kq;
       }
       ss.bmap = psi_map[g.b_off];
       ss.nkt = (int32_t)(kq / CH);
-      ss.brows = req1[ss.bmap].box_rows;
+      ss.brows = 0;  // set by configure_stage
       sp.s1.segs.push_back(ss);
     }
     sp.s1.outs.push_back(so);
@@ -357,7 +501,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
     so.rstride = 0;
     so.seg_begin = (int32_t)sp.s2.segs.size();
     so.seg_count = d.seg_count;
-    so.tnw = tile_width(d.n, false);
+    so.tnw = 0;
     for (int q = 0; q < d.seg_count; q++) {
       const DSeg& g = f2.segs[d.seg_begin + q];
       const int N1 = st_shape[g.b_off].second;
@@ -375,18 +519,16 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
       auto ib = stb_map.find(g.b_off);
       if (ib == stb_map.end()) {
         stb_map[g.b_off] = (int)req2.size();
-        req2.push_back({3, st_off[g.b_off], kq2, d.n, tile_width(d.n, false)});
+        req2.push_back({3, st_off[g.b_off], kq2, d.n, 0});
       }
       ss.bmap = stb_map[g.b_off];
       ss.nkt = (int32_t)(kq2 / CH);
-      ss.brows = req2[ss.bmap].box_rows;
+      ss.brows = 0;
       sp.s2.segs.push_back(ss);
     }
     sp.s2.outs.push_back(so);
   }
   sp.s2.full_cover = f2.full_cover;
-  make_units(sp.s1, c->num_sms);
-  make_units(sp.s2, c->num_sms);
   auto len = [eb](int64_t n) { return rup(std::max<int64_t>(n, 1), 256 / eb); };
   sp.a1_len = len(a1_len);
   sp.a2_len = len(a2_len);
@@ -400,8 +542,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
   SP_TRY(c->sa2.ensure(sp.a2_len * eb));
   SP_TRY(c->spsi.ensure(sp.psi_len * eb));
   SP_TRY(c->sstore.ensure(sp.store_len * eb));
-  const int slots = std::max(1, std::max(sp.s1.nslots, sp.s2.nslots));
-  SP_TRY(c->sws.ensure((size_t)slots * tc_tile_m() * tc_tile_n() * sizeof(float)));
+  SP_TRY(prepare_tc_gemm());
   SP_TRY(c->err.ensure(16));
   SP_TRY(cudaMemsetAsync(c->sa1.p, 0, sp.a1_len * eb, s));
   SP_TRY(cudaMemsetAsync(c->sa2.p, 0, sp.a2_len * eb, s));
@@ -416,29 +557,23 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
   if (rc) return rc;
   rc = run_jobs(eb, (const double*)c->lenv.p, a2, a2_jobs, s);
   if (rc) return rc;
-  // ---- tensor maps
-  std::string why;
-  auto build_maps = [&](const std::vector<MapReq>& req, std::vector<CUtensorMap>& out) -> bool {
-    out.resize(req.size());
-    for (size_t i = 0; i < req.size(); i++) {
-      const MapReq& r = req[i];
+  // ---- operand blocks of the tensor maps
+  auto to_req = [&](const std::vector<MapReq>& req, SplitStage& st) {
+    st.req.clear();
+    for (const MapReq& r : req) {
       uint8_t* base = r.which == 0 ? a1 : r.which == 1 ? psi : r.which == 2 ? a2 : stb;
-      if (!make_map(&out[i], eb, base + r.off * eb, r.kq, r.rows, r.box_rows, why)) return false;
+      st.req.push_back({base + r.off * eb, r.kq, r.rows, r.which == 1 || r.which == 3});
     }
-    return true;
   };
-  if (!build_maps(req1, sp.s1.maps) || !build_maps(req2, sp.s2.maps)) {
-    set_error("split plan: " + why);
-    return DMRGX_E_CUDA;
-  }
-  rc = upload(sp.s1, s);
-  if (!rc) rc = upload(sp.s2, s);
-  if (rc) return rc;
+  to_req(req1, sp.s1);
+  to_req(req2, sp.s2);
+  sp.eb = eb;
   rc = upload_vec(sp.psi_jobs, sp.d_psi_jobs, s);
   if (!rc) rc = upload_vec(sp.psi_rows, sp.d_psi_rows, s);
+  if (!rc) rc = tune_stage(c, 1);
+  if (!rc) rc = tune_stage(c, 2);
   if (rc) return rc;
   SP_TRY(cudaStreamSynchronize(s));
-  sp.eb = eb;
   return 0;
 }
 
@@ -452,13 +587,13 @@ int run_matvec_split(dmrgx_ctx* c, const double* in, double* out) {
   SP_TRY(launch_pad_split(eb, in, psi, sp.d_psi_jobs, sp.d_psi_rows, (int)sp.psi_rows.size(),
                           s));
   c->prof_mark();
-  SP_TRY(launch_tc_gemm(eb, true, sp.s1.d_maps, sp.s1.d_units, sp.s1.d_cta_begin,
+  SP_TRY(launch_tc_gemm(eb, true, sp.s1.cfg, sp.s1.d_maps, sp.s1.d_units, sp.s1.d_cta_begin,
                         (int)sp.s1.cta_begin.size() - 1, sp.s1.d_outs, sp.s1.d_segs, stb, nullptr,
                         (float*)c->sws.p, sp.s1.d_reds, sp.s1.d_redblk,
                         (int)sp.s1.redblk.size(), (int*)c->err.p, s));
   c->prof_mark();
   if (!sp.s2.full_cover) SP_TRY(cudaMemsetAsync(out, 0, sizeof(double) * c->n, s));
-  SP_TRY(launch_tc_gemm(eb, false, sp.s2.d_maps, sp.s2.d_units, sp.s2.d_cta_begin,
+  SP_TRY(launch_tc_gemm(eb, false, sp.s2.cfg, sp.s2.d_maps, sp.s2.d_units, sp.s2.d_cta_begin,
                         (int)sp.s2.cta_begin.size() - 1, sp.s2.d_outs, sp.s2.d_segs, nullptr,
                         out, (float*)c->sws.p, sp.s2.d_reds, sp.s2.d_redblk,
                         (int)sp.s2.redblk.size(), (int*)c->err.p, s));

@@ -49,15 +49,11 @@ namespace {
 
 constexpr int THREADS = 192;
 constexpr int TM = 128;
-constexpr int TNMAX = 256;
-constexpr int STAGES = 4;
+constexpr int TNMAX = 256;                    // widest tile; also the workspace row stride
 constexpr int ROWB = 128;                     // bytes per row of one k-tile (hi + lo)
 constexpr int HALF = 64;                      // byte offset of the lo parts in a row
 constexpr int A_BYTES = TM * ROWB;            // 16 KB
-constexpr int B_BYTES = TNMAX * ROWB;         // 32 KB
-constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int SBO = 8 * ROWB;                 // 1 KB between 8-row atoms
-constexpr uint32_t TMEM_COLS = 512;           // two 256-column accumulators
 constexpr uint64_t WAIT_NS = 2000000000ull;  // a wait gives up after 2 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -215,12 +211,18 @@ __device__ __forceinline__ void store16(const SOut& o, int row, int col0, const 
   }
 }
 
-template <int EB, bool OUT_SPLIT>
+// TNX: widest tile (MMA N) of this instantiation; STAGES: depth of the ring.
+// Configurations: (256, 4) and (128, 7) -- the narrow one keeps more k-tiles in
+// flight for the same shared memory.
+template <int EB, bool OUT_SPLIT, int TNX, int STAGES>
 __global__ void __launch_bounds__(THREADS, 1)
 tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ units,
                 const int* __restrict__ cta_begin, const SOut* __restrict__ outs,
                 const SSeg2* __restrict__ segs, uint8_t* __restrict__ c_pair,
                 double* __restrict__ c64, float* __restrict__ ws, int* __restrict__ err) {
+  constexpr int B_BYTES = TNX * ROWB;
+  constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  constexpr uint32_t TMEM_COLS = 2 * TNX;  // two accumulators
   extern __shared__ uint8_t smem_raw[];
   // 1024-aligned ring (the swizzle pattern repeats every 512 B)
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
@@ -315,7 +317,7 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
           break;
         }
         tc_fence_after();
-        const uint32_t tacc = tmem + acc * TNMAX;
+        const uint32_t tacc = tmem + acc * TNX;
         int s = o.seg_begin, base = 0;
         while (s < o.seg_begin + o.seg_count && base + segs[s].nkt <= un.kt0) {
           base += segs[s].nkt;
@@ -376,7 +378,7 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
         }
         tc_fence_after();
       }
-      const uint32_t taddr = tmem + acc * TNMAX + ((uint32_t)(q * 32) << 16);
+      const uint32_t taddr = tmem + acc * TNX + ((uint32_t)(q * 32) << 16);
       for (int cc = 0; cc < nmma; cc += 16) {
         float v[16];
         if (has) {
@@ -474,34 +476,68 @@ split_reduce(const SRed* __restrict__ reds, const SRedBlk* __restrict__ blks,
 
 }  // namespace
 
-int tc_smem_bytes() { return STAGES * STAGE_BYTES + 1024 + (2 * STAGES + 4) * 8 + 16; }
+int tc_configs() { return 2; }
+int tc_cfg_tn(int cfg) { return cfg == 0 ? 256 : 128; }
+int tc_cfg_stages(int cfg) { return cfg == 0 ? 4 : 7; }
+int tc_smem_bytes(int cfg) {
+  const int st = tc_cfg_stages(cfg);
+  return st * (A_BYTES + tc_cfg_tn(cfg) * ROWB) + 1024 + (2 * st + 4) * 8 + 16;
+}
 int tc_tile_m() { return TM; }
-int tc_tile_n() { return TNMAX; }
+int tc_tile_n() { return TNMAX; }  // workspace row stride (floats)
 int tc_ktile_bytes() { return ROWB; }
 
-cudaError_t launch_tc_gemm(int eb, bool out_split, const CUtensorMap* maps, const SUnit* units,
-                           const int* cta_begin, int nctas, const SOut* outs, const SSeg2* segs,
-                           void* c_pair, double* c64, float* ws, const SRed* reds,
-                           const SRedBlk* redblk, int nredblk, int* err, cudaStream_t st) {
+// Opt the kernels into their shared memory on the current device (once per plan,
+// outside any stream capture).
+cudaError_t prepare_tc_gemm() {
+  cudaError_t e = cudaSuccess;
+#define DMRGX_TC_ATTR(EB, OS, TN, ST, CFG)                                    \
+  if (e == cudaSuccess)                                                       \
+    e = cudaFuncSetAttribute(tc_grouped_gemm<EB, OS, TN, ST>,                 \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_bytes(CFG));
+  DMRGX_TC_ATTR(2, true, 256, 4, 0)
+  DMRGX_TC_ATTR(2, false, 256, 4, 0)
+  DMRGX_TC_ATTR(4, true, 256, 4, 0)
+  DMRGX_TC_ATTR(4, false, 256, 4, 0)
+  DMRGX_TC_ATTR(2, true, 128, 7, 1)
+  DMRGX_TC_ATTR(2, false, 128, 7, 1)
+  DMRGX_TC_ATTR(4, true, 128, 7, 1)
+  DMRGX_TC_ATTR(4, false, 128, 7, 1)
+#undef DMRGX_TC_ATTR
+  return e;
+}
+
+cudaError_t launch_tc_gemm(int eb, bool out_split, int cfg, const CUtensorMap* maps,
+                           const SUnit* units, const int* cta_begin, int nctas, const SOut* outs,
+                           const SSeg2* segs, void* c_pair, double* c64, float* ws,
+                           const SRed* reds, const SRedBlk* redblk, int nredblk, int* err,
+                           cudaStream_t st) {
   if (nctas <= 0) return cudaSuccess;
-  const int sm = tc_smem_bytes();
-#define DMRGX_TC_LAUNCH(EB, OS)                                                               \
+  const int sm = tc_smem_bytes(cfg);
+#define DMRGX_TC_LAUNCH(EB, OS, TN, STG)                                                      \
   do {                                                                                        \
-    cudaError_t e = cudaFuncSetAttribute(tc_grouped_gemm<EB, OS>,                             \
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, sm);    \
-    if (e != cudaSuccess) return e;                                                           \
-    tc_grouped_gemm<EB, OS><<<nctas, THREADS, sm, st>>>(maps, units, cta_begin, outs, segs,   \
-                                                       (uint8_t*)c_pair, c64, ws, err);       \
+    tc_grouped_gemm<EB, OS, TN, STG><<<nctas, THREADS, sm, st>>>(                              \
+        maps, units, cta_begin, outs, segs, (uint8_t*)c_pair, c64, ws, err);                  \
     if (nredblk > 0)                                                                          \
       split_reduce<EB, OS><<<nredblk, 256, 0, st>>>(reds, redblk, outs, ws, (uint8_t*)c_pair, \
                                                    c64);                                      \
   } while (0)
-  if (eb == 2) {
-    if (out_split) DMRGX_TC_LAUNCH(2, true);
-    else DMRGX_TC_LAUNCH(2, false);
+  if (cfg == 0) {
+    if (eb == 2) {
+      if (out_split) DMRGX_TC_LAUNCH(2, true, 256, 4);
+      else DMRGX_TC_LAUNCH(2, false, 256, 4);
+    } else {
+      if (out_split) DMRGX_TC_LAUNCH(4, true, 256, 4);
+      else DMRGX_TC_LAUNCH(4, false, 256, 4);
+    }
   } else {
-    if (out_split) DMRGX_TC_LAUNCH(4, true);
-    else DMRGX_TC_LAUNCH(4, false);
+    if (eb == 2) {
+      if (out_split) DMRGX_TC_LAUNCH(2, true, 128, 7);
+      else DMRGX_TC_LAUNCH(2, false, 128, 7);
+    } else {
+      if (out_split) DMRGX_TC_LAUNCH(4, true, 128, 7);
+      else DMRGX_TC_LAUNCH(4, false, 128, 7);
+    }
   }
 #undef DMRGX_TC_LAUNCH
   return cudaGetLastError();

@@ -42,6 +42,7 @@ SIGNATURES = {
     "dmrgx_dmrg": (_i, [_vp, _i, _i, _i, _i, _i, _dp, _i, _dp, _dp, _ip, _i64p, _i64, _i64p,
                         _dp]),
     "dmrgx_set_schedule": (_i, [_vp, _i]),
+    "dmrgx_split_tuning": (_i, [_vp, _ip, _i]),
     "dmrgx_adjoint": (_i, [_vp, _i, _dp, _i, _dp, _i64, _i64p, _dp, _dp]),
     "dmrgx_expect": (_i, [_vp, _dp, _i, _dp]),
     "dmrgx_profile": (_i, [_vp, _i]),
@@ -139,6 +140,13 @@ class Context:
 
     def set_precision(self, prec):
         _check(lib().dmrgx_set_precision(self.ptr, prec))
+
+    def split_tuning(self):
+        """Autotuner choice per split stage: list of (cfg, halve, cap_scale, tuned)."""
+        out = np.zeros(8, np.int32)
+        _check(lib().dmrgx_split_tuning(self.ptr, _ip(out), 8))
+        return [(int(out[4 * i]), bool(out[4 * i + 1]), out[4 * i + 2] / 100.0, bool(out[4 * i + 3]))
+                for i in range(2)]
 
     def set_schedule(self, schedule):
         """SCHED_GROUPED (default) or SCHED_PER_BLOCK (one cuBLAS GEMM per task row)."""

@@ -73,6 +73,17 @@ void dmrgx_ctx_destroy(dmrgx_ctx* ctx);
 /* Select the matvec arithmetic (DMRGX_PREC_*).  Default FP64. */
 int dmrgx_set_precision(dmrgx_ctx* ctx, int prec);
 
+/* The tiling the autotuner chose for the current split-precision plan.  The
+ * split stages run one of two kernel configurations (tiles up to 256 columns
+ * with a 4-deep shared-memory ring, or up to 128 with a 7-deep ring); when a
+ * plan's block-shape histogram (rows, columns and K-tiles of every output block,
+ * rounded) is new, every candidate tiling is timed once on the device and the
+ * fastest is cached for later plans (DMRGX_TUNE=0 in the environment turns the
+ * tuner off).  out[0..3] stage 1, out[4..7] stage 2: configuration, halving of
+ * one-tile blocks, K-split threshold scale x100, 1 if measured for this plan
+ * (0: from the cache).  cap >= 8. */
+int dmrgx_split_tuning(dmrgx_ctx* ctx, int* out, int cap);
+
 /* Select the launch schedule of the matvec (DMRGX_SCHED_*).  Default grouped.
  * The per-block schedule is the plain FP64 GPU path: same plan, same
  * eigensolver, one library GEMM per task row with the row's sign as alpha. */
