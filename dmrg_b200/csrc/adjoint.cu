@@ -26,6 +26,7 @@
 
 #include "../../include/dmrgx.h"
 #include "adjoint.h"
+#include "devmem.h"
 #include "kernels.h"
 
 namespace dmrgx {
@@ -58,13 +59,13 @@ GSrc gsrc(int64_t off, const std::vector<int64_t>& strides, double sign, bool co
   return g;
 }
 
-// scoped device array of doubles
+// scoped device array of doubles (stream-ordered)
 struct DevArr {
   double* p = nullptr;
-  cudaError_t alloc(int64_t n) { return cudaMalloc(&p, sizeof(double) * std::max<int64_t>(1, n)); }
-  ~DevArr() {
-    if (p) cudaFree(p);
-  }
+  cudaStream_t s = nullptr;
+  explicit DevArr(cudaStream_t st) : s(st) {}
+  cudaError_t alloc(int64_t n) { return dalloc(&p, (size_t)std::max<int64_t>(1, n), s); }
+  ~DevArr() { dfree(p, s); }
 };
 
 int64_t label_key(const std::vector<int>& st, const std::vector<std::vector<int>>& dim) {
@@ -166,7 +167,7 @@ int heff_adjoint(dmrgx_ctx* c, const Engine& E, const QTensor& Lop, const QTenso
   const bool cplx = f == 2;
   const int64_t n = c->n;
   const cudaStream_t st = E.stream;
-  DevArr out;
+  DevArr out(st);
   if (out.alloc(n * f) != cudaSuccess) {
     err = "adjoint: allocation failed";
     return DMRGX_E_CUDA;
@@ -202,7 +203,7 @@ int heff_adjoint(dmrgx_ctx* c, const Engine& E, const QTensor& Lop, const QTenso
   cudaError_t e = cudaSuccess;
 
   // conj(psi) and -conj(psi): the A operand of dE/dLop carries alpha by choice of image
-  DevArr cpsi;
+  DevArr cpsi(st);
   if (want_l) {
     if (cpsi.alloc(2 * n * f) != cudaSuccess) {
       err = "adjoint: allocation failed";
@@ -235,7 +236,7 @@ int heff_adjoint(dmrgx_ctx* c, const Engine& E, const QTensor& Lop, const QTenso
       err = "adjoint: store transpose descriptors out of range";
       return DMRGX_E_STATE;
     }
-    DevArr stT;
+    DevArr stT(st);
     e = stT.alloc(stl * f);
     if (e == cudaSuccess && !go.empty()) e = launch_gather(store, stT.p, go, gs, cplx, st);
     gl = std::make_shared<QTensor>();
@@ -287,7 +288,7 @@ int heff_adjoint(dmrgx_ctx* c, const Engine& E, const QTensor& Lop, const QTenso
       err = "adjoint: transpose descriptors out of range";
       return DMRGX_E_STATE;
     }
-    DevArr pT, lT, dstore;
+    DevArr pT(st), lT(st), dstore(st);
     e = pT.alloc(ptl * f);
     if (e == cudaSuccess) e = lT.alloc(ltl * f);
     if (e == cudaSuccess) e = dstore.alloc(c->d_store * f);
@@ -331,7 +332,7 @@ int heff_adjoint(dmrgx_ctx* c, const Engine& E, const QTensor& Lop, const QTenso
       err = "adjoint: psi transpose descriptors out of range";
       return DMRGX_E_STATE;
     }
-    DevArr qT;
+    DevArr qT(st);
     if (e == cudaSuccess) e = qT.alloc(qtl * f);
     if (e == cudaSuccess && !go.empty()) e = launch_gather(psi, qT.p, go, gs, cplx, st);
     gr = std::make_shared<QTensor>();
@@ -434,7 +435,7 @@ int fusion_adjoint(const Engine& E, const QTensor& env, const QTensor& W, const 
     err = "fusion adjoint: descriptors out of range";
     return DMRGX_E_STATE;
   }
-  DevArr part;
+  DevArr part(E.stream);
   cudaError_t e = part.alloc(partl * f);
   if (e == cudaSuccess) e = qt_grouped_gemm(E, env.d, gfused.d, part.p, outs, segs);
   std::vector<double> hp((size_t)(partl * f));

@@ -8,6 +8,7 @@
 
 #include "../../include/dmrgx.h"
 #include "ctx.h"
+#include "devmem.h"
 #include "kernels.h"
 #include "qtensor.h"
 #include "split.h"
@@ -438,6 +439,7 @@ int dmrgx_ctx_create(dmrgx_ctx** out, int dtype, int device) {
     set_error("ctx_create: this library is built for sm_100a (Blackwell B200)");
     return DMRGX_E_CUDA;
   }
+  keep_pool(device);
   e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete c;

@@ -19,6 +19,7 @@
 #include "../../include/dmrgx.h"
 #include "adjoint.h"
 #include "ctx.h"
+#include "devmem.h"
 #include "qtensor.h"
 
 namespace dmrgx {
@@ -499,13 +500,13 @@ struct Run {
     rc = plan_build_device(c, *F.lop, *F.rop, F.ln, F.rn, sector, E.G);
     if (rc) return fail(rc);
     double* d = nullptr;
-    if (cudaMalloc(&d, sizeof(double) * std::max<int64_t>(1, c->n * c->f())) != cudaSuccess) {
+    if (dalloc(&d, (size_t)std::max<int64_t>(1, c->n * c->f()), E.stream) != cudaSuccess) {
       err = "centre allocation failed";
       return DMRGX_E_CUDA;
     }
     rc = to_plan(*cpsi, d);
     if (!rc) rc = heff_adjoint(c, E, *F.lop, *F.rop, d, want_l, want_r, gl, gr, en, nn, err);
-    cudaFree(d);
+    dfree(d, E.stream);
     return rc;
   }
 

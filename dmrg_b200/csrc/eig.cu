@@ -31,6 +31,7 @@
 
 #include "../../include/dmrgx.h"
 #include "ctx.h"
+#include "devmem.h"
 
 namespace dmrgx {
 
@@ -234,15 +235,16 @@ void jacobi_eig(std::vector<double> A, int m, std::vector<double>& w, std::vecto
 
 struct DevMem {
   std::vector<void*> ptrs;
+  cudaStream_t s = nullptr;
   ~DevMem() {
-    for (void* p : ptrs) cudaFree(p);
+    for (void* p : ptrs) dfree(p, s);
   }
   template <class T>
   cudaError_t alloc(T*& p, size_t count) {
-    void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, sizeof(T) * std::max<size_t>(1, count));
+    T* q = nullptr;
+    cudaError_t e = dalloc(&q, count, s);
     if (e == cudaSuccess) ptrs.push_back(q);
-    p = (T*)q;
+    p = q;
     return e;
   }
 };
@@ -271,6 +273,7 @@ struct Lanczos {
   double* col(double* M, int j) { return M + (int64_t)j * len; }
 
   int init() {
+    mem.s = s;
     EIG_TRY(mem.alloc(V, (size_t)len * (m + 1)));
     EIG_TRY(mem.alloc(V2, (size_t)len * (m + 1)));
     EIG_TRY(mem.alloc(w, (size_t)len));

@@ -17,21 +17,21 @@
 #include <map>
 #include <mutex>
 
+#include "devmem.h"
 #include "kernels.h"
 #include "qtensor.h"
 
 namespace dmrgx {
 
-QTensor::~QTensor() {
-  if (d) cudaFree(d);
-}
+QTensor::~QTensor() { dfree(d, st); }
 
 cudaError_t QTensor::alloc(cudaStream_t s) {
   off.assign(m.syms.size() + 1, 0);
   for (size_t b = 0; b < m.syms.size(); b++) off[b + 1] = off[b] + m.block_size((int)b);
-  if (d) cudaFree(d);
+  dfree(d, st);
   d = nullptr;
-  cudaError_t e = cudaMalloc(&d, sizeof(double) * std::max<int64_t>(1, total() * f));
+  st = s;
+  cudaError_t e = dalloc(&d, (size_t)std::max<int64_t>(1, total() * f), s);
   if (e != cudaSuccess) return e;
   return cudaMemsetAsync(d, 0, sizeof(double) * std::max<int64_t>(1, total() * f), s);
 }
@@ -42,9 +42,10 @@ namespace {
 struct DevGather {
   GOut* outs = nullptr;
   GSrc* srcs = nullptr;
+  cudaStream_t s = nullptr;
   ~DevGather() {
-    cudaFree(outs);
-    cudaFree(srcs);
+    dfree(outs, s);
+    dfree(srcs, s);
   }
 };
 
@@ -153,9 +154,9 @@ cudaError_t run_gemms(const Engine& E, const double* A, const double* B, double*
   DOut* d_o = nullptr;
   DSeg* d_s = nullptr;
   DTile* d_t = nullptr;
-  cudaError_t e = cudaMalloc(&d_o, sizeof(DOut) * outs.size());
-  if (e == cudaSuccess) e = cudaMalloc(&d_s, sizeof(DSeg) * std::max<size_t>(1, segs.size()));
-  if (e == cudaSuccess) e = cudaMalloc(&d_t, sizeof(DTile) * tiles.size());
+  cudaError_t e = dalloc(&d_o, outs.size(), E.stream);
+  if (e == cudaSuccess) e = dalloc(&d_s, segs.size(), E.stream);
+  if (e == cudaSuccess) e = dalloc(&d_t, tiles.size(), E.stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(d_o, outs.data(), sizeof(DOut) * outs.size(), cudaMemcpyHostToDevice, E.stream);
   if (e == cudaSuccess && !segs.empty())
@@ -165,10 +166,9 @@ cudaError_t run_gemms(const Engine& E, const double* A, const double* B, double*
   if (e == cudaSuccess)
     e = launch_grouped_f64(A, B, C, d_t, (int)tiles.size(), d_o, d_s, E.f == 2, E.num_sms * 3,
                            E.stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
-  cudaFree(d_o);
-  cudaFree(d_s);
-  cudaFree(d_t);
+  dfree(d_o, E.stream);
+  dfree(d_s, E.stream);
+  dfree(d_t, E.stream);
   return e;
 }
 
@@ -256,8 +256,9 @@ cudaError_t launch_gather(const double* src, double* dst, const std::vector<GOut
                           const std::vector<GSrc>& srcs, bool cplx, cudaStream_t st) {
   if (outs.empty()) return cudaSuccess;
   DevGather g;
-  cudaError_t e = cudaMalloc(&g.outs, sizeof(GOut) * outs.size());
-  if (e == cudaSuccess) e = cudaMalloc(&g.srcs, sizeof(GSrc) * std::max<size_t>(1, srcs.size()));
+  g.s = st;
+  cudaError_t e = dalloc(&g.outs, outs.size(), st);
+  if (e == cudaSuccess) e = dalloc(&g.srcs, srcs.size(), st);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(g.outs, outs.data(), sizeof(GOut) * outs.size(), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && !srcs.empty())
@@ -273,7 +274,6 @@ cudaError_t launch_gather(const double* src, double* dst, const std::vector<GOut
       gather_kernel<false><<<grid, 256, 0, st>>>(src, dst, g.outs + y0, g.srcs);
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   return e;
 }
 
@@ -423,9 +423,9 @@ QTPtr qt_contract_legs(const Engine& E, const QTensor& A, int a, const QTensor& 
     lc += al * ar * bl * br;
   }
   double *dA = nullptr, *dB = nullptr, *dC = nullptr;
-  cudaError_t e = cudaMalloc(&dA, sizeof(double) * std::max<int64_t>(1, la * f));
-  if (e == cudaSuccess) e = cudaMalloc(&dB, sizeof(double) * std::max<int64_t>(1, lb * f));
-  if (e == cudaSuccess) e = cudaMalloc(&dC, sizeof(double) * std::max<int64_t>(1, lc * f));
+  cudaError_t e = dalloc(&dA, (size_t)(la * f), E.stream);
+  if (e == cudaSuccess) e = dalloc(&dB, (size_t)(lb * f), E.stream);
+  if (e == cudaSuccess) e = dalloc(&dC, (size_t)(lc * f), E.stream);
   std::vector<GOut> go;
   std::vector<GSrc> gs;
   std::vector<DOut> douts;
@@ -512,9 +512,9 @@ QTPtr qt_contract_legs(const Engine& E, const QTensor& A, int a, const QTensor& 
     }
     e = launch_gather(dC, T->d, go, gs, f == 2, E.stream);
   }
-  cudaFree(dA);
-  cudaFree(dB);
-  cudaFree(dC);
+  dfree(dA, E.stream);
+  dfree(dB, E.stream);
+  dfree(dC, E.stream);
   if (e != cudaSuccess) {
     err = std::string("contract: ") + cudaGetErrorString(e);
     return nullptr;
@@ -649,8 +649,8 @@ QTPtr qt_contract_mat(const Engine& E, const QTensor& A, const QTensor& B, char 
   }
   double *dA = nullptr, *dB = nullptr;
   cudaError_t e = cudaSuccess;
-  if (la) e = cudaMalloc(&dA, sizeof(double) * la * f);
-  if (e == cudaSuccess && lb) e = cudaMalloc(&dB, sizeof(double) * lb * f);
+  if (la) e = dalloc(&dA, (size_t)(la * f), E.stream);
+  if (e == cudaSuccess && lb) e = dalloc(&dB, (size_t)(lb * f), E.stream);
   if (e == cudaSuccess && la) e = launch_gather(A.d, dA, goa, gsa, f == 2, E.stream);
   if (e == cudaSuccess && lb) e = launch_gather(B.d, dB, gob, gsb, f == 2, E.stream);
   // both staged operands live in one buffer pair: A side and B side
@@ -688,8 +688,8 @@ QTPtr qt_contract_mat(const Engine& E, const QTensor& A, const QTensor& B, char 
     // the GEMM kernel takes one A and one B base: both operands may be staged
     e = run_gemms(E, Abase, Bbase, T->d, douts, dsegs);
   }
-  cudaFree(dA);
-  cudaFree(dB);
+  dfree(dA, E.stream);
+  dfree(dB, E.stream);
   if (e != cudaSuccess) {
     err = std::string("contract: ") + cudaGetErrorString(e);
     return nullptr;
@@ -802,7 +802,7 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
   };
   // place every block into its sector matrix (row-major R x C)
   double* dM = nullptr;
-  cudaError_t e = cudaMalloc(&dM, sizeof(double) * std::max<int64_t>(1, moff[ns] * f));
+  cudaError_t e = dalloc(&dM, (size_t)std::max<int64_t>(1, moff[ns] * f), E.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(dM, 0, sizeof(double) * std::max<int64_t>(1, moff[ns] * f), E.stream);
   std::vector<GOut> go;
   std::vector<GSrc> gs;
@@ -820,74 +820,93 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
   }
   if (e == cudaSuccess) e = launch_gather(A.d, dM, go, gs, f == 2, E.stream);
   if (e != cudaSuccess) {
-    cudaFree(dM);
+    dfree(dM, E.stream);
     err = std::string("svd: ") + cudaGetErrorString(e);
     return -1;
   }
   if (!load_solver(err) || !thread_handle(err)) {
-    cudaFree(dM);
+    dfree(dM, E.stream);
     return -1;
   }
-  // per-sector SVD of X = A^T (column-major C x R view of the row-major block)
+  // per-sector SVD of X = A^T (column-major C x R view of the row-major block),
+  // all sectors queued on the stream, one synchronisation at the end
   std::vector<std::vector<double>> S(ns);
   std::vector<double*> Ux(ns, nullptr), Vx(ns, nullptr);
+  std::vector<int64_t> soff(ns + 1, 0);
+  for (int i = 0; i < ns; i++) soff[i + 1] = soff[i] + std::min(Cc[i], Rr[i]);
   int* dinfo = nullptr;
-  cudaMalloc(&dinfo, sizeof(int));
-  bool fail = false;
+  double *dS = nullptr, *work = nullptr;
+  bool fail = dalloc(&dinfo, (size_t)std::max(1, ns), E.stream) != cudaSuccess ||
+              dalloc(&dS, (size_t)std::max<int64_t>(1, soff[ns]), E.stream) != cudaSuccess;
   g_sol.set_stream(t_sol.h, E.stream);
+  int lmax = 1;
+  cusolverStatus_t st = CUSOLVER_STATUS_SUCCESS;
   for (int i = 0; i < ns && !fail; i++) {
     const int m = (int)Cc[i], n = (int)Rr[i];
-    const int mn = std::min(m, n);
-    S[i].assign(mn, 0.0);
-    if (mn == 0) continue;
-    double *dS = nullptr, *work = nullptr;
-    cudaMalloc(&Ux[i], sizeof(double) * (size_t)m * m * f);
-    cudaMalloc(&Vx[i], sizeof(double) * (size_t)n * n * f);
-    cudaMalloc(&dS, sizeof(double) * mn);
+    S[i].assign(std::min(m, n), 0.0);
+    if (std::min(m, n) == 0) continue;
+    if (dalloc(&Ux[i], (size_t)m * m * f, E.stream) != cudaSuccess ||
+        dalloc(&Vx[i], (size_t)n * n * f, E.stream) != cudaSuccess) {
+      fail = true;
+      break;
+    }
     int lwork = 0;
-    cusolverStatus_t st;
+    double* X = dM + moff[i] * f;
+    if (f == 1)
+      st = g_sol.d_buf(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, X, m, dS + soff[i], Ux[i], m,
+                       Vx[i], n, &lwork, t_sol.info);
+    else
+      st = g_sol.z_buf(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, (cuDoubleComplex*)X, m,
+                       dS + soff[i], (cuDoubleComplex*)Ux[i], m, (cuDoubleComplex*)Vx[i], n,
+                       &lwork, t_sol.info);
+    if (st != CUSOLVER_STATUS_SUCCESS) fail = true;
+    lmax = std::max(lmax, lwork);
+  }
+  if (!fail) fail = dalloc(&work, (size_t)lmax * f, E.stream) != cudaSuccess;
+  for (int i = 0; i < ns && !fail; i++) {
+    const int m = (int)Cc[i], n = (int)Rr[i];
+    if (std::min(m, n) == 0) continue;
     double* X = dM + moff[i] * f;
     // gesvdj overwrites its input: the sector matrices are not needed afterwards
     if (f == 1)
-      st = g_sol.d_buf(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, X, m, dS, Ux[i], m, Vx[i], n,
-                       &lwork, t_sol.info);
+      st = g_sol.d_svd(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, X, m, dS + soff[i], Ux[i], m,
+                       Vx[i], n, work, lmax, dinfo + i, t_sol.info);
     else
-      st = g_sol.z_buf(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, (cuDoubleComplex*)X, m, dS,
-                       (cuDoubleComplex*)Ux[i], m, (cuDoubleComplex*)Vx[i], n, &lwork, t_sol.info);
-    if (st == CUSOLVER_STATUS_SUCCESS) cudaMalloc(&work, sizeof(double) * (size_t)std::max(1, lwork) * f);
-    if (st == CUSOLVER_STATUS_SUCCESS) {
-      if (f == 1)
-        st = g_sol.d_svd(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, X, m, dS, Ux[i], m, Vx[i], n,
-                         work, lwork, dinfo, t_sol.info);
-      else
-        st = g_sol.z_svd(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, (cuDoubleComplex*)X, m, dS,
-                         (cuDoubleComplex*)Ux[i], m, (cuDoubleComplex*)Vx[i], n,
-                         (cuDoubleComplex*)work, lwork, dinfo, t_sol.info);
-    }
-    int hinfo = 0;
-    if (st == CUSOLVER_STATUS_SUCCESS) {
-      cudaMemcpyAsync(S[i].data(), dS, sizeof(double) * mn, cudaMemcpyDeviceToHost, E.stream);
-      cudaMemcpyAsync(&hinfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost, E.stream);
-      cudaStreamSynchronize(E.stream);
-    }
-    cudaFree(dS);
-    cudaFree(work);
-    if (st != CUSOLVER_STATUS_SUCCESS || hinfo != 0) {
-      err = "svd: cuSOLVER gesvdj failed (status " + std::to_string((int)st) + ", info " +
-            std::to_string(hinfo) + ")";
+      st = g_sol.z_svd(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, (cuDoubleComplex*)X, m,
+                       dS + soff[i], (cuDoubleComplex*)Ux[i], m, (cuDoubleComplex*)Vx[i], n,
+                       (cuDoubleComplex*)work, lmax, dinfo + i, t_sol.info);
+    if (st != CUSOLVER_STATUS_SUCCESS) fail = true;
+  }
+  std::vector<double> hS((size_t)std::max<int64_t>(1, soff[ns]));
+  std::vector<int> hinfo((size_t)std::max(1, ns), 0);
+  if (!fail) {
+    cudaMemcpyAsync(hS.data(), dS, sizeof(double) * hS.size(), cudaMemcpyDeviceToHost, E.stream);
+    cudaMemcpyAsync(hinfo.data(), dinfo, sizeof(int) * hinfo.size(), cudaMemcpyDeviceToHost,
+                    E.stream);
+    if (cudaStreamSynchronize(E.stream) != cudaSuccess) fail = true;
+  }
+  for (int i = 0; i < ns && !fail; i++) {
+    if (hinfo[i] != 0) {
+      err = "svd: cuSOLVER gesvdj failed (info " + std::to_string(hinfo[i]) + ")";
       fail = true;
+      break;
     }
-    for (int q = 1; q < mn && !fail; q++)
+    for (size_t q = 0; q < S[i].size(); q++) S[i][q] = hS[soff[i] + q];
+    for (size_t q = 1; q < S[i].size() && !fail; q++)
       if (S[i][q] > S[i][q - 1]) {
         err = "svd: singular values not in descending order";
         fail = true;
       }
   }
-  cudaFree(dinfo);
-  cudaFree(dM);
+  if (fail && err.empty())
+    err = "svd: cuSOLVER gesvdj failed (status " + std::to_string((int)st) + ")";
+  dfree(dS, E.stream);
+  dfree(work, E.stream);
+  dfree(dinfo, E.stream);
+  dfree(dM, E.stream);
   auto free_all = [&]() {
-    for (auto p : Ux) cudaFree(p);
-    for (auto p : Vx) cudaFree(p);
+    for (auto p : Ux) dfree(p, E.stream);
+    for (auto p : Vx) dfree(p, E.stream);
   };
   if (fail) {
     free_all();

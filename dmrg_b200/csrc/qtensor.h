@@ -23,6 +23,7 @@ struct QTensor {
   std::vector<int64_t> off;  // element offset of every block (+ total at the end)
   double* d = nullptr;       // device values, f doubles per element
   int f = 1;                 // 1 real, 2 complex (interleaved)
+  cudaStream_t st = nullptr; // stream the values were allocated on (freed there)
   QTensor() = default;
   QTensor(const QTensor&) = delete;
   QTensor& operator=(const QTensor&) = delete;
