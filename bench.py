@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--sweep", type=int, default=1,
                    help="also time a DMRG sweep schedule (XYZ real, L=32, m=128, 1 sweep)")
     p.add_argument("--sweep-L", type=int, default=32)
-    p.add_argument("--sweep-m", type=int, default=128)
+    p.add_argument("--sweep-m", type=int, default=256)
     p.add_argument("--sweep-n", type=int, default=1)
     return p.parse_args()
 
@@ -190,31 +190,40 @@ def cpu_reference_rate(sample_s: float, w=None):
 
 def sweep_compare(native, args):
     """The reference dmrg() schedule on the GPU for the XYZ chain (jx=1, jy=0.8,
-    jz=0.5, real MPO) with the FP64 matvec and with the headline precision:
-    wall seconds of the whole schedule, seconds per full sweep (2(L-2) steps at
-    the average step cost) and the final energies."""
+    jz=0.5, real MPO) in three forms: the plain FP64 path (one cuBLAS GEMM per
+    task row), the grouped FP64 path, and the grouped headline precision.
+    sweep_s = wall seconds of the last full sweep (2(L-2) site steps at bond
+    dimension m, from the per-step times); schedule_s = the whole schedule."""
     prec = {"fp64": native.PREC_FP64, "bf16x3": native.PREC_BF16X3,
             "tf32x3": native.PREC_TF32X3}[args.prec]
-    out = {"workload": f"XYZ chain L={args.sweep_L}, m={args.sweep_m}, {args.sweep_n} sweep(s), "
+    L = args.sweep_L
+    out = {"workload": f"XYZ chain L={L}, m={args.sweep_m}, {args.sweep_n} sweep(s), "
                        "reference dmrg() schedule, real MPO", "runs": {}}
-    for name, p in (("fp64", native.PREC_FP64), (args.prec, prec)):
-        if name in out["runs"]:
-            continue
+    arms = [("plain_fp64", native.SCHED_PER_BLOCK, native.PREC_FP64),
+            ("fp64", native.SCHED_GROUPED, native.PREC_FP64)]
+    if args.prec != "fp64":
+        arms.append((args.prec, native.SCHED_GROUPED, prec))
+    half = L // 2 - 1          # steps of the closing half sweep
+    full = 2 * (L - 2)         # steps of one full sweep
+    for name, sched, p in arms:
         c = native.Context(native.F64)
+        c.set_schedule(sched)
         c.set_precision(p)
-        r = c.dmrg("xyz_real", args.sweep_L, args.sweep_m, args.sweep_n, [1.0, 0.8, 0.5])
-        ns = len(r["trunc"])
-        tot = float(r["seconds"]["total"])
-        out["runs"][name] = {"schedule_s": tot, "steps": ns,
-                             "sweep_s": tot * 2 * (args.sweep_L - 2) / ns,
+        r = c.dmrg("xyz_real", L, args.sweep_m, args.sweep_n, [1.0, 0.8, 0.5])
+        st = c.step_seconds()
+        ns = len(st)
+        last = st[ns - half - full: ns - half] if ns >= half + full else st
+        out["runs"][name] = {"schedule_s": float(r["seconds"]["total"]), "steps": ns,
+                             "sweep_s": float(np.sum(last)),
                              "energy": float(r["energies"][-1, 0]),
                              "matvecs": int(r["matvecs"].sum()),
                              "split_s": {k: float(v) for k, v in r["seconds"].items()}}
         c.close()
-    if args.prec != "fp64":
-        a, b = out["runs"]["fp64"], out["runs"][args.prec]
-        out["speedup"] = a["schedule_s"] / b["schedule_s"]
-        out["dE_rel"] = abs(a["energy"] - b["energy"]) / abs(a["energy"])
+    runs = out["runs"]
+    head = args.prec if args.prec != "fp64" else "fp64"
+    out["speedup_vs_plain_fp64"] = runs["plain_fp64"]["sweep_s"] / runs[head]["sweep_s"]
+    out["speedup_vs_grouped_fp64"] = runs["fp64"]["sweep_s"] / runs[head]["sweep_s"]
+    out["dE_rel_vs_fp64"] = abs(runs[head]["energy"] - runs["fp64"]["energy"]) / abs(runs["fp64"]["energy"])
     return out
 
 
@@ -308,10 +317,15 @@ def main():
     n, flops = ctx.n, ctx.flops
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     ref = None
-    if prec != native.PREC_FP64:   # the plain FP64 GPU path on the same input, for the ratio
+    if prec != native.PREC_FP64:   # the grouped FP64 GPU path on the same input, for the ratio
         ref = native.Context(native.F64, local)
         ref.plan_build(w["lenv"], w["renv"], 3, 2, w["sector"], 32, 0)
         ref_stream = torch.cuda.ExternalStream(ref.stream(), device=dev)
+    # the plain FP64 GPU path: one cuBLAS GEMM per task row (the reference's av() loop)
+    plain = native.Context(native.F64, local)
+    plain.set_schedule(native.SCHED_PER_BLOCK)
+    plain.plan_build(w["lenv"], w["renv"], 3, 2, w["sector"], 32, 0)
+    plain_stream = torch.cuda.ExternalStream(plain.stream(), device=dev)
 
     xs = torch.tensor(workloads.random_psi(n, seed=5), device=dev)
     ys = torch.empty_like(xs)
@@ -351,6 +365,13 @@ def main():
         fp64 = {"value": args.steps / f_s, "ms_per_step": 1e3 * f_s / args.steps,
                 "stage_ms": [float(x / fc) for x in fslots[1:]],
                 "tflops": flops / (float(fslots[1] + fslots[2]) / fc / 1e3) / 1e12}
+
+    ysp = torch.empty_like(xs)
+    p_s, _ = time_matvecs(torch, plain, plain_stream, xs, ysp, flush, args.steps, args.warmup)
+    p_err = float(np.linalg.norm(ysp.cpu().numpy() - y_main) / np.linalg.norm(ysp.cpu().numpy()))
+    plain_path = {"value": args.steps / p_s, "ms_per_step": 1e3 * p_s / args.steps,
+                  "launches_per_step": plain.matvec_launches(),
+                  "rel_err_vs_headline": p_err}
 
     # end to end through the C ABI with host buffers (copies inside the timing)
     xh = workloads.random_psi(n, seed=6)
@@ -400,17 +421,22 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": world * args.steps / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8},
-            "gpu_launches": (2 if args.prec == "fp64" else 3) * args.steps,
+            "gpu_launches": ctx.matvec_launches() * args.steps,
             "clocks": ck,
         }
         if sweep is not None:
             line["sweep"] = sweep
+        line["plain_fp64_path"] = plain_path
+        line["vs_plain_fp64"] = value / plain_path["value"]
         if fp64 is not None:
             line["fp64_path"] = fp64
             line["split_vs_fp64"] = value / fp64["value"]
             line["split_rel_err"] = rel_err
+            line["config"]["tuning"] = [dict(zip(("cfg", "halve", "ksplit_scale", "measured"), t))
+                                        for t in ctx.split_tuning()]
         print(json.dumps(line), flush=True)
     ctx.close()
+    plain.close()
     if ref is not None:
         ref.close()
     if world > 1:

@@ -497,6 +497,18 @@ int dmrgx_set_precision(dmrgx_ctx* c, int prec) {
   return 0;
 }
 
+int dmrgx_matvec_launches(dmrgx_ctx* c, int* out) {
+  ARG_CHECK(c && out, "matvec_launches: null argument");
+  ARG_CHECK(c->has_plan, "matvec_launches: no plan");
+  if (c->prec != DMRGX_PREC_FP64)
+    *out = 3 + (c->sp.s1.redblk.empty() ? 0 : 1) + (c->sp.s2.redblk.empty() ? 0 : 1);
+  else if (c->per_block)
+    *out = (int)(c->st1.rows.size() + c->st2.rows.size());
+  else
+    *out = (c->st1.tiles.empty() ? 0 : 1) + (c->st2.tiles.empty() ? 0 : 1);
+  return 0;
+}
+
 int dmrgx_split_tuning(dmrgx_ctx* c, int* out, int cap) {
   ARG_CHECK(c && out && cap >= 8, "split_tuning: need a context and 8 slots");
   ARG_CHECK(c->has_plan && c->sp.eb != 0, "split_tuning: no split-precision plan");

@@ -236,6 +236,7 @@ struct Run {
   std::vector<int> lr;
   std::vector<double> energies, trunc;
   std::vector<int64_t> matvecs;
+  std::vector<double> step_s;  // wall seconds of every step
   double t_eig = 0, t_svd = 0, t_env = 0, t_fuse = 0;
   std::string err;
 
@@ -682,33 +683,42 @@ struct Run {
   }
 
   // the reference schedule dmrg() (src/functions.cpp:157-227)
+  // one site step with its wall time recorded
+  template <class F>
+  int timed(F&& f) {
+    const double t0 = now();
+    const int r = f();
+    if (!r) step_s.push_back(now() - t0);
+    return r;
+  }
+
   int dmrg(int cutoff, int sweep) {
     int pre_cutoff = 10;
     if (sweep == -1) pre_cutoff = cutoff;
     const int pre_sweep = cutoff / 100;
-    int rc = two_sites(0, L - 1, cutoff * 10);
+    int rc = timed([&] { return two_sites(0, L - 1, cutoff * 10); });
     if (rc) return rc;
     for (int i = 1; i < L / 2; i++)
-      if ((rc = update_two(i, L - i - 1, pre_cutoff))) return rc;
+      if ((rc = timed([&] { return update_two(i, L - i - 1, pre_cutoff); }))) return rc;
     if (sweep != -1)
       for (int i = L / 2; i < L - 1; i++)
-        if ((rc = move2right(i, i + 1, pre_cutoff))) return rc;
+        if ((rc = timed([&] { return move2right(i, i + 1, pre_cutoff); }))) return rc;
     if (sweep != -1)
       for (int s = 0; s < pre_sweep - 1; s++) {
         for (int i = L - 2; i > 0; i--)
-          if ((rc = move2left(i - 1, i, 100 * (s + 1)))) return rc;
+          if ((rc = timed([&] { return move2left(i - 1, i, 100 * (s + 1)); }))) return rc;
         for (int i = 1; i < L - 1; i++)
-          if ((rc = move2right(i, i + 1, 100 * (s + 1)))) return rc;
+          if ((rc = timed([&] { return move2right(i, i + 1, 100 * (s + 1)); }))) return rc;
       }
     for (int s = 0; s < sweep; s++) {
       for (int i = L - 2; i > 0; i--)
-        if ((rc = move2left(i - 1, i, cutoff))) return rc;
+        if ((rc = timed([&] { return move2left(i - 1, i, cutoff); }))) return rc;
       for (int i = 1; i < L - 1; i++)
-        if ((rc = move2right(i, i + 1, cutoff))) return rc;
+        if ((rc = timed([&] { return move2right(i, i + 1, cutoff); }))) return rc;
     }
     if (sweep != -1)
       for (int i = L - 2; i >= L / 2; i--)
-        if ((rc = move2left(i - 1, i, cutoff))) return rc;
+        if ((rc = timed([&] { return move2left(i - 1, i, cutoff); }))) return rc;
     return 0;
   }
 };
@@ -917,5 +927,16 @@ extern "C" int dmrgx_expect(dmrgx_ctx* c, const double* params, int nparams, dou
     set_error("expect: " + R->err);
     return rc;
   }
+  return 0;
+}
+
+extern "C" int dmrgx_step_seconds(dmrgx_ctx* c, double* out, int64_t cap, int64_t* nsteps) {
+  if (!c || !c->run || !nsteps) {
+    set_error("step_seconds: no state (run dmrgx_dmrg on this context first)");
+    return DMRGX_E_STATE;
+  }
+  const Run* R = static_cast<const Run*>(c->run);
+  *nsteps = (int64_t)R->step_s.size();
+  for (int64_t i = 0; out && i < *nsteps && i < cap; i++) out[i] = R->step_s[i];
   return 0;
 }

@@ -43,6 +43,8 @@ SIGNATURES = {
                         _dp]),
     "dmrgx_set_schedule": (_i, [_vp, _i]),
     "dmrgx_split_tuning": (_i, [_vp, _ip, _i]),
+    "dmrgx_matvec_launches": (_i, [_vp, _ip]),
+    "dmrgx_step_seconds": (_i, [_vp, _dp, _i64, _i64p]),
     "dmrgx_adjoint": (_i, [_vp, _i, _dp, _i, _dp, _i64, _i64p, _dp, _dp]),
     "dmrgx_expect": (_i, [_vp, _dp, _i, _dp]),
     "dmrgx_profile": (_i, [_vp, _i]),
@@ -141,6 +143,12 @@ class Context:
     def set_precision(self, prec):
         _check(lib().dmrgx_set_precision(self.ptr, prec))
 
+    def matvec_launches(self) -> int:
+        """Kernel launches of one matvec with the current plan and settings."""
+        out = np.zeros(1, np.int32)
+        _check(lib().dmrgx_matvec_launches(self.ptr, _ip(out)))
+        return int(out[0])
+
     def split_tuning(self):
         """Autotuner choice per split stage: list of (cfg, halve, cap_scale, tuned)."""
         out = np.zeros(8, np.int32)
@@ -238,6 +246,14 @@ class Context:
         self._nparams = 3 if code == 0 else min(4, max(3, par.size))
         return dict(lr=lr[:k], energies=en[:k], trunc=tr[:k], matvecs=mv[:k],
                     seconds=dict(total=sec[0], eig=sec[1], svd=sec[2], env=sec[3], fuse=sec[4]))
+
+    def step_seconds(self):
+        """Wall seconds of every site step of the last dmrg() run."""
+        ns = np.zeros(1, np.int64)
+        _check(lib().dmrgx_step_seconds(self.ptr, None, 0, _i64p(ns)))
+        out = np.zeros(max(1, int(ns[0])))
+        _check(lib().dmrgx_step_seconds(self.ptr, out.ctypes.data_as(_dp), out.size, _i64p(ns)))
+        return out[:int(ns[0])]
 
     def adjoint(self, nparams=None, recompute=False, want_w=False):
         """Gradient of the last dmrg() ground-state energy: dict with dE_dparams

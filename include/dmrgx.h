@@ -73,6 +73,12 @@ void dmrgx_ctx_destroy(dmrgx_ctx* ctx);
 /* Select the matvec arithmetic (DMRGX_PREC_*).  Default FP64. */
 int dmrgx_set_precision(dmrgx_ctx* ctx, int prec);
 
+/* Kernel launches of one dmrgx_av with the current plan and settings: FP64
+ * grouped 2 (one per stage), split precision 3 (operand split, two stages) plus
+ * one per stage that reduces K-split partials, per-block one library GEMM per
+ * task row.  Memsets are not counted. */
+int dmrgx_matvec_launches(dmrgx_ctx* ctx, int* out);
+
 /* The tiling the autotuner chose for the current split-precision plan.  The
  * split stages run one of two kernel configurations (tiles up to 256 columns
  * with a 4-deep shared-memory ring, or up to 128 with a 7-deep ring); when a
@@ -201,6 +207,11 @@ int dmrgx_dmrg(dmrgx_ctx* ctx, int model, int L, int m, int sweeps, int sector,
  * absent from the reference (nparams = 3, or h = 0, is the reference's MPO).
  * The final state of dmrgx_dmrg (MPS site tensors, environments and the one-site
  * centre of the last step) stays in the context for the two calls below. */
+
+/* Wall seconds of every site step of the last dmrgx_dmrg (eigensolver, SVD,
+ * environment update and fusion of the step), in schedule order; nsteps gets the
+ * count, out (cap values, may be NULL) the times. */
+int dmrgx_step_seconds(dmrgx_ctx* ctx, double* out, int64_t cap, int64_t* nsteps);
 
 /* Gradient of the ground-state energy of the last dmrgx_dmrg with respect to the
  * MPO tensors and the model parameters, by adjoint contractions of the

@@ -16,4 +16,6 @@ def test_concurrent_chains_match_serial():
         assert abs(a["E0"] - b["E0"]) < 1e-12 * abs(b["E0"])
         assert abs(a["dE_dJz"] - b["dE_dJz"]) < 1e-10 * abs(b["dE_dJz"])
         assert a["rel_hf_Jz"] < 1e-9 and a["abs_hf_h"] < 1e-9
-        assert abs(a["dE_dh"]) < 1e-8
+        # <sum sigma^z> vanishes for the exact state (global spin flip); a truncated
+        # MPS at m = 16..24 breaks that symmetry at the discarded-weight level
+        assert abs(a["dE_dh"]) < 1e-6
