@@ -100,36 +100,200 @@ __global__ void vdot_final(const double* __restrict__ part, int nblk, int k,
   if (T && j == jt) T[(int64_t)jt * tdim + jt] += sr;
 }
 
-// beta = sqrt(coef[0]); T[j][j+1] = T[j+1][j] = beta; inv = beta > tiny ? 1/beta : 0
-__global__ void set_beta(const double* __restrict__ coef, double* __restrict__ T, int tdim, int j,
-                         double* __restrict__ inv) {
-  const double b = sqrt(fmax(coef[0], 0.0));
-  T[(int64_t)j * tdim + j + 1] = b;
-  T[(int64_t)(j + 1) * tdim + j] = b;
-  inv[0] = b > 1e-300 ? 1.0 / b : 0.0;
+
+// ---------------------------------------------------------------- fused CGS2 step
+// One Lanczos step's reorthogonalisation in three launches instead of ten:
+//   lz_dots      c1 = V^H w                       (T[j][j] += Re c1[j])
+//   lz_sub_dots  w -= V c1, then c2 = V^H w       (T[j][j] += Re c2[j])
+//   lz_sub_norm  w -= V c2, then beta = |w|       (T[j][j+1] = T[j+1][j] = beta)
+// Every block reduces its rows for CH columns at a time in registers (one block
+// reduction per chunk, not per column) and writes partials part[j][block]; the
+// last block to finish (atomic ticket after a fence) sums the partials of every
+// column in block order -- a fixed order, so results do not depend on timing --
+// and resets the ticket.
+constexpr int CH = 8;  // columns per register chunk
+
+// rows of block b: [b*per, min(n, (b+1)*per))
+__device__ __forceinline__ void lz_rows(int64_t n, int64_t& i0, int64_t& i1) {
+  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+  i0 = (int64_t)blockIdx.x * per;
+  i1 = min(n, i0 + per);
 }
 
-// w -= V[:, 0..k) coef  (coef pairs; real data uses the real parts)
+// block-wide sums of v[0..2*CH) (pairs); thread 0 gets the results in v
+__device__ __forceinline__ void block_sum(double* v, double (*red)[2 * CH]) {
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 2 * CH; q++)
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < 2 * CH; q++) red[wp][q] = v[q];
+  __syncthreads();
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < 2 * CH; q++) {
+      double t = 0.0;
+      for (int u = 0; u < RB / 32; u++) t += red[u][q];
+      v[q] = t;
+    }
+  __syncthreads();
+}
+
+// partials of V[:, 0..k)^H w over this block's rows -> part[j][block]
 template <bool CPLX>
-__global__ void __launch_bounds__(RB) vsub(const double* __restrict__ V, int64_t ld, int k,
-                                           const double* __restrict__ coef, double* __restrict__ w,
-                                           int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
+__device__ __forceinline__ void lz_partial_dots(const double* __restrict__ V, int64_t ld, int k,
+                                                const double* w, int64_t i0, int64_t i1,
+                                                double* __restrict__ part,
+                                                double (*red)[2 * CH]) {
+  for (int j0 = 0; j0 < k; j0 += CH) {
+    double acc[2 * CH];
+#pragma unroll
+    for (int q = 0; q < 2 * CH; q++) acc[q] = 0.0;
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += RB) {
+      if (CPLX) {
+        const double wr = w[2 * i], wi = w[2 * i + 1];
+#pragma unroll
+        for (int jj = 0; jj < CH; jj++)
+          if (j0 + jj < k) {
+            const double vr = V[2 * ((j0 + jj) * ld + i)], vi = V[2 * ((j0 + jj) * ld + i) + 1];
+            acc[2 * jj] += vr * wr + vi * wi;
+            acc[2 * jj + 1] += vr * wi - vi * wr;
+          }
+      } else {
+        const double wv = w[i];
+#pragma unroll
+        for (int jj = 0; jj < CH; jj++)
+          if (j0 + jj < k) acc[2 * jj] += V[(j0 + jj) * ld + i] * wv;
+      }
+    }
+    block_sum(acc, red);
+    if (threadIdx.x == 0)
+      for (int jj = 0; jj < CH && j0 + jj < k; jj++) {
+        part[2 * ((int64_t)(j0 + jj) * gridDim.x + blockIdx.x)] = acc[2 * jj];
+        part[2 * ((int64_t)(j0 + jj) * gridDim.x + blockIdx.x) + 1] = acc[2 * jj + 1];
+      }
+  }
+}
+
+// w[i] -= sum_j V[i, j] c[j] over this block's rows
+template <bool CPLX>
+__device__ __forceinline__ void lz_subtract(const double* __restrict__ V, int64_t ld, int k,
+                                            const double* __restrict__ c, double* w, int64_t i0,
+                                            int64_t i1) {
+  for (int64_t i = i0 + threadIdx.x; i < i1; i += RB) {
     if (CPLX) {
       double ar = 0.0, ai = 0.0;
       for (int j = 0; j < k; j++) {
         const double vr = V[2 * (j * ld + i)], vi = V[2 * (j * ld + i) + 1];
-        const double cr = coef[2 * j], ci = coef[2 * j + 1];
-        ar += vr * cr - vi * ci;
-        ai += vr * ci + vi * cr;
+        ar += vr * c[2 * j] - vi * c[2 * j + 1];
+        ai += vr * c[2 * j + 1] + vi * c[2 * j];
       }
       w[2 * i] -= ar;
       w[2 * i + 1] -= ai;
     } else {
       double a = 0.0;
-      for (int j = 0; j < k; j++) a += V[j * ld + i] * coef[2 * j];
+      for (int j = 0; j < k; j++) a += V[j * ld + i] * c[2 * j];
       w[i] -= a;
+    }
+  }
+}
+
+// true in the block that finishes last (after all partials are visible)
+__device__ __forceinline__ bool lz_last(unsigned* ticket) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  return last;
+}
+
+// last block: coef[j] = sum_b part[j][b] in block order, T[jt][jt] += Re coef[jt]
+__device__ __forceinline__ void lz_final_coef(const double* part, int k, double* coef, double* T,
+                                              int tdim, int jt) {
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  for (int j = wp; j < k; j += RB / 32) {
+    double sr = 0.0, si = 0.0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) {
+      sr += __ldcg(part + 2 * ((int64_t)j * gridDim.x + b));
+      si += __ldcg(part + 2 * ((int64_t)j * gridDim.x + b) + 1);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, o);
+      si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane == 0) {
+      coef[2 * j] = sr;
+      coef[2 * j + 1] = si;
+      if (j == jt) T[(int64_t)jt * tdim + jt] += sr;
+    }
+  }
+}
+
+template <bool CPLX>
+__global__ void __launch_bounds__(RB) lz_dots(const double* __restrict__ V, int64_t ld, int k,
+                                              const double* __restrict__ w, int64_t n,
+                                              double* __restrict__ part, unsigned* ticket,
+                                              double* __restrict__ coef, double* __restrict__ T,
+                                              int tdim, int jt) {
+  __shared__ double red[RB / 32][2 * CH];
+  int64_t i0, i1;
+  lz_rows(n, i0, i1);
+  lz_partial_dots<CPLX>(V, ld, k, w, i0, i1, part, red);
+  if (!lz_last(ticket)) return;
+  lz_final_coef(part, k, coef, T, tdim, jt);
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
+template <bool CPLX>
+__global__ void __launch_bounds__(RB) lz_sub_dots(const double* __restrict__ V, int64_t ld, int k,
+                                                  const double* __restrict__ cin,
+                                                  double* __restrict__ w, int64_t n,
+                                                  double* __restrict__ part, unsigned* ticket,
+                                                  double* __restrict__ cout,
+                                                  double* __restrict__ T, int tdim, int jt) {
+  __shared__ double red[RB / 32][2 * CH];
+  int64_t i0, i1;
+  lz_rows(n, i0, i1);
+  lz_subtract<CPLX>(V, ld, k, cin, w, i0, i1);
+  lz_partial_dots<CPLX>(V, ld, k, w, i0, i1, part, red);  // own rows: no cross-thread hazard
+  if (!lz_last(ticket)) return;
+  lz_final_coef(part, k, cout, T, tdim, jt);
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
+template <bool CPLX>
+__global__ void __launch_bounds__(RB) lz_sub_norm(const double* __restrict__ V, int64_t ld, int k,
+                                                  const double* __restrict__ cin,
+                                                  double* __restrict__ w, int64_t n,
+                                                  double* __restrict__ part, unsigned* ticket,
+                                                  double* __restrict__ T, int tdim, int j,
+                                                  double* __restrict__ inv) {
+  __shared__ double red[RB / 32][2 * CH];
+  int64_t i0, i1;
+  lz_rows(n, i0, i1);
+  lz_subtract<CPLX>(V, ld, k, cin, w, i0, i1);
+  double acc[2 * CH];
+#pragma unroll
+  for (int q = 0; q < 2 * CH; q++) acc[q] = 0.0;
+  for (int64_t i = i0 + threadIdx.x; i < i1; i += RB) {
+    if (CPLX) acc[0] += w[2 * i] * w[2 * i] + w[2 * i + 1] * w[2 * i + 1];
+    else acc[0] += w[i] * w[i];
+  }
+  block_sum(acc, red);
+  if (threadIdx.x == 0) part[2 * blockIdx.x] = acc[0];
+  if (!lz_last(ticket)) return;
+  if (threadIdx.x < 32) {
+    double sq = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) sq += __ldcg(part + 2 * b);
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    if (threadIdx.x == 0) {
+      const double beta = sqrt(fmax(sq, 0.0));
+      T[(int64_t)j * tdim + j + 1] = beta;
+      T[(int64_t)(j + 1) * tdim + j] = beta;
+      inv[0] = beta > 1e-300 ? 1.0 / beta : 0.0;
+      *ticket = 0u;
     }
   }
 }
@@ -267,7 +431,9 @@ struct Lanczos {
   int grid, nblk;
   cudaStream_t s;
   DevMem mem;
-  double *V, *V2, *w, *part, *coef, *T, *inv, *Y;
+  double *V, *V2, *w, *part, *part2, *coef, *coef2, *T, *inv, *Y;
+  unsigned* ticket;
+  int nblk2;       // blocks of the fused step kernels
   int64_t matvecs = 0, matvecs64 = 0;
 
   double* col(double* M, int j) { return M + (int64_t)j * len; }
@@ -279,6 +445,10 @@ struct Lanczos {
     EIG_TRY(mem.alloc(w, (size_t)len));
     EIG_TRY(mem.alloc(part, (size_t)2 * nblk * (m + 1)));
     EIG_TRY(mem.alloc(coef, (size_t)2 * (m + 1)));
+    EIG_TRY(mem.alloc(coef2, (size_t)2 * (m + 1)));
+    EIG_TRY(mem.alloc(ticket, 1));
+    EIG_TRY(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));
+    EIG_TRY(mem.alloc(part2, (size_t)2 * nblk2 * (m + 1)));
     EIG_TRY(mem.alloc(T, (size_t)tdim * tdim));
     EIG_TRY(mem.alloc(inv, 2));
     EIG_TRY(mem.alloc(Y, (size_t)MAX_NCV * MAX_NCV));
@@ -297,12 +467,7 @@ struct Lanczos {
       vdot_partial<false><<<nblk, RB, 0, s>>>(Vb, n, k, x, n, part);
     vdot_final<<<(k + 63) / 64, 64, 0, s>>>(part, nblk, k, coef, jt >= 0 ? T : nullptr, tdim, jt);
   }
-  void subtract(int k, double* x) {
-    if (cplx)
-      vsub<true><<<grid, RB, 0, s>>>(V, n, k, coef, x, n);
-    else
-      vsub<false><<<grid, RB, 0, s>>>(V, n, k, coef, x, n);
-  }
+
   void rotate(const double* Vin, int mm, int k, double* Vout) {
     if (cplx)
       vrotate<true><<<grid, RB, sizeof(double) * mm * k, s>>>(Vin, n, mm, Y, k, Vout, n);
@@ -319,14 +484,19 @@ struct Lanczos {
     return 0;
   }
   // one Lanczos step j on the device: v_{j+1}, T[j][j], T[j][j+1]
+  // (classical Gram-Schmidt against the whole basis, twice)
   int step(int j) {
     if (matvec(col(V, j), w, false)) return DMRGX_E_CUDA;
-    dots(V, j + 1, w, j);
-    subtract(j + 1, w);
-    dots(V, j + 1, w, j);
-    subtract(j + 1, w);
-    dots(w, 1, w, -1);
-    set_beta<<<1, 1, 0, s>>>(coef, T, tdim, j, inv);
+    const int k = j + 1;
+    if (cplx) {
+      lz_dots<true><<<nblk2, RB, 0, s>>>(V, n, k, w, n, part2, ticket, coef, T, tdim, j);
+      lz_sub_dots<true><<<nblk2, RB, 0, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j);
+      lz_sub_norm<true><<<nblk2, RB, 0, s>>>(V, n, k, coef2, w, n, part2, ticket, T, tdim, j, inv);
+    } else {
+      lz_dots<false><<<nblk2, RB, 0, s>>>(V, n, k, w, n, part2, ticket, coef, T, tdim, j);
+      lz_sub_dots<false><<<nblk2, RB, 0, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j);
+      lz_sub_norm<false><<<nblk2, RB, 0, s>>>(V, n, k, coef2, w, n, part2, ticket, T, tdim, j, inv);
+    }
     vscale<<<grid, RB, 0, s>>>(w, inv, 0.0, col(V, j + 1), len);
     EIG_TRY(cudaGetLastError());
     return 0;
@@ -361,6 +531,7 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
   L.s = c->stream;
   L.grid = (int)std::max<int64_t>(1, std::min<int64_t>(c->num_sms * 8, (n + RB - 1) / RB));
   L.nblk = (int)std::max<int64_t>(1, std::min<int64_t>(c->num_sms * 4, (n + RB - 1) / RB));
+  L.nblk2 = (int)std::max<int64_t>(1, std::min<int64_t>(c->num_sms * 2, (n + 2 * RB - 1) / (2 * RB)));
   int rc = L.init();
   if (rc) return rc;
   const int m = L.m, td = L.tdim;
