@@ -42,9 +42,10 @@ def parse():
     p.add_argument("--impl", default="dmrgx", choices=["dmrgx", "reference"])
     p.add_argument("--cpu-sample-s", type=float, default=12.0)
     p.add_argument("--sweep", type=int, default=1,
-                   help="also time a DMRG sweep schedule (XYZ real, L=32, m=128, 1 sweep)")
+                   help="also time the DMRG schedule (XYZ real chain) in three forms: plain "
+                        "per-block FP64, grouped FP64, grouped headline precision")
     p.add_argument("--sweep-L", type=int, default=32)
-    p.add_argument("--sweep-m", type=int, default=256)
+    p.add_argument("--sweep-m", type=int, default=512)
     p.add_argument("--sweep-n", type=int, default=1)
     return p.parse_args()
 

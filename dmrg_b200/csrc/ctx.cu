@@ -478,8 +478,6 @@ int dmrgx_set_precision(dmrgx_ctx* c, int prec) {
   ARG_CHECK(c, "null context");
   ARG_CHECK(prec == DMRGX_PREC_FP64 || prec == DMRGX_PREC_BF16X3 || prec == DMRGX_PREC_TF32X3,
             "set_precision: unknown precision");
-  ARG_CHECK(prec == DMRGX_PREC_FP64 || c->dtype == DMRGX_F64,
-            "set_precision: split precision is available for F64 contexts");
   if (prec == c->prec) return 0;
   ARG_CHECK(prec == DMRGX_PREC_FP64 || !c->per_block,
             "set_precision: the per-block schedule is FP64 only");

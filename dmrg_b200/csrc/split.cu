@@ -54,6 +54,19 @@ __global__ void __launch_bounds__(64) pad_split_kernel(const double* __restrict_
   const PadJob jb = jobs[pr.job];
   const int gc = jb.groups * jb.cols;
   const double* s = src + jb.src + (int64_t)pr.row * gc;
+  if (jb.expand) {
+    // complex row -> (re, -im, ...) and (im, re, ...)
+    uint8_t* r0 = dst + (jb.dst + (int64_t)(2 * pr.row) * 2 * jb.kq) * EB;
+    uint8_t* r1 = r0 + (int64_t)2 * jb.kq * EB;
+    for (int e = threadIdx.x; e < gc / 2; e += blockDim.x) {
+      const double re = __ldg(s + 2 * e), im = __ldg(s + 2 * e + 1);
+      put_pair<EB>(r0, 2 * e, re);
+      put_pair<EB>(r0, 2 * e + 1, -im);
+      put_pair<EB>(r1, 2 * e, im);
+      put_pair<EB>(r1, 2 * e + 1, re);
+    }
+    return;
+  }
   uint8_t* row = dst + (jb.dst + (int64_t)pr.row * 2 * jb.kq) * EB;
   for (int e0 = 0; e0 < gc; e0 += 4 * 64) {
     double x[4];

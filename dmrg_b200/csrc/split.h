@@ -31,7 +31,15 @@ struct SOut {
   int32_t tnw;       // tile width (columns per tile, <= 256, a multiple of 16)
   int32_t grp;       // stage 1: output rows per pair-layout row (MPO channels)
   int32_t rstride;   // stage 1: elements per pair-layout row (2 * kq)
+  int32_t cplx;      // stage 1, complex data: write the B-expanded form (see below)
 };
+
+// Complex data.  A complex product C = A B^T is one real product of
+//   A as real rows (re, im, re, im, ...) and
+//   B "expanded": complex row j becomes real rows 2j = (re, -im, ...) and
+//   2j+1 = (im, re, ...),
+// giving real C rows (Re, Im, Re, Im, ...) -- the interleaved complex result.
+// Stage 1 writes the intermediate directly in the expanded form stage 2 reads.
 
 // One segment of an output block: tensor-map indices of its A block (m x kp) and
 // B block (n x kp), its k-tile count, and the row count of the B map's box.
@@ -75,7 +83,9 @@ struct PadRow {
 struct PadJob {
   int64_t src, dst;
   int32_t rows, groups, cols, colsp;
-  int32_t kq, pad_;
+  int32_t kq;
+  int32_t expand;  // complex B operand: each source row (cols doubles = cols/2 complex)
+                   // becomes the two expanded destination rows 2*row, 2*row + 1
 };
 
 // Kernel configurations: cfg 0 tiles up to 256 columns with a 4-deep ring, cfg 1

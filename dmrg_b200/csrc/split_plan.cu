@@ -390,10 +390,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
   SplitPlan& sp = c->sp;
   sp.free_device();
   sp = SplitPlan();
-  if (c->dtype != DMRGX_F64) {
-    set_error("split precision is available for F64 contexts");
-    return DMRGX_E_ARG;
-  }
+  const int f = c->f();  // complex data: real view of A, expanded B (split.h)
   const int64_t P = 16 / eb;   // padding of stage-1 output rows (16 bytes)
   const int64_t CH = 64 / eb;  // elements per half-chunk of the pair layout = per k-tile
   const Stage& f1 = c->st1;
@@ -416,7 +413,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
         return DMRGX_E_ARG;
       }
       const int M1 = is->second.first, N1 = is->second.second;
-      if (N1 <= 0 || g.k % N1 != 0 || (int64_t)(g.k / N1) * d.n != M1) {
+      if (N1 <= 0 || g.k % N1 != 0 || (int64_t)(g.k / N1) * (d.n / f) != M1) {
         set_error("split plan: stage-2 K does not factor as channels x stage-1 columns");
         return DMRGX_E_ARG;
       }
@@ -447,13 +444,14 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
     if (st_off.find(d.c_off) == st_off.end()) {
       st_off[d.c_off] = st_len;
       st_kq[d.c_off] = kq2;
-      st_len += (int64_t)(d.m / D) * 2 * kq2;
+      st_len += (int64_t)f * (d.m / D) * 2 * kq2;  // complex: two expanded rows each
     }
     so.c_off = st_off[d.c_off];
     so.m = d.m;
     so.n = d.n;
     so.ldc = (int32_t)n1p;
     so.grp = D;
+    so.cplx = f == 2 ? 1 : 0;
     so.rstride = (int32_t)(2 * kq2);
     so.seg_begin = (int32_t)sp.s1.segs.size();
     so.seg_count = d.seg_count;
@@ -472,7 +470,8 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
       ss.amap = a1_map[g.a_off];
       auto ib = psi_map.find(g.b_off);
       if (ib == psi_map.end()) {
-        sp.psi_jobs.push_back(PadJob{g.b_off, psi_len, d.n, 1, g.k, g.k, (int32_t)kq, 0});
+        sp.psi_jobs.push_back(
+            PadJob{g.b_off, psi_len, d.n / f, 1, g.k, g.k, (int32_t)kq, f == 2 ? 1 : 0});
         psi_map[g.b_off] = (int)req1.size();
         req1.push_back({1, psi_len, kq, d.n, 0});
         psi_len += (int64_t)d.n * 2 * kq;
@@ -499,6 +498,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
     so.ldc = d.n;
     so.grp = 1;
     so.rstride = 0;
+    so.cplx = 0;
     so.seg_begin = (int32_t)sp.s2.segs.size();
     so.seg_count = d.seg_count;
     so.tnw = 0;

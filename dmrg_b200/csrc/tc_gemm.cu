@@ -171,37 +171,66 @@ __device__ __forceinline__ void split_f32(float v, uint32_t& hi, uint32_t& lo) {
   }
 }
 
+// (hi, lo) pairs of EPC = 16 / EB consecutive values (16 bytes of each half)
+// at logical k of a pair-layout row; a group never crosses a chunk (k is a
+// multiple of EPC)
+template <int EB>
+__device__ __forceinline__ void put_group(uint8_t* c_pair, int64_t rbase, int64_t k,
+                                          const float* v) {
+  constexpr int CH = 64 / EB;
+  uint32_t hw[4], lw[4];
+  if (EB == 2) {
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      uint32_t h0, l0, h1, l1;
+      split_f32<2>(v[2 * p], h0, l0);
+      split_f32<2>(v[2 * p + 1], h1, l1);
+      hw[p] = h0 | (h1 << 16);
+      lw[p] = l0 | (l1 << 16);
+    }
+  } else {
+#pragma unroll
+    for (int p = 0; p < 4; p++) split_f32<4>(v[p], hw[p], lw[p]);
+  }
+  const int64_t eoff = (rbase + pair_off(k, CH)) * EB;
+  *reinterpret_cast<uint4*>(c_pair + eoff) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+  *reinterpret_cast<uint4*>(c_pair + eoff + HALF) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+}
+
 // Final store of 16 consecutive columns of one row (cols [col0, col0+16)).
-// Stage 1 (OUT_SPLIT): (hi, lo) pairs in pair layout, 16 bytes of each per
-// group of 16 / EB columns (a group never crosses a chunk: n1p and col0 are
-// multiples of it).
+// Stage 1 (OUT_SPLIT): (hi, lo) pairs in pair layout, groups of 16 / EB columns
+// (n1p and col0 are multiples of a group).  Complex data: columns are (Re, Im)
+// pairs and the row is written in the expanded form of split.h, rows 2q, 2q+1.
 template <int EB, bool OUT_SPLIT>
 __device__ __forceinline__ void store16(const SOut& o, int row, int col0, const float* v,
                                         uint8_t* c_pair, double* c64) {
   if (OUT_SPLIT) {
-    constexpr int EPC = 16 / EB, CH = 64 / EB;
-    const int64_t rbase = o.c_off + (int64_t)(row / o.grp) * o.rstride;
+    constexpr int EPC = 16 / EB;
+    const int64_t q = row / o.grp;
     const int64_t kb = (int64_t)(row % o.grp) * o.ldc;
+    if (!o.cplx) {
+      const int64_t rbase = o.c_off + q * o.rstride;
 #pragma unroll
-    for (int gq = 0; gq < 16 / EPC; gq++) {
-      if (col0 + gq * EPC >= o.ldc) break;
-      uint32_t hw[4], lw[4];
-      if (EB == 2) {
-#pragma unroll
-        for (int p = 0; p < 4; p++) {
-          uint32_t h0, l0, h1, l1;
-          split_f32<2>(v[gq * 8 + 2 * p], h0, l0);
-          split_f32<2>(v[gq * 8 + 2 * p + 1], h1, l1);
-          hw[p] = h0 | (h1 << 16);
-          lw[p] = l0 | (l1 << 16);
-        }
-      } else {
-#pragma unroll
-        for (int p = 0; p < 4; p++) split_f32<4>(v[gq * 4 + p], hw[p], lw[p]);
+      for (int gq = 0; gq < 16 / EPC; gq++) {
+        if (col0 + gq * EPC >= o.ldc) break;
+        put_group<EB>(c_pair, rbase, kb + col0 + gq * EPC, v + gq * EPC);
       }
-      const int64_t eoff = (rbase + pair_off(kb + col0 + gq * EPC, CH)) * EB;
-      *reinterpret_cast<uint4*>(c_pair + eoff) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-      *reinterpret_cast<uint4*>(c_pair + eoff + HALF) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    } else {
+      const int64_t r0 = o.c_off + 2 * q * o.rstride, r1 = r0 + o.rstride;
+      float va[16], vb[16];
+#pragma unroll
+      for (int t = 0; t < 8; t++) {
+        va[2 * t] = v[2 * t];
+        va[2 * t + 1] = -v[2 * t + 1];
+        vb[2 * t] = v[2 * t + 1];
+        vb[2 * t + 1] = v[2 * t];
+      }
+#pragma unroll
+      for (int gq = 0; gq < 16 / EPC; gq++) {
+        if (col0 + gq * EPC >= o.ldc) break;
+        put_group<EB>(c_pair, r0, kb + col0 + gq * EPC, va + gq * EPC);
+        put_group<EB>(c_pair, r1, kb + col0 + gq * EPC, vb + gq * EPC);
+      }
     }
   } else {
     const int64_t rbase = o.c_off + (int64_t)row * o.ldc + col0;
@@ -414,26 +443,39 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
                  : "memory");
 }
 
+// 4 values as (hi, lo) pairs at logical k of a pair-layout row
+template <int EB>
+__device__ __forceinline__ void put4(uint8_t* c_pair, int64_t rbase, int64_t k, float4 v) {
+  constexpr int CH = 64 / EB;
+  const int64_t e = rbase + pair_off(k, CH);
+  uint32_t h[4], l[4];
+  split_f32<EB>(v.x, h[0], l[0]);
+  split_f32<EB>(v.y, h[1], l[1]);
+  split_f32<EB>(v.z, h[2], l[2]);
+  split_f32<EB>(v.w, h[3], l[3]);
+  if (EB == 2) {
+    *reinterpret_cast<uint2*>(c_pair + e * 2) = make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
+    *reinterpret_cast<uint2*>(c_pair + e * 2 + HALF) = make_uint2(l[0] | (l[1] << 16), l[2] | (l[3] << 16));
+  } else {
+    *reinterpret_cast<uint4*>(c_pair + e * 4) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4*>(c_pair + e * 4 + HALF) = make_uint4(l[0], l[1], l[2], l[3]);
+  }
+}
+
 // Final store of 4 consecutive columns of one row (cols [col0, col0+4)).
 template <int EB, bool OUT_SPLIT>
 __device__ __forceinline__ void store4(const SOut& o, int row, int col0, float4 v,
                                        uint8_t* c_pair, double* c64) {
   if (OUT_SPLIT) {
     if (col0 >= o.ldc) return;  // ldc is a multiple of 4 elements
-    constexpr int CH = 64 / EB;
-    const int64_t e = o.c_off + (int64_t)(row / o.grp) * o.rstride +
-                      pair_off((int64_t)(row % o.grp) * o.ldc + col0, CH);
-    uint32_t h[4], l[4];
-    split_f32<EB>(v.x, h[0], l[0]);
-    split_f32<EB>(v.y, h[1], l[1]);
-    split_f32<EB>(v.z, h[2], l[2]);
-    split_f32<EB>(v.w, h[3], l[3]);
-    if (EB == 2) {
-      *reinterpret_cast<uint2*>(c_pair + e * 2) = make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
-      *reinterpret_cast<uint2*>(c_pair + e * 2 + HALF) = make_uint2(l[0] | (l[1] << 16), l[2] | (l[3] << 16));
+    const int64_t q = row / o.grp;
+    const int64_t k = (int64_t)(row % o.grp) * o.ldc + col0;
+    if (!o.cplx) {
+      put4<EB>(c_pair, o.c_off + q * o.rstride, k, v);
     } else {
-      *reinterpret_cast<uint4*>(c_pair + e * 4) = make_uint4(h[0], h[1], h[2], h[3]);
-      *reinterpret_cast<uint4*>(c_pair + e * 4 + HALF) = make_uint4(l[0], l[1], l[2], l[3]);
+      const int64_t r0 = o.c_off + 2 * q * o.rstride;
+      put4<EB>(c_pair, r0, k, make_float4(v.x, -v.y, v.z, -v.w));
+      put4<EB>(c_pair, r0 + o.rstride, k, make_float4(v.y, v.x, v.w, v.z));
     }
   } else {
     const int64_t e = o.c_off + (int64_t)row * o.ldc + col0;

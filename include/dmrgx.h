@@ -141,8 +141,8 @@ int dmrgx_plan_psi_layout(dmrgx_ctx* ctx, int* out, int64_t cap);
 
 /* out = H_eff in, exactly av() of the reference (src/core.cpp:22-31):
  * store = renv (x)_{r_num} in, out = lenv (x)_{l_num} store.
- * mem = DMRGX_MEM_HOST: in/out are host arrays (copied through the context's
- * pinned staging buffers); DMRGX_MEM_DEVICE: device arrays on this context's
+ * mem = DMRGX_MEM_HOST: in/out are host arrays (copied straight from and to
+ * them); DMRGX_MEM_DEVICE: device arrays on this context's
  * device, ordered on the context's stream.  Psi sectors no task writes are set
  * to zero (the reference leaves them untouched). */
 int dmrgx_av(dmrgx_ctx* ctx, const void* in, void* out, int mem);

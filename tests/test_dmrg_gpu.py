@@ -60,3 +60,17 @@ def test_dmrg_split_precision_energy(prec):
     r = ctx.dmrg("xyz_real", 16, 32, 2, [1.0, 0.8, 0.5])
     print(prec, r["energies"][-1, 0], r64["energies"][-1, 0], r["seconds"])
     assert abs(r["energies"][-1, 0] - r64["energies"][-1, 0]) <= 1e-9 * abs(r64["energies"][-1, 0])
+
+
+@pytest.mark.parametrize("prec", [native.PREC_BF16X3, native.PREC_TF32X3])
+@pytest.mark.parametrize("model,L,par", [("potts", 12, [1.0, 1.0, 0.0, 0.0]),
+                                         ("xyz", 14, [1.0, 0.8, 0.5])])
+def test_dmrg_split_precision_complex(model, L, par, prec):
+    """Complex models (C128) with split-precision contractions reach the FP64 energy."""
+    c64 = native.Context(native.C128)
+    r64 = c64.dmrg(model, L, 32, 2, par)
+    ctx = native.Context(native.C128)
+    ctx.set_precision(prec)
+    r = ctx.dmrg(model, L, 32, 2, par)
+    print(model, prec, r["energies"][-1, 0], r64["energies"][-1, 0])
+    assert abs(r["energies"][-1, 0] - r64["energies"][-1, 0]) <= 1e-9 * abs(r64["energies"][-1, 0])

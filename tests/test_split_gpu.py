@@ -66,3 +66,34 @@ def test_split_real_physical_steps(model):
         ctx.plan_build(st["lenv"], st["renv"], st["l_num"], st["r_num"], st["sector"],
                        st["group_n"], st["fermion"])
         assert rel(ctx.av(st["x"]), st["ax"]) < BOUND[native.PREC_TF32X3]
+
+
+@pytest.mark.parametrize("prec", [native.PREC_BF16X3, native.PREC_TF32X3])
+@pytest.mark.parametrize("model", ["xyz", "potts"])
+def test_split_complex_physical_steps(model, prec):
+    """Complex contractions as one real split GEMM with the B operand expanded."""
+    for st in load_steps(model):
+        ctx = native.Context(native.C128)
+        ctx.set_precision(prec)
+        ctx.plan_build(st["lenv"], st["renv"], st["l_num"], st["r_num"], st["sector"],
+                       st["group_n"], st["fermion"])
+        e = rel(ctx.av(st["x"]), st["ax"])
+        assert e < BOUND[prec], (model, e)
+
+
+@pytest.mark.parametrize("prec", [native.PREC_BF16X3, native.PREC_TF32X3])
+@pytest.mark.parametrize("m", [35, 256])
+def test_split_complex_against_fp64(prec, m):
+    a, b = workloads.microbench(m, seed=m), workloads.microbench(m, seed=m + 1)
+    lenv = (a["lenv"][0], a["lenv"][1] + 1j * b["lenv"][1])
+    renv = (a["renv"][0], a["renv"][1] - 0.5j * b["renv"][1])
+    ref_ctx = native.Context(native.C128)
+    ref_ctx.plan_build(lenv, renv, 3, 2, a["sector"], 32, 0)
+    ctx = native.Context(native.C128)
+    ctx.set_precision(prec)
+    ctx.plan_build(lenv, renv, 3, 2, a["sector"], 32, 0)
+    rng = np.random.default_rng(m)
+    x = rng.standard_normal(ctx.n) + 1j * rng.standard_normal(ctx.n)
+    e = rel(ctx.av(x), ref_ctx.av(x))
+    print("complex m", m, "prec", prec, "rel err", e)
+    assert e < BOUND[prec]
