@@ -218,7 +218,7 @@ def sweep_compare(native, args):
                              "sweep_s": float(np.sum(last)),
                              "energy": float(r["energies"][-1, 0]),
                              "matvecs": int(r["matvecs"].sum()),
-                             "split_s": {k: float(v) for k, v in r["seconds"].items()}}
+                             "split_s": c.run_seconds()}
         c.close()
     runs = out["runs"]
     head = args.prec if args.prec != "fp64" else "fp64"

@@ -26,9 +26,9 @@ static thread_local std::string g_err;
 void set_error(const std::string& msg) { g_err = msg; }
 
 void Stage::free_device() {
-  cudaFree(d_outs);
-  cudaFree(d_segs);
-  cudaFree(d_tiles);
+  dfree(d_outs, st);
+  dfree(d_segs, st);
+  dfree(d_tiles, st);
   d_outs = nullptr;
   d_segs = nullptr;
   d_tiles = nullptr;
@@ -213,9 +213,10 @@ std::string build_stage(const std::vector<MapRow>& rows, const std::vector<int64
 
 int upload_stage(Stage& st, cudaStream_t s) {
   st.free_device();
-  CUDA_TRY(cudaMalloc(&st.d_outs, sizeof(DOut) * std::max<size_t>(1, st.outs.size())));
-  CUDA_TRY(cudaMalloc(&st.d_segs, sizeof(DSeg) * std::max<size_t>(1, st.segs.size())));
-  CUDA_TRY(cudaMalloc(&st.d_tiles, sizeof(DTile) * std::max<size_t>(1, st.tiles.size())));
+  st.st = s;
+  CUDA_TRY(dalloc(&st.d_outs, st.outs.size(), s));
+  CUDA_TRY(dalloc(&st.d_segs, st.segs.size(), s));
+  CUDA_TRY(dalloc(&st.d_tiles, st.tiles.size(), s));
   if (!st.outs.empty())
     CUDA_TRY(cudaMemcpyAsync(st.d_outs, st.outs.data(), sizeof(DOut) * st.outs.size(),
                              cudaMemcpyHostToDevice, s));
@@ -305,16 +306,6 @@ int finalize_plan(dmrgx_ctx* c, const double* renv_vals, const std::vector<int64
   if (rc) return rc;
   rc = upload_stage(c->st2, c->stream);
   if (rc) return rc;
-  const size_t need = sizeof(double) * (size_t)std::max<int64_t>(1, c->n * f);
-  if (need > c->h_cap) {
-    if (c->h_in) cudaFreeHost(c->h_in);
-    if (c->h_out) cudaFreeHost(c->h_out);
-    c->h_in = c->h_out = nullptr;
-    c->h_cap = 0;
-    CUDA_TRY(cudaMallocHost((void**)&c->h_in, need));
-    CUDA_TRY(cudaMallocHost((void**)&c->h_out, need));
-    c->h_cap = need;
-  }
   // ri/li are host temporaries: wait for the uploads before they go away
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->sp.free_device();
@@ -468,8 +459,6 @@ void dmrgx_ctx_destroy(dmrgx_ctx* c) {
   c->store.release();
   c->din.release();
   c->dout.release();
-  if (c->h_in) cudaFreeHost(c->h_in);
-  if (c->h_out) cudaFreeHost(c->h_out);
   cudaStreamDestroy(c->stream);
   delete c;
 }

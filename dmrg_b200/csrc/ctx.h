@@ -33,6 +33,7 @@ struct Stage {
   DTile* d_tiles = nullptr;
   bool full_cover = true;   // every element of the output is written by some tile
   int64_t a_len = 0;        // real length of operand-A image
+  cudaStream_t st = nullptr; // stream of the device arrays
   void free_device();
 };
 
@@ -114,9 +115,6 @@ struct dmrgx_ctx {
   bool prof = false;                            // per-launch event timing
   std::vector<cudaEvent_t> prof_ev;             // 4 per timed matvec
   void prof_mark();                             // record one event if profiling
-  double* h_in = nullptr;                       // pinned staging
-  double* h_out = nullptr;
-  size_t h_cap = 0;
 
   bool per_block = false;                       // DMRGX_SCHED_PER_BLOCK: one GEMM per task row
   void* blas = nullptr;                         // cuBLAS handle of the per-block schedule

@@ -237,7 +237,7 @@ struct Run {
   std::vector<double> energies, trunc;
   std::vector<int64_t> matvecs;
   std::vector<double> step_s;  // wall seconds of every step
-  double t_eig = 0, t_svd = 0, t_env = 0, t_fuse = 0;
+  double t_eig = 0, t_svd = 0, t_env = 0, t_fuse = 0, t_plan = 0;
   std::string err;
 
   const QTensor& mpo(int i) const { return i == 0 ? *ledge : (i == L - 1 ? *redge : *bulk); }
@@ -245,6 +245,14 @@ struct Run {
   static double now() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
         .count();
+  }
+
+  // plan of a step (timed)
+  int plan(const QTensor& Lop, const QTensor& Rop, int ln, int rn, int sec, const Group& G) {
+    const double t0 = now();
+    const int rc = plan_build_device(c, Lop, Rop, ln, rn, sec, G);
+    t_plan += now() - t0;
+    return rc;
   }
 
   // lowest state of the current plan -> psi tensor; records energies
@@ -338,7 +346,7 @@ struct Run {
   int two_sites(int l, int r, int cutoff) {
     const QTensor& le = mpo(l);
     const QTensor& re = mpo(r);
-    int rc = plan_build_device(c, le, re, 2, 1, sector, E.G);
+    int rc = plan(le, re, 2, 1, sector, E.G);
     if (rc) return fail(rc);
     QTPtr psi, U, V;
     if ((rc = solve(l, r, psi))) return rc;
@@ -354,7 +362,7 @@ struct Run {
   int update_two(int l, int r, int cutoff) {
     QTPtr le = fuse_left(l), re = fuse_right(r);
     if (!le || !re) return DMRGX_E_CUDA;
-    int rc = plan_build_device(c, *le, *re, 3, 2, sector, E.G);
+    int rc = plan(*le, *re, 3, 2, sector, E.G);
     if (rc) return fail(rc);
     QTPtr psi, U, V;
     if ((rc = solve(l, r, psi))) return rc;
@@ -370,7 +378,7 @@ struct Run {
   int move2right(int l, int r, int cutoff) {
     QTPtr le = fuse_left(l);
     if (!le) return DMRGX_E_CUDA;
-    int rc = plan_build_device(c, *le, *env[r], 3, 1, sector, E.G);
+    int rc = plan(*le, *env[r], 3, 1, sector, E.G);
     if (rc) return fail(rc);
     QTPtr psi, U, V;
     if ((rc = solve(l, r, psi))) return rc;
@@ -385,7 +393,7 @@ struct Run {
   int move2left(int l, int r, int cutoff) {
     QTPtr re = fuse_right(r);
     if (!re) return DMRGX_E_CUDA;
-    int rc = plan_build_device(c, *env[l], *re, 2, 2, sector, E.G);
+    int rc = plan(*env[l], *re, 2, 2, sector, E.G);
     if (rc) return fail(rc);
     QTPtr psi, U, V;
     if ((rc = solve(l, r, psi))) return rc;
@@ -938,5 +946,22 @@ extern "C" int dmrgx_step_seconds(dmrgx_ctx* c, double* out, int64_t cap, int64_
   const Run* R = static_cast<const Run*>(c->run);
   *nsteps = (int64_t)R->step_s.size();
   for (int64_t i = 0; out && i < *nsteps && i < cap; i++) out[i] = R->step_s[i];
+  return 0;
+}
+
+extern "C" int dmrgx_run_seconds(dmrgx_ctx* c, double* out, int cap) {
+  if (!c || !c->run || !out || cap < 6) {
+    set_error("run_seconds: need a context with a dmrgx_dmrg state and 6 slots");
+    return DMRGX_E_ARG;
+  }
+  const Run* R = static_cast<const Run*>(c->run);
+  double tot = 0;
+  for (double x : R->step_s) tot += x;
+  out[0] = tot;
+  out[1] = R->t_eig;
+  out[2] = R->t_svd;
+  out[3] = R->t_env;
+  out[4] = R->t_fuse;
+  out[5] = R->t_plan;
   return 0;
 }

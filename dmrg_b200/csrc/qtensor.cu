@@ -8,6 +8,7 @@
 // SVDs through cuSOLVER's Jacobi SVD (gesvdj), loaded at run time.
 #include <cuComplex.h>
 #include <cuda_runtime.h>
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 #include <dlfcn.h>
 
@@ -177,13 +178,23 @@ struct Solver {
   bool tried = false, ok = false;
   decltype(&cusolverDnCreate) create;
   decltype(&cusolverDnSetStream) set_stream;
-  decltype(&cusolverDnCreateGesvdjInfo) create_info;
-  decltype(&cusolverDnXgesvdjSetTolerance) set_tol;
-  decltype(&cusolverDnXgesvdjSetMaxSweeps) set_sweeps;
-  decltype(&cusolverDnDgesvdj_bufferSize) d_buf;
-  decltype(&cusolverDnDgesvdj) d_svd;
-  decltype(&cusolverDnZgesvdj_bufferSize) z_buf;
-  decltype(&cusolverDnZgesvdj) z_svd;
+  decltype(&cusolverDnDsyevd_bufferSize) d_evd_buf;
+  decltype(&cusolverDnDsyevd) d_evd;
+  decltype(&cusolverDnZheevd_bufferSize) z_evd_buf;
+  decltype(&cusolverDnZheevd) z_evd;
+  decltype(&cusolverDnDgeqrf_bufferSize) d_qrf_buf;
+  decltype(&cusolverDnDgeqrf) d_qrf;
+  decltype(&cusolverDnZgeqrf_bufferSize) z_qrf_buf;
+  decltype(&cusolverDnZgeqrf) z_qrf;
+  decltype(&cusolverDnDorgqr_bufferSize) d_orgqr_buf;
+  decltype(&cusolverDnDorgqr) d_orgqr;
+  decltype(&cusolverDnZungqr_bufferSize) z_ungqr_buf;
+  decltype(&cusolverDnZungqr) z_ungqr;
+  // cuBLAS (libcublas.so.12) for the Gram and projection products
+  decltype(&cublasCreate_v2) blas_create;
+  decltype(&cublasSetStream_v2) blas_set_stream;
+  decltype(&cublasDgemm_v2) dgemm;
+  decltype(&cublasZgemm_v2) zgemm;
 };
 Solver g_sol;
 std::mutex g_sol_mu;
@@ -212,13 +223,33 @@ bool load_solver(std::string& err) {
   }
   SYM(create, cusolverDnCreate);
   SYM(set_stream, cusolverDnSetStream);
-  SYM(create_info, cusolverDnCreateGesvdjInfo);
-  SYM(set_tol, cusolverDnXgesvdjSetTolerance);
-  SYM(set_sweeps, cusolverDnXgesvdjSetMaxSweeps);
-  SYM(d_buf, cusolverDnDgesvdj_bufferSize);
-  SYM(d_svd, cusolverDnDgesvdj);
-  SYM(z_buf, cusolverDnZgesvdj_bufferSize);
-  SYM(z_svd, cusolverDnZgesvdj);
+  SYM(d_evd_buf, cusolverDnDsyevd_bufferSize);
+  SYM(d_evd, cusolverDnDsyevd);
+  SYM(z_evd_buf, cusolverDnZheevd_bufferSize);
+  SYM(z_evd, cusolverDnZheevd);
+  SYM(d_qrf_buf, cusolverDnDgeqrf_bufferSize);
+  SYM(d_qrf, cusolverDnDgeqrf);
+  SYM(z_qrf_buf, cusolverDnZgeqrf_bufferSize);
+  SYM(z_qrf, cusolverDnZgeqrf);
+  SYM(d_orgqr_buf, cusolverDnDorgqr_bufferSize);
+  SYM(d_orgqr, cusolverDnDorgqr);
+  SYM(z_ungqr_buf, cusolverDnZungqr_bufferSize);
+  SYM(z_ungqr, cusolverDnZungqr);
+  {
+    const char* bn[] = {getenv("DMRGX_CUBLAS"), "libcublas.so.12",
+                        "/usr/local/cuda/lib64/libcublas.so.12", "libcublas.so"};
+    lib = nullptr;
+    for (const char* n : bn)
+      if (n && (lib = dlopen(n, RTLD_NOW | RTLD_LOCAL))) break;
+    if (!lib) {
+      err = "cuBLAS (libcublas.so.12) not found";
+      return false;
+    }
+  }
+  SYM(blas_create, cublasCreate_v2);
+  SYM(blas_set_stream, cublasSetStream_v2);
+  SYM(dgemm, cublasDgemm_v2);
+  SYM(zgemm, cublasZgemm_v2);
 #undef SYM
   g_sol.ok = true;
   return true;
@@ -228,22 +259,75 @@ bool load_solver(std::string& err) {
 // run their SVDs concurrently
 struct SolverHandle {
   cusolverDnHandle_t h = nullptr;
-  gesvdjInfo_t info = nullptr;
+  cublasHandle_t blas = nullptr;
 };
 thread_local SolverHandle t_sol;
 
 bool thread_handle(std::string& err) {
-  if (t_sol.h) return true;
-  if (g_sol.create(&t_sol.h) != CUSOLVER_STATUS_SUCCESS ||
-      g_sol.create_info(&t_sol.info) != CUSOLVER_STATUS_SUCCESS) {
-    err = "cuSOLVER initialisation failed";
-    t_sol.h = nullptr;
+  if (t_sol.h && t_sol.blas) return true;
+  if ((!t_sol.h && g_sol.create(&t_sol.h) != CUSOLVER_STATUS_SUCCESS) ||
+      (!t_sol.blas && g_sol.blas_create(&t_sol.blas) != CUBLAS_STATUS_SUCCESS)) {
+    err = "cuSOLVER / cuBLAS initialisation failed";
     return false;
   }
-  g_sol.set_tol(t_sol.info, 1e-15);
-  g_sol.set_sweeps(t_sol.info, 100);
   return true;
 }
+
+// ---- small kernels of the block SVD (column-major n_rows x n_cols, f doubles/element)
+// dst[:, j] = src[:, n-1-j] of an n x n matrix
+__global__ void rev_cols(const double* __restrict__ src, double* __restrict__ dst, int64_t n,
+                         int f) {
+  const int64_t tot = n * n * f;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t col = e / (n * f), rem = e % (n * f);
+    dst[e] = src[(n - 1 - col) * n * f + rem];
+  }
+}
+// Y[:, j] *= sc[j], j < k (real scale)
+__global__ void scale_cols(double* __restrict__ Y, int64_t rows, int k,
+                           const double* __restrict__ sc, int f) {
+  const int64_t tot = rows * k * f;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot;
+       e += (int64_t)gridDim.x * blockDim.x)
+    Y[e] *= sc[e / (rows * f)];
+}
+// ph[j] = R_jj / |R_jj| from the upper triangle of a QR factorisation (ld rows)
+__global__ void qr_phase(const double* __restrict__ Y, int64_t ld, int k, double* __restrict__ ph,
+                         int f) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= k) return;
+  const double re = Y[(j * ld + j) * f], im = f == 2 ? Y[(j * ld + j) * f + 1] : 0.0;
+  const double a = sqrt(re * re + im * im);
+  ph[2 * j] = a > 0 ? re / a : 1.0;
+  ph[2 * j + 1] = a > 0 ? im / a : 0.0;
+}
+// Q[:, j] *= ph[j], j < k
+__global__ void apply_phase(double* __restrict__ Q, int64_t rows, int k,
+                            const double* __restrict__ ph, int f) {
+  const int64_t tot = rows * k;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = e / rows;
+    if (f == 1) {
+      Q[e] *= ph[2 * j];
+    } else {
+      const double qr = Q[2 * e], qi = Q[2 * e + 1], pr = ph[2 * j], pi = ph[2 * j + 1];
+      Q[2 * e] = qr * pr - qi * pi;
+      Q[2 * e + 1] = qr * pi + qi * pr;
+    }
+  }
+}
+// identity n x n
+__global__ void eye(double* __restrict__ Q, int64_t n, int f) {
+  const int64_t tot = n * n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    Q[e * f] = (e % n == e / n) ? 1.0 : 0.0;
+    if (f == 2) Q[e * f + 1] = 0.0;
+  }
+}
+int gridfor(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(4096, (n + 255) / 256)); }
 
 }  // namespace
 
@@ -828,85 +912,203 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
     dfree(dM, E.stream);
     return -1;
   }
-  // per-sector SVD of X = A^T (column-major C x R view of the row-major block),
-  // all sectors queued on the stream, one synchronisation at the end
+  // Per-sector SVD of X = A^T (column-major C x R view of the row-major block),
+  // X = Ux S Vx^H with full Ux (C x C) and Vx (R x R), from the Hermitian
+  // eigenproblem of the smaller Gram matrix (divide and conquer, syevd/heevd):
+  //   C <= R: X X^H = Ux S^2 Ux^H, Vx[:, j] = X^H Ux[:, j] / s_j
+  //   C >  R: X^H X = Vx S^2 Vx^H, Ux[:, j] = X Vx[:, j] / s_j
+  // for s_j > 1e-13 s_0; a Householder QR of those derived columns makes them
+  // orthonormal to working precision (phases restored from R's diagonal) and
+  // completes them to a full unitary -- the complement columns the reference
+  // takes from LAPACK's full U / V (src/qtensor.cpp:1221-1252).  Singular values
+  // come out accurate to ~1e-16 s_0^2 / s_j absolutely, so the truncation weight
+  // sum_{discarded} s^2 is exact to ~1e-16 per value.
   std::vector<std::vector<double>> S(ns);
   std::vector<double*> Ux(ns, nullptr), Vx(ns, nullptr);
-  std::vector<int64_t> soff(ns + 1, 0);
-  for (int i = 0; i < ns; i++) soff[i + 1] = soff[i] + std::min(Cc[i], Rr[i]);
+  std::vector<double*> Gm(ns, nullptr), Wd(ns, nullptr);
   int* dinfo = nullptr;
-  double *dS = nullptr, *work = nullptr;
-  bool fail = dalloc(&dinfo, (size_t)std::max(1, ns), E.stream) != cudaSuccess ||
-              dalloc(&dS, (size_t)std::max<int64_t>(1, soff[ns]), E.stream) != cudaSuccess;
+  double *work = nullptr, *aux = nullptr;
+  bool fail = dalloc(&dinfo, (size_t)std::max(1, 3 * ns), E.stream) != cudaSuccess;
   g_sol.set_stream(t_sol.h, E.stream);
+  g_sol.blas_set_stream(t_sol.blas, E.stream);
+  const bool cx = f == 2;
+  const cuDoubleComplex z1 = make_cuDoubleComplex(1.0, 0.0), z0 = make_cuDoubleComplex(0.0, 0.0);
+  const double d1 = 1.0, d0 = 0.0;
+  const cublasOperation_t OPH = cx ? CUBLAS_OP_C : CUBLAS_OP_T;
+  auto gemm = [&](cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
+                  const double* A_, int lda, const double* B_, int ldb, double* C_, int ldc) {
+    if (cx)
+      return g_sol.zgemm(t_sol.blas, ta, tb, m, n, k, &z1, (const cuDoubleComplex*)A_, lda,
+                         (const cuDoubleComplex*)B_, ldb, &z0, (cuDoubleComplex*)C_, ldc) ==
+             CUBLAS_STATUS_SUCCESS;
+    return g_sol.dgemm(t_sol.blas, ta, tb, m, n, k, &d1, A_, lda, B_, ldb, &d0, C_, ldc) ==
+           CUBLAS_STATUS_SUCCESS;
+  };
+  // ---- phase 1: Gram matrices and their eigendecompositions, all sectors queued
   int lmax = 1;
-  cusolverStatus_t st = CUSOLVER_STATUS_SUCCESS;
   for (int i = 0; i < ns && !fail; i++) {
-    const int m = (int)Cc[i], n = (int)Rr[i];
-    S[i].assign(std::min(m, n), 0.0);
-    if (std::min(m, n) == 0) continue;
-    if (dalloc(&Ux[i], (size_t)m * m * f, E.stream) != cudaSuccess ||
-        dalloc(&Vx[i], (size_t)n * n * f, E.stream) != cudaSuccess) {
+    const int C = (int)Cc[i], R = (int)Rr[i], p = std::min(C, R);
+    S[i].assign(p, 0.0);
+    if (p == 0) continue;
+    const double* X = dM + moff[i] * f;
+    if (dalloc(&Gm[i], (size_t)p * p * f, E.stream) != cudaSuccess ||
+        dalloc(&Wd[i], (size_t)p, E.stream) != cudaSuccess) {
       fail = true;
       break;
     }
-    int lwork = 0;
-    double* X = dM + moff[i] * f;
-    if (f == 1)
-      st = g_sol.d_buf(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, X, m, dS + soff[i], Ux[i], m,
-                       Vx[i], n, &lwork, t_sol.info);
-    else
-      st = g_sol.z_buf(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, (cuDoubleComplex*)X, m,
-                       dS + soff[i], (cuDoubleComplex*)Ux[i], m, (cuDoubleComplex*)Vx[i], n,
-                       &lwork, t_sol.info);
+    if (C <= R) fail = !gemm(CUBLAS_OP_N, OPH, C, C, R, X, C, X, C, Gm[i], C);
+    else fail = !gemm(OPH, CUBLAS_OP_N, R, R, C, X, C, X, C, Gm[i], R);
+    int lw = 0;
+    const cusolverStatus_t st = cx ? g_sol.z_evd_buf(t_sol.h, CUSOLVER_EIG_MODE_VECTOR,
+                                                     CUBLAS_FILL_MODE_LOWER, p,
+                                                     (cuDoubleComplex*)Gm[i], p, Wd[i], &lw)
+                                   : g_sol.d_evd_buf(t_sol.h, CUSOLVER_EIG_MODE_VECTOR,
+                                                     CUBLAS_FILL_MODE_LOWER, p, Gm[i], p, Wd[i],
+                                                     &lw);
     if (st != CUSOLVER_STATUS_SUCCESS) fail = true;
-    lmax = std::max(lmax, lwork);
+    lmax = std::max(lmax, lw);
   }
   if (!fail) fail = dalloc(&work, (size_t)lmax * f, E.stream) != cudaSuccess;
   for (int i = 0; i < ns && !fail; i++) {
-    const int m = (int)Cc[i], n = (int)Rr[i];
-    if (std::min(m, n) == 0) continue;
-    double* X = dM + moff[i] * f;
-    // gesvdj overwrites its input: the sector matrices are not needed afterwards
-    if (f == 1)
-      st = g_sol.d_svd(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, X, m, dS + soff[i], Ux[i], m,
-                       Vx[i], n, work, lmax, dinfo + i, t_sol.info);
-    else
-      st = g_sol.z_svd(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, 0, m, n, (cuDoubleComplex*)X, m,
-                       dS + soff[i], (cuDoubleComplex*)Ux[i], m, (cuDoubleComplex*)Vx[i], n,
-                       (cuDoubleComplex*)work, lmax, dinfo + i, t_sol.info);
+    const int p = (int)std::min(Cc[i], Rr[i]);
+    if (p == 0) continue;
+    const cusolverStatus_t st =
+        cx ? g_sol.z_evd(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, p,
+                         (cuDoubleComplex*)Gm[i], p, Wd[i], (cuDoubleComplex*)work, lmax,
+                         dinfo + 3 * i)
+           : g_sol.d_evd(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, p, Gm[i], p,
+                         Wd[i], work, lmax, dinfo + 3 * i);
     if (st != CUSOLVER_STATUS_SUCCESS) fail = true;
   }
-  std::vector<double> hS((size_t)std::max<int64_t>(1, soff[ns]));
-  std::vector<int> hinfo((size_t)std::max(1, ns), 0);
+  std::vector<std::vector<double>> lam(ns);
+  std::vector<int> hinfo((size_t)std::max(1, 3 * ns), 0);
   if (!fail) {
-    cudaMemcpyAsync(hS.data(), dS, sizeof(double) * hS.size(), cudaMemcpyDeviceToHost, E.stream);
-    cudaMemcpyAsync(hinfo.data(), dinfo, sizeof(int) * hinfo.size(), cudaMemcpyDeviceToHost,
-                    E.stream);
+    for (int i = 0; i < ns; i++) {
+      lam[i].assign(S[i].size(), 0.0);
+      if (!lam[i].empty())
+        cudaMemcpyAsync(lam[i].data(), Wd[i], sizeof(double) * lam[i].size(),
+                        cudaMemcpyDeviceToHost, E.stream);
+    }
     if (cudaStreamSynchronize(E.stream) != cudaSuccess) fail = true;
   }
-  for (int i = 0; i < ns && !fail; i++) {
-    if (hinfo[i] != 0) {
-      err = "svd: cuSOLVER gesvdj failed (info " + std::to_string(hinfo[i]) + ")";
-      fail = true;
-      break;
-    }
-    for (size_t q = 0; q < S[i].size(); q++) S[i][q] = hS[soff[i] + q];
-    for (size_t q = 1; q < S[i].size() && !fail; q++)
-      if (S[i][q] > S[i][q - 1]) {
-        err = "svd: singular values not in descending order";
+  // ---- phase 2: singular values, the derived side, QR completion
+  std::vector<int> kk(ns, 0);
+  std::vector<double*> taus(ns, nullptr), scs(ns, nullptr), phs(ns, nullptr);
+  if (!fail) {
+    int lw2 = 1;
+    for (int i = 0; i < ns && !fail; i++) {
+      const int p = (int)S[i].size();
+      if (p == 0) continue;
+      for (int j = 0; j < p; j++) S[i][j] = std::sqrt(std::max(lam[i][p - 1 - j], 0.0));
+      int k = 0;
+      while (k < p && S[i][k] > 1e-13 * S[i][0]) k++;
+      kk[i] = k;
+      const int C = (int)Cc[i], R = (int)Rr[i], q = std::max(C, R);
+      double* full = nullptr;  // the Gram side, columns in descending order
+      double* other = nullptr; // the derived side, q x q
+      if (dalloc(&full, (size_t)p * p * f, E.stream) != cudaSuccess ||
+          dalloc(&other, (size_t)q * q * f, E.stream) != cudaSuccess) {
+        dfree(full, E.stream);
         fail = true;
+        break;
       }
+      rev_cols<<<gridfor((int64_t)p * p * f), 256, 0, E.stream>>>(Gm[i], full, p, f);
+      if (C <= R) {
+        Ux[i] = full;
+        Vx[i] = other;
+      } else {
+        Vx[i] = full;
+        Ux[i] = other;
+      }
+      int lq = 0, lo = 0;
+      if (k > 0) {
+        const cusolverStatus_t a =
+            cx ? g_sol.z_qrf_buf(t_sol.h, q, k, (cuDoubleComplex*)other, q, &lq)
+               : g_sol.d_qrf_buf(t_sol.h, q, k, other, q, &lq);
+        const cusolverStatus_t b =
+            cx ? g_sol.z_ungqr_buf(t_sol.h, q, q, k, (const cuDoubleComplex*)other, q,
+                                   (const cuDoubleComplex*)other, &lo)
+               : g_sol.d_orgqr_buf(t_sol.h, q, q, k, other, q, other, &lo);
+        if (a != CUSOLVER_STATUS_SUCCESS || b != CUSOLVER_STATUS_SUCCESS) fail = true;
+      }
+      lw2 = std::max(lw2, std::max(lq, lo));
+    }
+    if (!fail && lw2 > lmax) {
+      dfree(work, E.stream);
+      work = nullptr;
+      fail = dalloc(&work, (size_t)lw2 * f, E.stream) != cudaSuccess;
+      lmax = lw2;
+    }
+    for (int i = 0; i < ns && !fail; i++) {
+      const int p = (int)S[i].size(), k = kk[i];
+      if (p == 0) continue;
+      const int C = (int)Cc[i], R = (int)Rr[i], q = std::max(C, R);
+      double* other = C <= R ? Vx[i] : Ux[i];
+      const double* full = C <= R ? Ux[i] : Vx[i];
+      const double* X = dM + moff[i] * f;
+      if (k == 0) {
+        eye<<<gridfor((int64_t)q * q), 256, 0, E.stream>>>(other, q, f);
+        continue;
+      }
+      std::vector<double> inv_s(k);
+      for (int j = 0; j < k; j++) inv_s[j] = 1.0 / S[i][j];
+      if (dalloc(&scs[i], (size_t)k, E.stream) != cudaSuccess ||
+          dalloc(&taus[i], (size_t)k * f, E.stream) != cudaSuccess ||
+          dalloc(&phs[i], (size_t)2 * k, E.stream) != cudaSuccess) {
+        fail = true;
+        break;
+      }
+      cudaMemcpyAsync(scs[i], inv_s.data(), sizeof(double) * k, cudaMemcpyHostToDevice, E.stream);
+      // derived columns into the first k columns of `other` (q x q, ld q)
+      if (C <= R) fail = !gemm(OPH, CUBLAS_OP_N, R, k, C, X, C, full, C, other, R);
+      else fail = !gemm(CUBLAS_OP_N, CUBLAS_OP_N, C, k, R, X, C, full, R, other, C);
+      if (fail) break;
+      scale_cols<<<gridfor((int64_t)q * k * f), 256, 0, E.stream>>>(other, q, k, scs[i], f);
+      cusolverStatus_t st =
+          cx ? g_sol.z_qrf(t_sol.h, q, k, (cuDoubleComplex*)other, q, (cuDoubleComplex*)taus[i],
+                           (cuDoubleComplex*)work, lmax, dinfo + 3 * i + 1)
+             : g_sol.d_qrf(t_sol.h, q, k, other, q, taus[i], work, lmax, dinfo + 3 * i + 1);
+      if (st != CUSOLVER_STATUS_SUCCESS) {
+        fail = true;
+        break;
+      }
+      qr_phase<<<(k + 127) / 128, 128, 0, E.stream>>>(other, q, k, phs[i], f);
+      st = cx ? g_sol.z_ungqr(t_sol.h, q, q, k, (cuDoubleComplex*)other, q,
+                              (const cuDoubleComplex*)taus[i], (cuDoubleComplex*)work, lmax,
+                              dinfo + 3 * i + 2)
+              : g_sol.d_orgqr(t_sol.h, q, q, k, other, q, taus[i], work, lmax, dinfo + 3 * i + 2);
+      if (st != CUSOLVER_STATUS_SUCCESS) {
+        fail = true;
+        break;
+      }
+      apply_phase<<<gridfor((int64_t)q * k), 256, 0, E.stream>>>(other, q, k, phs[i], f);
+    }
+    if (!fail) {
+      cudaMemcpyAsync(hinfo.data(), dinfo, sizeof(int) * hinfo.size(), cudaMemcpyDeviceToHost,
+                      E.stream);
+      if (cudaStreamSynchronize(E.stream) != cudaSuccess) fail = true;
+      for (int i = 0; i < 3 * ns && !fail; i++)
+        if (hinfo[i] != 0) {
+          err = "svd: cuSOLVER eigensolver / QR failed (info " + std::to_string(hinfo[i]) + ")";
+          fail = true;
+        }
+    }
   }
-  if (fail && err.empty())
-    err = "svd: cuSOLVER gesvdj failed (status " + std::to_string((int)st) + ")";
-  dfree(dS, E.stream);
+  if (fail && err.empty()) err = "svd: cuSOLVER / cuBLAS call failed";
+  for (int i = 0; i < ns; i++) {
+    dfree(Gm[i], E.stream);
+    dfree(Wd[i], E.stream);
+    dfree(taus[i], E.stream);
+    dfree(scs[i], E.stream);
+    dfree(phs[i], E.stream);
+  }
   dfree(work, E.stream);
+  dfree(aux, E.stream);
   dfree(dinfo, E.stream);
   dfree(dM, E.stream);
   auto free_all = [&]() {
-    for (auto p : Ux) dfree(p, E.stream);
-    for (auto p : Vx) dfree(p, E.stream);
+    for (auto p2 : Ux) dfree(p2, E.stream);
+    for (auto p2 : Vx) dfree(p2, E.stream);
   };
   if (fail) {
     free_all();

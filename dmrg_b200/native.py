@@ -45,6 +45,7 @@ SIGNATURES = {
     "dmrgx_split_tuning": (_i, [_vp, _ip, _i]),
     "dmrgx_matvec_launches": (_i, [_vp, _ip]),
     "dmrgx_step_seconds": (_i, [_vp, _dp, _i64, _i64p]),
+    "dmrgx_run_seconds": (_i, [_vp, _dp, _i]),
     "dmrgx_adjoint": (_i, [_vp, _i, _dp, _i, _dp, _i64, _i64p, _dp, _dp]),
     "dmrgx_expect": (_i, [_vp, _dp, _i, _dp]),
     "dmrgx_profile": (_i, [_vp, _i]),
@@ -246,6 +247,12 @@ class Context:
         self._nparams = 3 if code == 0 else min(4, max(3, par.size))
         return dict(lr=lr[:k], energies=en[:k], trunc=tr[:k], matvecs=mv[:k],
                     seconds=dict(total=sec[0], eig=sec[1], svd=sec[2], env=sec[3], fuse=sec[4]))
+
+    def run_seconds(self):
+        """Time split of the last dmrg() run: steps, eig, svd, env, fuse, plan (seconds)."""
+        out = np.zeros(6)
+        _check(lib().dmrgx_run_seconds(self.ptr, out.ctypes.data_as(_dp), 6))
+        return dict(zip(("steps", "eig", "svd", "env", "fuse", "plan"), out.tolist()))
 
     def step_seconds(self):
         """Wall seconds of every site step of the last dmrg() run."""

@@ -213,6 +213,12 @@ int dmrgx_dmrg(dmrgx_ctx* ctx, int model, int L, int m, int sweeps, int sector,
  * count, out (cap values, may be NULL) the times. */
 int dmrgx_step_seconds(dmrgx_ctx* ctx, double* out, int64_t cap, int64_t* nsteps);
 
+/* Time split of the last dmrgx_dmrg (wall seconds): out[0] all site steps,
+ * [1] eigensolver, [2] block SVD, [3] environment update, [4] env (x) MPO fusion,
+ * [5] plan building (sector bookkeeping, task lists, device images, split-precision
+ * images and tuning).  cap >= 6. */
+int dmrgx_run_seconds(dmrgx_ctx* ctx, double* out, int cap);
+
 /* Gradient of the ground-state energy of the last dmrgx_dmrg with respect to the
  * MPO tensors and the model parameters, by adjoint contractions of the
  * effective Hamiltonian.  New work: the reference has no derivatives; it
