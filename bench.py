@@ -285,7 +285,9 @@ def time_matvecs(torch, ctx, stream, xs, ys, flush, steps, warmup, profile=False
     torch.cuda.synchronize()
     if profile:
         ctx.profile(True)
+    torch.cuda.nvtx.range_push("timed")  # ncu --nvtx --nvtx-include "timed/" selects these
     evs = [one(True) for _ in range(steps)]
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     prof = None
     if profile:

@@ -89,3 +89,36 @@ def run_batch(specs, workers=None, **kw):
     with cf.ThreadPoolExecutor(max_workers=workers) as ex:
         res = list(ex.map(lambda s: run_chain(s, **kw), specs))
     return res, time.time() - t0
+
+
+def main():
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="16-chain gradient check (XYZ, L=64, m in {64..512})")
+    ap.add_argument("--sweeps", type=int, default=2)
+    ap.add_argument("--prec", default="bf16x3", choices=["fp64", "bf16x3", "tf32x3"])
+    ap.add_argument("--workers", type=int, default=16)
+    ap.add_argument("--L", type=int, default=64)
+    ap.add_argument("--no-fd", action="store_true")
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+    prec = {"fp64": native.PREC_FP64, "bf16x3": native.PREC_BF16X3,
+            "tf32x3": native.PREC_TF32X3}[a.prec]
+    specs = config5_chains(L=a.L)
+    res, wall = run_batch(specs, workers=a.workers, sweeps=a.sweeps, prec=prec, fd=not a.no_fd)
+    summary = {"wall_s": wall, "chains": len(res), "sweeps": a.sweeps, "prec": a.prec,
+               "max_rel_hf_Jz": max(r["rel_hf_Jz"] for r in res),
+               "max_abs_hf_h": max(r["abs_hf_h"] for r in res)}
+    if not a.no_fd:
+        summary["max_rel_fd_Jz"] = max(r["rel_fd_Jz"] for r in res)
+        summary["max_abs_fd_h"] = max(r["abs_fd_h"] for r in res)
+    out = {"summary": summary, "chains": res}
+    if a.out:
+        with open(a.out, "w") as fh:
+            json.dump(out, fh, indent=1)
+    print(json.dumps(summary))
+
+
+if __name__ == "__main__":
+    main()
