@@ -33,6 +33,9 @@ METRIC = "H_eff matvec/s at m=1024 (U(1) microbench, two-site, D=5)"
 UNIT = "matvec/s"
 
 
+TRAFFIC_BF16X3 = 15.136512e6 + 24.813056e6  # bytes per matvec (both stage launches), ncu
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -416,7 +419,12 @@ def main():
                        "parallelism": f"replicas x{world}",
                        "l2": "flushed before every timed step: 256 MiB write, then 256 MiB read of a clean buffer (write-back done outside the timing)"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
-                         "frac": achieved / pk, "traffic": None, "kernel": kernel,
+                         "frac": achieved / pk,
+                         # dram__bytes_read.sum + dram__bytes_write.sum of the stage-1 and
+                         # stage-2 launches of one steady-state BF16x3 matvec of this workload,
+                         # one ncu capture (--nvtx-include "timed/", --set full)
+                         "traffic": TRAFFIC_BF16X3 if args.prec == "bf16x3" else None,
+                         "kernel": kernel,
                          "peak_source": peak_note,
                          "note": "achieved = algorithmic flops (2MNK per task, not counting the "
                                  "3 split products) / summed device time of the stage launches",
