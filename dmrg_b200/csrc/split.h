@@ -89,10 +89,12 @@ struct PadJob {
 };
 
 // Kernel configurations: cfg 0 tiles up to 256 columns with a 4-deep ring, cfg 1
-// up to 128 columns with a 7-deep ring.
+// up to 128 columns with a 7-deep ring (one CTA per SM); cfg 2 up to 128 / 3-deep
+// and cfg 3 up to 64 / 4-deep (two CTAs per SM).
 int tc_configs();
 int tc_cfg_tn(int cfg);
 int tc_cfg_stages(int cfg);
+int tc_cfg_ctas_per_sm(int cfg);
 int tc_smem_bytes(int cfg);
 int tc_tile_m();
 int tc_tile_n();        // workspace row stride (floats): the widest tile of any cfg

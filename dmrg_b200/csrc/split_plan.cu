@@ -266,7 +266,7 @@ int configure_stage(dmrgx_ctx* c, SplitStage& st, int cfg, bool halve, double ca
     const auto& r = st.req[g.bmap];
     g.brows = tile_width((int)r.rows, tn, halve);
   }
-  make_units(st, c->num_sms, cap_scale);
+  make_units(st, c->num_sms * tc_cfg_ctas_per_sm(cfg), cap_scale);
   const int slots = std::max(1, st.nslots);
   SP_TRY(c->sws.ensure((size_t)slots * tc_tile_m() * tc_tile_n() * sizeof(float)));
   return upload(st, c->stream);
@@ -277,8 +277,8 @@ namespace {
 // Autotuner of the split stages.  Key: the stage's block-shape histogram (the
 // multiset of output blocks' rows, columns and K-tile counts, rounded) and the
 // element type.  On a miss every candidate tiling -- kernel configuration
-// (256-column tiles / 4-deep ring or 128 / 7), halving of one-tile blocks,
-// K-split threshold x {0.5, 1, 2} -- is timed with CUDA events on the
+// (tc_cfg_*: four tile-width / ring-depth / CTAs-per-SM choices), halving of
+// one-tile blocks, K-split threshold x {0.5, 1, 2} -- is timed with CUDA events on the
 // context's stream (best of three launches after one warm-up, on the plan's own
 // buffers) and the fastest is kept for every later plan with the same histogram.
 struct TuneVal {

@@ -241,10 +241,12 @@ __device__ __forceinline__ void store16(const SOut& o, int row, int col0, const 
 }
 
 // TNX: widest tile (MMA N) of this instantiation; STAGES: depth of the ring.
-// Configurations: (256, 4) and (128, 7) -- the narrow one keeps more k-tiles in
-// flight for the same shared memory.
+// Configurations: (256, 4) and (128, 7) with one CTA per SM -- the narrow one
+// keeps more k-tiles in flight for the same shared memory -- and (128, 3),
+// (64, 4) sized for two CTAs per SM (one waits on TMA while the other computes;
+// the two accumulator pairs use all 512 TMEM columns).
 template <int EB, bool OUT_SPLIT, int TNX, int STAGES>
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(THREADS, 2)
 tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ units,
                 const int* __restrict__ cta_begin, const SOut* __restrict__ outs,
                 const SSeg2* __restrict__ segs, uint8_t* __restrict__ c_pair,
@@ -518,9 +520,10 @@ split_reduce(const SRed* __restrict__ reds, const SRedBlk* __restrict__ blks,
 
 }  // namespace
 
-int tc_configs() { return 2; }
-int tc_cfg_tn(int cfg) { return cfg == 0 ? 256 : 128; }
-int tc_cfg_stages(int cfg) { return cfg == 0 ? 4 : 7; }
+int tc_configs() { return 4; }
+int tc_cfg_tn(int cfg) { return cfg == 0 ? 256 : cfg == 3 ? 64 : 128; }
+int tc_cfg_stages(int cfg) { return cfg == 0 ? 4 : cfg == 1 ? 7 : cfg == 2 ? 3 : 4; }
+int tc_cfg_ctas_per_sm(int cfg) { return cfg >= 2 ? 2 : 1; }
 int tc_smem_bytes(int cfg) {
   const int st = tc_cfg_stages(cfg);
   return st * (A_BYTES + tc_cfg_tn(cfg) * ROWB) + 1024 + (2 * st + 4) * 8 + 16;
@@ -545,6 +548,14 @@ cudaError_t prepare_tc_gemm() {
   DMRGX_TC_ATTR(2, false, 128, 7, 1)
   DMRGX_TC_ATTR(4, true, 128, 7, 1)
   DMRGX_TC_ATTR(4, false, 128, 7, 1)
+  DMRGX_TC_ATTR(2, true, 128, 3, 2)
+  DMRGX_TC_ATTR(2, false, 128, 3, 2)
+  DMRGX_TC_ATTR(4, true, 128, 3, 2)
+  DMRGX_TC_ATTR(4, false, 128, 3, 2)
+  DMRGX_TC_ATTR(2, true, 64, 4, 3)
+  DMRGX_TC_ATTR(2, false, 64, 4, 3)
+  DMRGX_TC_ATTR(4, true, 64, 4, 3)
+  DMRGX_TC_ATTR(4, false, 64, 4, 3)
 #undef DMRGX_TC_ATTR
   return e;
 }
@@ -572,13 +583,29 @@ cudaError_t launch_tc_gemm(int eb, bool out_split, int cfg, const CUtensorMap* m
       if (out_split) DMRGX_TC_LAUNCH(4, true, 256, 4);
       else DMRGX_TC_LAUNCH(4, false, 256, 4);
     }
-  } else {
+  } else if (cfg == 1) {
     if (eb == 2) {
       if (out_split) DMRGX_TC_LAUNCH(2, true, 128, 7);
       else DMRGX_TC_LAUNCH(2, false, 128, 7);
     } else {
       if (out_split) DMRGX_TC_LAUNCH(4, true, 128, 7);
       else DMRGX_TC_LAUNCH(4, false, 128, 7);
+    }
+  } else if (cfg == 2) {
+    if (eb == 2) {
+      if (out_split) DMRGX_TC_LAUNCH(2, true, 128, 3);
+      else DMRGX_TC_LAUNCH(2, false, 128, 3);
+    } else {
+      if (out_split) DMRGX_TC_LAUNCH(4, true, 128, 3);
+      else DMRGX_TC_LAUNCH(4, false, 128, 3);
+    }
+  } else {
+    if (eb == 2) {
+      if (out_split) DMRGX_TC_LAUNCH(2, true, 64, 4);
+      else DMRGX_TC_LAUNCH(2, false, 64, 4);
+    } else {
+      if (out_split) DMRGX_TC_LAUNCH(4, true, 64, 4);
+      else DMRGX_TC_LAUNCH(4, false, 64, 4);
     }
   }
 #undef DMRGX_TC_LAUNCH

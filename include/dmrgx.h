@@ -80,8 +80,10 @@ int dmrgx_set_precision(dmrgx_ctx* ctx, int prec);
 int dmrgx_matvec_launches(dmrgx_ctx* ctx, int* out);
 
 /* The tiling the autotuner chose for the current split-precision plan.  The
- * split stages run one of two kernel configurations (tiles up to 256 columns
- * with a 4-deep shared-memory ring, or up to 128 with a 7-deep ring); when a
+ * split stages run one of four kernel configurations: 0 tiles up to 256 columns
+ * with a 4-deep shared-memory ring, 1 up to 128 with a 7-deep ring (one CTA per
+ * SM), 2 up to 128 with a 3-deep ring and 3 up to 64 with a 4-deep ring (two
+ * CTAs per SM); when a
  * plan's block-shape histogram (rows, columns and K-tiles of every output block,
  * rounded) is new, every candidate tiling is timed once on the device and the
  * fastest is cached for later plans (DMRGX_TUNE=0 in the environment turns the
