@@ -48,7 +48,7 @@ def parse():
                    help="also time the DMRG schedule (XYZ real chain) in three forms: plain "
                         "per-block FP64, grouped FP64, grouped headline precision")
     p.add_argument("--sweep-L", type=int, default=32)
-    p.add_argument("--sweep-m", type=int, default=512)
+    p.add_argument("--sweep-m", type=int, default=1024)
     p.add_argument("--sweep-n", type=int, default=1)
     return p.parse_args()
 

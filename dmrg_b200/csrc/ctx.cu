@@ -503,7 +503,7 @@ int dmrgx_split_tuning(dmrgx_ctx* c, int* out, int cap) {
   for (int i = 0; i < 2; i++) {
     out[4 * i] = st[i]->cfg;
     out[4 * i + 1] = st[i]->halve ? 1 : 0;
-    out[4 * i + 2] = (int)(st[i]->cap_scale * 100 + 0.5);
+    out[4 * i + 2] = st[i]->cap_scale >= 1e6 ? -100 : (int)(st[i]->cap_scale * 100 + 0.5);
     out[4 * i + 3] = st[i]->tuned ? 1 : 0;
   }
   return 0;

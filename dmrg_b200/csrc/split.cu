@@ -23,9 +23,9 @@ __device__ __forceinline__ uint32_t tf32_rna(float x) {
   return r;
 }
 
-// FP64 rows -> (hi, lo) pairs in pair layout.  Block b converts row rows[b].row
-// of job rows[b].job.  Each thread keeps up to 4 loads in flight (the kernel is
-// latency-bound on short rows otherwise).
+// FP64 rows -> (hi, lo) pairs in pair layout.  Each group of 64 threads converts
+// one listed row (RPB rows per block); each thread keeps up to 4 loads in flight
+// (the rows are short and the kernel is latency-bound otherwise).
 template <int EB>
 __device__ __forceinline__ void put_pair(uint8_t* row, int64_t k, double x) {
   constexpr int CH = 64 / EB;
@@ -45,12 +45,18 @@ __device__ __forceinline__ void put_pair(uint8_t* row, int64_t k, double x) {
   }
 }
 
+constexpr int RPB = 4;  // rows per block
+
 template <int EB>
-__global__ void __launch_bounds__(64) pad_split_kernel(const double* __restrict__ src,
-                                                       uint8_t* __restrict__ dst,
-                                                       const PadJob* __restrict__ jobs,
-                                                       const PadRow* __restrict__ rows) {
-  const PadRow pr = rows[blockIdx.x];
+__global__ void __launch_bounds__(64 * RPB) pad_split_kernel(const double* __restrict__ src,
+                                                             uint8_t* __restrict__ dst,
+                                                             const PadJob* __restrict__ jobs,
+                                                             const PadRow* __restrict__ rows,
+                                                             int nrows) {
+  const int r = blockIdx.x * RPB + (int)(threadIdx.x >> 6);
+  if (r >= nrows) return;
+  const PadRow pr = rows[r];
+  const int tx = (int)(threadIdx.x & 63);
   const PadJob jb = jobs[pr.job];
   const int gc = jb.groups * jb.cols;
   const double* s = src + jb.src + (int64_t)pr.row * gc;
@@ -58,7 +64,7 @@ __global__ void __launch_bounds__(64) pad_split_kernel(const double* __restrict_
     // complex row -> (re, -im, ...) and (im, re, ...)
     uint8_t* r0 = dst + (jb.dst + (int64_t)(2 * pr.row) * 2 * jb.kq) * EB;
     uint8_t* r1 = r0 + (int64_t)2 * jb.kq * EB;
-    for (int e = threadIdx.x; e < gc / 2; e += blockDim.x) {
+    for (int e = tx; e < gc / 2; e += 64) {
       const double re = __ldg(s + 2 * e), im = __ldg(s + 2 * e + 1);
       put_pair<EB>(r0, 2 * e, re);
       put_pair<EB>(r0, 2 * e + 1, -im);
@@ -72,12 +78,12 @@ __global__ void __launch_bounds__(64) pad_split_kernel(const double* __restrict_
     double x[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      const int e = e0 + u * 64 + threadIdx.x;
+      const int e = e0 + u * 64 + tx;
       x[u] = e < gc ? __ldg(s + e) : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      const int e = e0 + u * 64 + threadIdx.x;
+      const int e = e0 + u * 64 + tx;
       if (e >= gc) break;
       const int grp = e / jb.cols, j = e - grp * jb.cols;
       put_pair<EB>(row, (int64_t)grp * jb.colsp + j, x[u]);
@@ -89,12 +95,13 @@ __global__ void __launch_bounds__(64) pad_split_kernel(const double* __restrict_
 
 cudaError_t launch_pad_split(int eb, const double* src, void* dst, const PadJob* jobs,
                              const PadRow* rows, int nrows, cudaStream_t st) {
-  for (int r0 = 0; r0 < nrows; r0 += 1 << 30) {
-    const int n = std::min(nrows - r0, 1 << 30);
+  for (int r0 = 0; r0 < nrows; r0 += 1 << 28) {
+    const int n = std::min(nrows - r0, 1 << 28);
+    const int blocks = (n + RPB - 1) / RPB;
     if (eb == 2)
-      pad_split_kernel<2><<<n, 64, 0, st>>>(src, (uint8_t*)dst, jobs, rows + r0);
+      pad_split_kernel<2><<<blocks, 64 * RPB, 0, st>>>(src, (uint8_t*)dst, jobs, rows + r0, n);
     else
-      pad_split_kernel<4><<<n, 64, 0, st>>>(src, (uint8_t*)dst, jobs, rows + r0);
+      pad_split_kernel<4><<<blocks, 64 * RPB, 0, st>>>(src, (uint8_t*)dst, jobs, rows + r0, n);
   }
   return cudaGetLastError();
 }

@@ -100,7 +100,7 @@ int tc_tile_m();
 int tc_tile_n();        // workspace row stride (floats): the widest tile of any cfg
 int tc_ktile_bytes();
 
-// Convert the rows listed in `rows` (one thread block each) into pair layout.
+// Convert the rows listed in `rows` (64 threads each) into pair layout.
 cudaError_t launch_pad_split(int eb, const double* src, void* dst, const PadJob* jobs,
                              const PadRow* rows, int nrows, cudaStream_t st);
 

@@ -278,7 +278,7 @@ namespace {
 // multiset of output blocks' rows, columns and K-tile counts, rounded) and the
 // element type.  On a miss every candidate tiling -- kernel configuration
 // (tc_cfg_*: four tile-width / ring-depth / CTAs-per-SM choices), halving of
-// one-tile blocks, K-split threshold x {0.5, 1, 2} -- is timed with CUDA events on the
+// one-tile blocks, K-split threshold x {1, 2, 4, none} -- is timed with CUDA events on the
 // context's stream (best of three launches after one warm-up, on the plan's own
 // buffers) and the fastest is kept for every later plan with the same histogram.
 struct TuneVal {
@@ -348,7 +348,7 @@ int tune_stage(dmrgx_ctx* c, int which) {
   int rc = 0;
   for (int cfg = 0; cfg < tc_configs() && !rc; cfg++)
     for (int hv = 0; hv < 2 && !rc; hv++)
-      for (double cs : {0.5, 1.0, 2.0}) {
+      for (double cs : {1.0, 2.0, 4.0, 1e9}) {  // 1e9: no K-split
         rc = configure_stage(c, st, cfg, hv != 0, cs);
         if (rc) break;
         rc = launch_stage(c, which);  // warm-up

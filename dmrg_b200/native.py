@@ -151,7 +151,8 @@ class Context:
         return int(out[0])
 
     def split_tuning(self):
-        """Autotuner choice per split stage: list of (cfg, halve, cap_scale, tuned)."""
+        """Autotuner choice per split stage: list of (cfg, halve, cap_scale, tuned);
+        cap_scale -1 means no K-split."""
         out = np.zeros(8, np.int32)
         _check(lib().dmrgx_split_tuning(self.ptr, _ip(out), 8))
         return [(int(out[4 * i]), bool(out[4 * i + 1]), out[4 * i + 2] / 100.0, bool(out[4 * i + 3]))

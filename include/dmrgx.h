@@ -88,8 +88,8 @@ int dmrgx_matvec_launches(dmrgx_ctx* ctx, int* out);
  * rounded) is new, every candidate tiling is timed once on the device and the
  * fastest is cached for later plans (DMRGX_TUNE=0 in the environment turns the
  * tuner off).  out[0..3] stage 1, out[4..7] stage 2: configuration, halving of
- * one-tile blocks, K-split threshold scale x100, 1 if measured for this plan
- * (0: from the cache).  cap >= 8. */
+ * one-tile blocks, K-split threshold scale x100 (-100: no K-split), 1 if
+ * measured for this plan (0: from the cache).  cap >= 8. */
 int dmrgx_split_tuning(dmrgx_ctx* ctx, int* out, int cap);
 
 /* Select the launch schedule of the matvec (DMRGX_SCHED_*).  Default grouped.
