@@ -524,7 +524,8 @@ int dmrgx_plan_build(dmrgx_ctx* c, const int* lenv_meta, const void* lenv_vals,
                      int sector, int group_n, int fermion) {
   ARG_CHECK(c, "null context");
   ARG_CHECK(lenv_vals && renv_vals, "plan_build: null environment values");
-  ARG_CHECK(group_n >= 1 && group_n <= 4096, "plan_build: group_n out of range");
+  Group G;
+  ARG_CHECK(make_group(group_n, fermion, G), "plan_build: group_n out of range");
   QMeta L, R;
   std::string e = L.parse(lenv_meta);
   ARG_CHECK(e.empty(), "plan_build: lenv metadata: " + e);
@@ -532,9 +533,6 @@ int dmrgx_plan_build(dmrgx_ctx* c, const int* lenv_meta, const void* lenv_vals,
   ARG_CHECK(e.empty(), "plan_build: renv metadata: " + e);
   ARG_CHECK(l_num >= 2 && l_num <= L.nleg() && r_num >= 1 && r_num <= R.nleg(),
             "plan_build: l_num/r_num out of range");
-  Group G;
-  G.n = group_n;
-  G.fermion = fermion != 0;
   std::vector<std::vector<int>> dim, sym, dim_ret, sym_ret;
   generate_dim_sym(G, L, l_num - 1, R, r_num, sector, dim, sym);
   c->n = get_dimension(dim, sym);
@@ -557,7 +555,8 @@ int dmrgx_build_maps(const int* lenv_meta, const int* renv_meta, int l_num, int 
                      int sector, int group_n, int fermion, int64_t* info, int* rmap,
                      int64_t rmap_cap, int* lmap, int64_t lmap_cap) {
   ARG_CHECK(info, "build_maps: null info");
-  ARG_CHECK(group_n >= 1 && group_n <= 4096, "build_maps: group_n out of range");
+  Group G;
+  ARG_CHECK(make_group(group_n, fermion, G), "build_maps: group_n out of range");
   QMeta L, R;
   std::string e = L.parse(lenv_meta);
   ARG_CHECK(e.empty(), "build_maps: lenv metadata: " + e);
@@ -565,9 +564,6 @@ int dmrgx_build_maps(const int* lenv_meta, const int* renv_meta, int l_num, int 
   ARG_CHECK(e.empty(), "build_maps: renv metadata: " + e);
   ARG_CHECK(l_num >= 2 && l_num <= L.nleg() && r_num >= 1 && r_num <= R.nleg(),
             "build_maps: l_num/r_num out of range");
-  Group G;
-  G.n = group_n;
-  G.fermion = fermion != 0;
   std::vector<std::vector<int>> dim, sym, dim_ret, sym_ret;
   std::vector<MapRow> rr, lr;
   generate_dim_sym(G, L, l_num - 1, R, r_num, sector, dim, sym);

@@ -62,6 +62,19 @@ static std::vector<std::vector<int>> label_tuples(const std::vector<int>& radix)
   return out;
 }
 
+bool make_group(int group_n, int fermion, Group& G) {
+  G = Group();
+  G.fermion = fermion != 0;
+  if (group_n == -8) {
+    G.n = 8;
+    G.z2cubed = true;
+    return true;
+  }
+  if (group_n < 1 || group_n > 4096) return false;
+  G.n = group_n;
+  return true;
+}
+
 void generate_dim_sym(const Group& G, const QMeta& lenv, int lnum, const QMeta& renv, int rnum,
                       int sector, std::vector<std::vector<int>>& dim,
                       std::vector<std::vector<int>>& sym) {

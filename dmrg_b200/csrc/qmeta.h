@@ -11,13 +11,26 @@
 namespace dmrgx {
 
 struct Group {
-  int n = 2;            // Z_N fusion rule, src/useful.cpp:30
-  bool fermion = false; // parity ff(a)=a%2 when true, 0 when false (bosonic models)
-  int ss(int a, int b) const { return (a + b + n) % n; }
-  int ff(int a) const { return fermion ? (a % 2) : 0; }
+  int n = 2;            // Z_N fusion rule, src/useful.cpp:30; 8 labels for Z2^3
+  bool z2cubed = false; // Z2 x Z2 x Z2 of the S4E build: labels 0..7 fuse by XOR,
+                        // a negative label -b stands for b (src/useful.cpp:4-20)
+  bool fermion = false; // parity ff when true, 0 when false (bosonic models)
+  int ss(int a, int b) const {
+    if (z2cubed) return a ^ (b < 0 ? -b : b);
+    return (a + b + n) % n;
+  }
+  // Z_N: a%2 (src/useful.cpp:32); Z2^3: odd for labels 2..5 (src/useful.cpp:22-26)
+  int ff(int a) const {
+    if (!fermion) return 0;
+    return z2cubed ? ((0x3C >> (a & 7)) & 1) : (a % 2);
+  }
   // 1-2*((ff(x)*ff(y))%2): the reference's sign form, src/qtensor.cpp:1084
   int sign(int x, int y) const { return 1 - 2 * ((ff(x) * ff(y)) % 2); }
 };
+
+// group_n >= 1: Z_N; group_n == -8 (DMRGX_GROUP_Z2CUBED): Z2^3.  Returns false
+// for any other value.
+bool make_group(int group_n, int fermion, Group& G);
 
 struct QMeta {
   std::vector<std::vector<int>> dims;  // dims[leg][sector]

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(PKG, "libdmrgx.so")
 F64, C128 = 0, 1
 PREC_FP64, PREC_BF16X3, PREC_TF32X3 = 0, 1, 2
 SCHED_GROUPED, SCHED_PER_BLOCK = 0, 1
+GROUP_Z2CUBED = -8  # group_n of the Z2 x Z2 x Z2 (S4E) fusion rule
 MEM_HOST, MEM_DEVICE = 0, 1
 
 # every entry point declared in include/dmrgx.h, with (restype, argtypes)

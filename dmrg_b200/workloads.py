@@ -136,6 +136,56 @@ def microbench(m: int = 1024, seed: int = 20261203, qmax: int = 4, width: float 
         l_num=3, r_num=2, sector=PSI_SECTOR, group_n=N, fermion=0, sizes=sizes)
 
 
+def random_z2cubed(seed: int = 3, complex_: bool = False, keep: float = 0.7, msize: int = 4):
+    """Random (L~, R~) pair under the Z2 x Z2 x Z2 fusion rule (labels 0..7 fusing
+    by XOR, group_n -8), with fermion directions, for l_num=3, r_num=2, sector 5.
+
+    Leg orders follow the reference's two-site environments (src/core.cpp:188-192):
+    L~ = [m_bra, d_bra, D, m_ket, d_ket], R~ = [d_bra, m_bra, D, d_ket, m_ket].
+    Bond legs: every label present with 1..msize states; physical legs: labels
+    {0, 3, 5, 6} with one state each; MPO leg: labels {0, 1, 2, 4} with 1..2 states.
+    A block exists where the XOR of its labels is 0, and is kept with probability
+    ``keep`` (missing blocks exercise the task-list matching).  Directions
+    L~ (+1, +1, 0, -1, -1), R~ (+1, +1, 0, -1, -1) make every parity sign of the
+    task list (src/qtensor.cpp:1078-1085) appear."""
+    rng = np.random.default_rng(seed)
+    N = 8
+    mdim = [int(v) for v in rng.integers(1, msize + 1, N)]
+    ddim = [1 if a in (0, 3, 5, 6) else 0 for a in range(N)]
+    Ddim = [int(rng.integers(1, 3)) if a in (0, 1, 2, 4) else 0 for a in range(N)]
+
+    def blocks(dims):
+        syms = []
+        for t in np.ndindex(*(N,) * len(dims)):
+            if any(dims[i][t[i]] == 0 for i in range(len(dims))):
+                continue
+            x = 0
+            for a in t:
+                x ^= a
+            if x == 0 and rng.random() < keep:
+                syms.append(tuple(int(a) for a in t))
+        return syms
+
+    def values(dims, syms):
+        out = []
+        for sy in syms:
+            k = int(np.prod([dims[i][sy[i]] for i in range(len(dims))]))
+            v = rng.standard_normal(k)
+            if complex_:
+                v = v + 1j * rng.standard_normal(k)
+            out.append(v)
+        return np.concatenate(out)
+
+    ldims = [mdim, ddim, Ddim, mdim, ddim]
+    rdims = [ddim, mdim, Ddim, ddim, mdim]
+    lsyms, rsyms = blocks(ldims), blocks(rdims)
+    dirs = [1, 1, 0, -1, -1]
+    return dict(
+        lenv=(_meta(ldims, dirs, lsyms), values(ldims, lsyms)),
+        renv=(_meta(rdims, dirs, rsyms), values(rdims, rsyms)),
+        l_num=3, r_num=2, sector=5, group_n=-8, fermion=1)
+
+
 def random_psi(n: int, seed: int = 7, complex_: bool = False):
     rng = np.random.default_rng(seed)
     x = rng.standard_normal(n)

@@ -61,6 +61,9 @@ enum {
 
 enum { DMRGX_MEM_HOST = 0, DMRGX_MEM_DEVICE = 1 };
 
+/* group_n value selecting the Z2 x Z2 x Z2 fusion rule (S4E, src/useful.cpp:4-27) */
+enum { DMRGX_GROUP_Z2CUBED = -8 };
+
 typedef struct dmrgx_ctx dmrgx_ctx;
 
 const char* dmrgx_last_error(void);
@@ -103,8 +106,11 @@ int dmrgx_set_schedule(dmrgx_ctx* ctx, int schedule);
  * generate_dim_sym(lenv, l_num-1, renv, r_num, sector) (src/useful.cpp:151-194),
  * rmap = renv.get_map(..., 'N','T', r_num, 0) and
  * lmap = lenv.get_map(..., 'N','T', l_num, 0, back=true) (src/qtensor.cpp:997-1119).
- * group_n: Z_N fusion rule (src/useful.cpp:30); fermion: apply the direction
- * signs (src/qtensor.cpp:1078-1085); 0 for bosonic models.
+ * group_n: N >= 1 for the Z_N fusion rule (src/useful.cpp:30), or
+ * DMRGX_GROUP_Z2CUBED for the Z2 x Z2 x Z2 rule of the reference's S4E build
+ * (src/useful.cpp:4-27: labels 0..7 fuse by XOR, parity odd for labels 2..5);
+ * fermion: apply the direction signs (src/qtensor.cpp:1078-1085); 0 for
+ * bosonic models.
  * Environment values (host pointers) are copied to the device. */
 int dmrgx_plan_build(dmrgx_ctx* ctx, const int* lenv_meta, const void* lenv_vals,
                      const int* renv_meta, const void* renv_vals, int l_num, int r_num,

@@ -23,7 +23,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REFDIR = os.path.join(HERE, "_ref")
-VARIANTS = ("kitaev", "xyz", "potts", "u1")
+VARIANTS = ("kitaev", "xyz", "potts", "u1", "s4e")
 MODEL = {"kitaev": 0, "xyz": 1, "potts": 2}
 
 _EIG_CB = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double),

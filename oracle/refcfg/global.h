@@ -7,7 +7,8 @@
  * reference sources can be built unmodified, where they lie, for each symmetry
  * configuration.  The switches come from the compiler command line:
  *   -DORACLE_SYMMETRY=<N>   Z_N fusion rule (2 Kitaev/XYZ, 3 Potts, 32 U(1) embedding)
- *   -DORACLE_FERMION        fermionic operators and signs (Kitaev only)
+ *   -DORACLE_FERMION        fermionic operators and signs (Kitaev, S4E)
+ *   -DORACLE_S4E            Z2 x Z2 x Z2 fusion rule and parity table (with SYMMETRY 8)
  * The numerical constants (TOL, NEV, ...) keep the values the reference ships
  * with, because the reference's ARPACK wrapper and printers read them.
  */
@@ -30,6 +31,9 @@
 #define SYMMETRY ORACLE_SYMMETRY
 #ifdef ORACLE_FERMION
 #define FERMION
+#endif
+#ifdef ORACLE_S4E
+#define S4E
 #endif
 
 #define TOL 1e-10

@@ -23,7 +23,10 @@ import numpy as np
 # ----------------------------------------------------------------------------- fusion rule
 @dataclass(frozen=True)
 class Group:
-    """Z_N fusion rule ``ss`` and parity ``ff`` (src/useful.cpp:28-39).
+    """Z_N fusion rule ``ss`` and parity ``ff`` (src/useful.cpp:28-39), or with
+    ``N = -8`` the Z2 x Z2 x Z2 rule of the reference's S4E build
+    (src/useful.cpp:4-27): labels 0..7 fuse by bitwise XOR (a negative label -b
+    stands for b) and the parity is odd exactly for labels 2, 3, 4, 5.
 
     ``fermion=False`` gives parity 0 everywhere: the bosonic models with the
     reference's direction signs compiled out (the reference applies them to every
@@ -31,11 +34,21 @@ class Group:
     N: int
     fermion: bool = False
 
+    @property
+    def order(self) -> int:
+        return 8 if self.N == -8 else self.N
+
     def ss(self, a: int, b: int) -> int:
+        if self.N == -8:
+            return a ^ (-b if b < 0 else b)
         return (a + b + self.N) % self.N
 
     def ff(self, a: int) -> int:
-        return (a % 2) if self.fermion else 0
+        if not self.fermion:
+            return 0
+        if self.N == -8:
+            return 1 if a in (2, 3, 4, 5) else 0
+        return a % 2
 
     def sign(self, x: int, y: int) -> int:
         # 1 - 2*((ff(x)*ff(y)) % 2), the reference's sign form
@@ -122,7 +135,7 @@ def generate_dim_sym(G: Group, ldims, lnum, rdims, rnum, sector):
     rmap = generate_map([len(d) for d in dim[lnum:]])
     sym = []
     if sector != -1:
-        for s in range(G.N):
+        for s in range(G.order):
             t = G.ss(sector, -s)
             for lt in lmap:
                 lsym = 0

@@ -40,6 +40,20 @@ def load_microbench_m64():
                 sector=sector, group_n=gn, l_num=3, r_num=2, fermion=0, complex=False)
 
 
+def load_z2cubed():
+    """Golden Z2 x Z2 x Z2 (S4E) fixtures, real then complex (tests/golden/make_golden.py)."""
+    z = np.load(os.path.join(GOLDEN, "z2cubed.npz"))
+    out = []
+    for p in ("r_", "c_"):
+        n, d_store, sector, gn, ferm, l_num, r_num = (int(v) for v in z[p + "info"])
+        out.append(dict(lenv=(z[p + "lenv_meta"], z[p + "lenv_vals"]),
+                        renv=(z[p + "renv_meta"], z[p + "renv_vals"]),
+                        rmap=z[p + "rmap"], lmap=z[p + "lmap"], x=z[p + "x"], ax=z[p + "ax"],
+                        n=n, d_store=d_store, sector=sector, group_n=gn, fermion=ferm,
+                        l_num=l_num, r_num=r_num, complex=p == "c_"))
+    return out
+
+
 MODELS = ("kitaev", "xyz", "potts")
 
 

@@ -17,6 +17,13 @@ oracle/_ref by oracle/Makefile) and records:
                       av(x) from the Z_32-embedded reference build.
   energies.json       final energies and truncation errors of small reference
                       runs, with the exact energies (BdG / ED) beside them.
+  z2cubed.npz         random environments under the Z2 x Z2 x Z2 fusion rule
+                      (workloads.random_z2cubed, real and complex), with the
+                      task lists and av(x) of the reference's S4E build
+                      (SYMMETRY 8, FERMION, src/useful.cpp:4-27).
+
+``python tests/golden/make_golden.py z2cubed`` regenerates only the named
+fixtures (steps, microbench, z2cubed); no argument regenerates all of them.
 
 The files are small (tens of KB) and committed; the GPU box never needs the
 reference tree.
@@ -56,7 +63,7 @@ def pick_steps(steps):
     return [out[k] for k in sorted(out)]
 
 
-def main():
+def make_steps():
     energies = {}
     for model, (variant, L, m, n, par, gn, ferm, exact_fn) in RUNS.items():
         R = refbind.Ref(variant)
@@ -86,8 +93,12 @@ def main():
             trunc_err_rows=res["singular"][:, [0, 1, -1]].tolist(),
             exact=e_exact)
         print(model, "steps", len(cap.steps), "E", res["energy"][-1, 2], "exact", e_exact)
+    with open(os.path.join(HERE, "energies.json"), "w") as fh:
+        json.dump(energies, fh, indent=1)
 
-    # microbench at m=64 through the Z_32 reference build
+
+def make_microbench():
+    """The U(1) microbench at m=64 through the Z_32 reference build."""
     w = workloads.microbench(64)
     R = refbind.Ref("u1")
     le = R.py_to_qt(0, *w["lenv"])
@@ -108,9 +119,41 @@ def main():
     R.lib.oref_pv_free(0, box)
     print("microbench m=64: n", n, "d_store", info[1], "tasks", info[2], info[3])
 
-    with open(os.path.join(HERE, "energies.json"), "w") as fh:
-        json.dump(energies, fh, indent=1)
+
+def make_z2cubed():
+    """Task lists and av(x) of the reference's S4E build on random Z2^3 inputs."""
+    R = refbind.Ref("s4e")
+    arrs = {}
+    for cplx in (0, 1):
+        w = workloads.random_z2cubed(seed=3, complex_=bool(cplx), msize=3)
+        le = R.py_to_qt(cplx, *w["lenv"])
+        re_ = R.py_to_qt(cplx, *w["renv"])
+        info = (refbind.C.c_int * 4)()
+        box = R.lib.oref_pv_build(cplx, le, re_, w["l_num"], w["r_num"], w["sector"], info)
+        n = info[0]
+        rmap, lmap = R.pv_maps(cplx, box, dict(n_rmap=info[2], n_lmap=info[3]))
+        x = workloads.random_psi(n, seed=11, complex_=bool(cplx))
+        ax = np.zeros_like(x)
+        R.lib.oref_av(cplx, box, x.ctypes.data, ax.ctypes.data)
+        R.lib.oref_pv_free(cplx, box)
+        p = "c_" if cplx else "r_"
+        arrs[p + "lenv_meta"], arrs[p + "lenv_vals"] = w["lenv"]
+        arrs[p + "renv_meta"], arrs[p + "renv_vals"] = w["renv"]
+        arrs[p + "rmap"], arrs[p + "lmap"], arrs[p + "x"], arrs[p + "ax"] = rmap, lmap, x, ax
+        arrs[p + "info"] = np.array([n, info[1], w["sector"], w["group_n"], w["fermion"],
+                                     w["l_num"], w["r_num"]], np.int64)
+        print("z2cubed", "complex" if cplx else "real", "n", n, "d_store", info[1],
+              "tasks", info[2], info[3])
+    np.savez_compressed(os.path.join(HERE, "z2cubed.npz"), **arrs)
+
+
+PARTS = {"steps": make_steps, "microbench": make_microbench, "z2cubed": make_z2cubed}
+
+
+def main(parts):
+    for name in parts or PARTS:
+        PARTS[name]()
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

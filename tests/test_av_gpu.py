@@ -5,7 +5,7 @@ max|y - y_ref| <= 1e-13 * max|y_ref| (1e-12 at the m=1024 size)."""
 import numpy as np
 import pytest
 
-from conftest import MODELS, load_microbench_m64, load_steps
+from conftest import MODELS, load_microbench_m64, load_steps, load_z2cubed
 from dmrg_b200 import native, workloads
 from oracle import restate
 
@@ -58,6 +58,24 @@ def test_av_microbench_m64():
     ctx.plan_build(mb["lenv"], mb["renv"], 3, 2, mb["sector"], mb["group_n"], 0)
     assert ctx.n == mb["n"]
     assert close(ctx.av(mb["x"]), mb["ax"])
+
+
+def test_av_z2cubed():
+    """Z2 x Z2 x Z2 (S4E) plans, real and complex, FP64 and split precision."""
+    for z in load_z2cubed():
+        dt = native.C128 if z["complex"] else native.F64
+        for prec, tol in ((native.PREC_FP64, TOL), (native.PREC_BF16X3, 5e-5),
+                          (native.PREC_TF32X3, 5e-5)):
+            ctx = native.Context(dt)
+            ctx.set_precision(prec)
+            ctx.plan_build(z["lenv"], z["renv"], z["l_num"], z["r_num"], z["sector"],
+                           native.GROUP_Z2CUBED, z["fermion"])
+            r, l = ctx.maps()
+            assert np.array_equal(r, z["rmap"]) and np.array_equal(l, z["lmap"])
+            y = ctx.av(z["x"])
+            assert close(y, z["ax"], tol), (z["complex"], prec,
+                                             np.abs(y - z["ax"]).max() / np.abs(z["ax"]).max())
+            ctx.close()
 
 
 def test_av_microbench_full_size_against_restatement():

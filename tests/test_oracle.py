@@ -5,7 +5,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, MODELS, load_microbench_m64, load_steps
+from conftest import GOLDEN, MODELS, load_microbench_m64, load_steps, load_z2cubed
 from oracle import exact, restate
 
 
@@ -45,6 +45,27 @@ def test_restatement_microbench_m64():
     assert np.array_equal(ctx.rmap, mb["rmap"]) and np.array_equal(ctx.lmap, mb["lmap"])
     y = restate.av(ctx, mb["x"])
     assert np.allclose(y, mb["ax"], rtol=0, atol=1e-13 * np.abs(mb["ax"]).max())
+
+
+def test_restatement_z2cubed():
+    """Z2 x Z2 x Z2 fusion and parity table (S4E build), real and complex."""
+    for z in load_z2cubed():
+        ctx = _ctx(z)
+        assert ctx.n == z["n"] and ctx.d_store == z["d_store"]
+        assert np.array_equal(ctx.rmap, z["rmap"]) and np.array_equal(ctx.lmap, z["lmap"])
+        assert set(np.unique(z["rmap"][:, 6])) == {-1, 1}  # both parity signs occur
+        y = restate.av(ctx, z["x"])
+        assert np.allclose(y, z["ax"], rtol=0, atol=1e-13 * np.abs(z["ax"]).max())
+
+
+def test_z2cubed_rule():
+    """XOR fusion with -b standing for b; parity odd exactly for labels 2..5."""
+    G = restate.Group(-8, True)
+    for a in range(8):
+        for b in range(8):
+            assert G.ss(a, b) == a ^ b and G.ss(a, -b) == a ^ b
+    assert [G.ff(a) for a in range(8)] == [0, 0, 1, 1, 1, 1, 0, 0]
+    assert restate.Group(-8, False).ff(3) == 0
 
 
 def test_exact_energies_pin_reference_runs():

@@ -7,7 +7,7 @@ import re
 import numpy as np
 import pytest
 
-from conftest import MODELS, ROOT, load_microbench_m64, load_steps
+from conftest import MODELS, ROOT, load_microbench_m64, load_steps, load_z2cubed
 from dmrg_b200 import native, workloads
 
 
@@ -43,6 +43,17 @@ def test_native_maps_microbench_m64():
                                           mb["group_n"], 0)
     assert (n, ds) == (mb["n"], mb["d_store"])
     assert np.array_equal(rmap, mb["rmap"]) and np.array_equal(lmap, mb["lmap"])
+
+
+def test_native_maps_z2cubed():
+    """group_n = GROUP_Z2CUBED: the reference's S4E fusion rule and parity table."""
+    for z in load_z2cubed():
+        n, ds, rmap, lmap = native.build_maps(z["lenv"][0], z["renv"][0], z["l_num"], z["r_num"],
+                                              z["sector"], native.GROUP_Z2CUBED, z["fermion"])
+        assert (n, ds) == (z["n"], z["d_store"])
+        assert np.array_equal(rmap, z["rmap"]) and np.array_equal(lmap, z["lmap"])
+    with pytest.raises(native.DmrgxError, match="group_n out of range"):
+        native.build_maps(z["lenv"][0], z["renv"][0], 3, 2, 5, -7, 1)
 
 
 def test_microbench_m1024_sizes():
