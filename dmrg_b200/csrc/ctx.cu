@@ -229,8 +229,6 @@ int upload_stage(Stage& st, cudaStream_t s) {
   return 0;
 }
 
-// Common tail of both plan entry points: sign-folded env images, stage
-// descriptors, device uploads, scratch.
 // Device image of an environment with the signs folded in, gathered from a
 // device tensor (the site-step path: environments never leave the GPU).
 int device_image(dmrgx_ctx* c, const QTensor& T, const EnvImage& im, double* dst) {
@@ -265,17 +263,77 @@ int device_image(dmrgx_ctx* c, const QTensor& T, const EnvImage& im, double* dst
   return 0;
 }
 
-int finalize_plan(dmrgx_ctx* c, const double* renv_vals, const std::vector<int64_t>& roff,
-                  const std::vector<int64_t>& rsize, const double* lenv_vals,
-                  const std::vector<int64_t>& loff, const std::vector<int64_t>& lsize,
-                  const QTensor* rdev = nullptr, const QTensor* ldev = nullptr) {
+// One (R~, L~) pair of the matvec with its own task lists, environment blocks
+// and intermediate: the main pair, and on a periodic chain the edge pair
+// (src/core.cpp:27-30).  Values come from the host (rvals/lvals, blocks packed
+// at roff/loff) or from device tensors (rdev/ldev).
+struct PairSrc {
+  std::vector<MapRow> rmap, lmap;
+  const double* rvals = nullptr;
+  const double* lvals = nullptr;
+  std::vector<int64_t> roff, rsize, loff, lsize;
+  const QTensor* rdev = nullptr;
+  const QTensor* ldev = nullptr;
+  int64_t store = 0;
+};
+
+// Common tail of the plan entry points: sign-folded env images, stage
+// descriptors, device uploads, scratch.  The pairs are merged into one task
+// list per stage: each pair's stage-1 rows write their own part of the
+// intermediate, and its stage-2 rows are further K-segments of the psi blocks,
+// which is the reference's accumulation of the edge pair into out (lemap built
+// with beta = 1, src/core.cpp:247).
+int finalize_plan(dmrgx_ctx* c, const std::vector<PairSrc>& pairs) {
   const int f = c->f();
   c->has_plan = false;
   c->flops = 0;
-  EnvImage ri = make_image(renv_vals, roff, rsize, c->rmap, f);
-  EnvImage li = make_image(lenv_vals, loff, lsize, c->lmap, f);
-  std::string e = build_stage(c->rmap, rsize, ri, f, c->n, c->d_store, c->st1, c->flops);
-  if (e.empty()) e = build_stage(c->lmap, lsize, li, f, c->d_store, c->n, c->st2, c->flops);
+  std::vector<MapRow> R, Lr;
+  std::vector<int64_t> rsz, lsz;
+  EnvImage RI, LI;
+  std::vector<EnvImage> ris, lis;
+  std::vector<int64_t> rimg, limg;  // image offset (doubles) of every pair
+  int64_t soff = 0;
+  int rb = 0, lb = 0;
+  for (const PairSrc& p : pairs) {
+    ris.push_back(make_image(p.rvals, p.roff, p.rsize, p.rmap, f));
+    lis.push_back(make_image(p.lvals, p.loff, p.lsize, p.lmap, f));
+    const EnvImage& ri = ris.back();
+    const EnvImage& li = lis.back();
+    for (MapRow r : p.rmap) {
+      r.blk += rb;
+      r.out_beg += soff;
+      R.push_back(r);
+    }
+    for (MapRow r : p.lmap) {
+      r.blk += lb;
+      r.in_beg += soff;
+      Lr.push_back(r);
+    }
+    rsz.insert(rsz.end(), p.rsize.begin(), p.rsize.end());
+    lsz.insert(lsz.end(), p.lsize.begin(), p.lsize.end());
+    auto merge = [](EnvImage& all, const EnvImage& one, std::vector<int64_t>& at) {
+      at.push_back(all.len);
+      all.vals.insert(all.vals.end(), one.vals.begin(), one.vals.end());
+      for (int64_t x : one.plus) all.plus.push_back(x < 0 ? -1 : x + all.len);
+      for (int64_t x : one.minus) all.minus.push_back(x < 0 ? -1 : x + all.len);
+      all.len += one.len;
+    };
+    merge(RI, ri, rimg);
+    merge(LI, li, limg);
+    soff += p.store;
+    rb += (int)p.rsize.size();
+    lb += (int)p.lsize.size();
+  }
+  c->rmap = R;
+  c->lmap = Lr;
+  c->n_rmap_main = pairs.empty() ? 0 : (int64_t)pairs[0].rmap.size();
+  c->n_lmap_main = pairs.empty() ? 0 : (int64_t)pairs[0].lmap.size();
+  c->d_store_main = pairs.empty() ? 0 : pairs[0].store;
+  c->r_blocks_main = pairs.empty() ? 0 : (int)pairs[0].rsize.size();
+  c->l_blocks_main = pairs.empty() ? 0 : (int)pairs[0].lsize.size();
+  c->d_store = soff;
+  std::string e = build_stage(c->rmap, rsz, RI, f, c->n, c->d_store, c->st1, c->flops);
+  if (e.empty()) e = build_stage(c->lmap, lsz, LI, f, c->d_store, c->n, c->st2, c->flops);
   if (!e.empty()) {
     set_error(e);
     return DMRGX_E_ARG;
@@ -283,30 +341,35 @@ int finalize_plan(dmrgx_ctx* c, const double* renv_vals, const std::vector<int64
   std::map<int64_t, int> so;
   for (auto& r : c->rmap) so[r.out_beg] = 1;
   c->n_store_blocks = (int)so.size();
-  c->st1.a_len = ri.len;
-  c->st2.a_len = li.len;
+  c->st1.a_len = RI.len;
+  c->st2.a_len = LI.len;
   CUDA_TRY(cudaSetDevice(c->device));
-  CUDA_TRY(c->renv.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, ri.len)));
-  CUDA_TRY(c->lenv.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, li.len)));
-  if (rdev) {
-    int rc0 = device_image(c, *rdev, ri, (double*)c->renv.p);
-    if (!rc0) rc0 = device_image(c, *ldev, li, (double*)c->lenv.p);
-    if (rc0) return rc0;
+  CUDA_TRY(c->renv.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, RI.len)));
+  CUDA_TRY(c->lenv.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, LI.len)));
+  for (size_t i = 0; i < pairs.size(); i++) {
+    if (pairs[i].rdev) {
+      int rc0 = device_image(c, *pairs[i].rdev, ris[i], (double*)c->renv.p + rimg[i]);
+      if (rc0) return rc0;
+    }
+    if (pairs[i].ldev) {
+      int rc0 = device_image(c, *pairs[i].ldev, lis[i], (double*)c->lenv.p + limg[i]);
+      if (rc0) return rc0;
+    }
   }
   CUDA_TRY(c->store.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, c->d_store * f)));
   CUDA_TRY(c->din.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, c->n * f)));
   CUDA_TRY(c->dout.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, c->n * f)));
-  if (!ri.vals.empty())
-    CUDA_TRY(cudaMemcpyAsync(c->renv.p, ri.vals.data(), sizeof(double) * ri.vals.size(),
+  if (!RI.vals.empty())
+    CUDA_TRY(cudaMemcpyAsync(c->renv.p, RI.vals.data(), sizeof(double) * RI.vals.size(),
                              cudaMemcpyHostToDevice, c->stream));
-  if (!li.vals.empty())
-    CUDA_TRY(cudaMemcpyAsync(c->lenv.p, li.vals.data(), sizeof(double) * li.vals.size(),
+  if (!LI.vals.empty())
+    CUDA_TRY(cudaMemcpyAsync(c->lenv.p, LI.vals.data(), sizeof(double) * LI.vals.size(),
                              cudaMemcpyHostToDevice, c->stream));
   int rc = upload_stage(c->st1, c->stream);
   if (rc) return rc;
   rc = upload_stage(c->st2, c->stream);
   if (rc) return rc;
-  // ri/li are host temporaries: wait for the uploads before they go away
+  // RI/LI are host temporaries: wait for the uploads before they go away
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->sp.free_device();
   c->sp = SplitPlan();
@@ -372,35 +435,79 @@ int matvec_fp64(dmrgx_ctx* c, const double* in, double* out) {
   return run_matvec_fp64(c, in, out);
 }
 
+// The step functions' bookkeeping (src/core.cpp:236-247): psi layout from
+// generate_dim_sym, rmap / lmap of the main pair and, on a periodic chain,
+// remap / lemap of the edge pair against the same psi layout (its own
+// intermediate; lemap with beta = 1, so the edge pair accumulates into out).
+std::string step_maps(const Group& G, const QMeta& L, const QMeta& R, const QMeta* Le,
+                      const QMeta* Re, int l_num, int r_num, int sector,
+                      std::vector<std::vector<int>>& dim, std::vector<std::vector<int>>& sym,
+                      std::vector<MapRow>& rm, std::vector<MapRow>& lm, int64_t& d_store,
+                      std::vector<MapRow>& erm, std::vector<MapRow>& elm, int64_t& e_store) {
+  std::vector<std::vector<int>> dim_ret, sym_ret;
+  generate_dim_sym(G, L, l_num - 1, R, r_num, sector, dim, sym);
+  std::string e = get_map(G, R, dim, sym, r_num, 0, false, dim_ret, sym_ret, rm);
+  if (!e.empty()) return "rmap: " + e;
+  d_store = get_dimension(dim_ret, sym_ret);
+  e = get_map(G, L, dim_ret, sym_ret, l_num, 0, true, dim, sym, lm);
+  if (!e.empty()) return "lmap: " + e;
+  erm.clear();
+  elm.clear();
+  e_store = 0;
+  if (Le && Re) {
+    e = get_map(G, *Re, dim, sym, r_num, 0, false, dim_ret, sym_ret, erm);
+    if (!e.empty()) return "remap: " + e;
+    e_store = get_dimension(dim_ret, sym_ret);
+    e = get_map(G, *Le, dim_ret, sym_ret, l_num, 1, true, dim, sym, elm);
+    if (!e.empty()) return "lemap: " + e;
+  }
+  return "";
+}
+
 // Plan from device tensors (the site step): same bookkeeping as
-// dmrgx_plan_build, environment images gathered on the device.
+// dmrgx_plan_build, environment images gathered on the device.  Le / Re: the
+// edge pair of a periodic chain, or null.
 int plan_build_device(dmrgx_ctx* c, const QTensor& L, const QTensor& R, int l_num, int r_num,
-                      int sector, const Group& G) {
-  if (L.f != c->f() || R.f != c->f()) {
+                      int sector, const Group& G, const QTensor* Le, const QTensor* Re) {
+  if (L.f != c->f() || R.f != c->f() || (Le && Le->f != c->f()) || (Re && Re->f != c->f())) {
     set_error("plan: tensor element type differs from the context's");
     return DMRGX_E_ARG;
   }
-  std::vector<std::vector<int>> dim, sym, dim_ret, sym_ret;
-  generate_dim_sym(G, L.m, l_num - 1, R.m, r_num, sector, dim, sym);
-  c->n = get_dimension(dim, sym);
-  std::string e = get_map(G, R.m, dim, sym, r_num, 0, false, dim_ret, sym_ret, c->rmap);
-  if (e.empty()) {
-    c->d_store = get_dimension(dim_ret, sym_ret);
-    e = get_map(G, L.m, dim_ret, sym_ret, l_num, 0, true, dim, sym, c->lmap);
-  }
+  const bool pbc = Le && Re;
+  std::vector<PairSrc> pairs(pbc ? 2 : 1);
+  std::vector<std::vector<int>> dim, sym;
+  std::vector<MapRow> erm, elm;
+  int64_t es = 0;
+  std::string e = step_maps(G, L.m, R.m, pbc ? &Le->m : nullptr, pbc ? &Re->m : nullptr, l_num,
+                            r_num, sector, dim, sym, pairs[0].rmap, pairs[0].lmap,
+                            pairs[0].store, erm, elm, es);
   if (!e.empty()) {
     set_error("plan: " + e);
     return DMRGX_E_ARG;
   }
+  if (pbc) {
+    pairs[1].rmap = erm;
+    pairs[1].lmap = elm;
+    pairs[1].store = es;
+  }
+  c->n = get_dimension(dim, sym);
   c->psi_dim = dim;
   c->psi_sym = sym;
-  std::vector<int64_t> rsize(R.m.syms.size()), lsize(L.m.syms.size());
-  for (size_t b = 0; b < rsize.size(); b++) rsize[b] = R.bsize((int)b);
-  for (size_t b = 0; b < lsize.size(); b++) lsize[b] = L.bsize((int)b);
-  return finalize_plan(c, nullptr, R.off, rsize, nullptr, L.off, lsize, &R, &L);
+  auto dev = [](PairSrc& p, const QTensor& Ro, const QTensor& Lo) {
+    p.rdev = &Ro;
+    p.ldev = &Lo;
+    p.roff = Ro.off;
+    p.loff = Lo.off;
+    p.rsize.resize(Ro.m.syms.size());
+    p.lsize.resize(Lo.m.syms.size());
+    for (size_t b = 0; b < p.rsize.size(); b++) p.rsize[b] = Ro.bsize((int)b);
+    for (size_t b = 0; b < p.lsize.size(); b++) p.lsize[b] = Lo.bsize((int)b);
+  };
+  dev(pairs[0], R, L);
+  if (pbc) dev(pairs[1], *Re, *Le);
+  return finalize_plan(c, pairs);
 }
 
-// the context's matvec (fp64=false) or its FP64 form regardless of precision
 int run_matvec_any(dmrgx_ctx* c, const double* in, double* out, bool fp64) {
   if (fp64 && c->per_block) return run_matvec_plain(c, in, out);
   return fp64 ? run_matvec_fp64(c, in, out) : run_matvec(c, in, out);
@@ -519,118 +626,269 @@ int dmrgx_set_schedule(dmrgx_ctx* c, int schedule) {
   return 0;
 }
 
+namespace {
+void put_rows(const MapRow* rows, int64_t n, int* o) {
+  for (int64_t i = 0; i < n; i++) {
+    const MapRow& r = rows[i];
+    int* p = o + 7 * i;
+    p[0] = r.blk;
+    p[1] = (int)r.in_beg;
+    p[2] = (int)r.out_beg;
+    p[3] = r.rows;
+    p[4] = r.cols;
+    p[5] = r.beta;
+    p[6] = r.alpha;
+  }
+}
+
+void rows_of(const int* m, int nr, std::vector<MapRow>& out) {
+  out.resize(nr);
+  for (int i = 0; i < nr; i++) {
+    const int* r = m + 7 * i;
+    out[i] = MapRow{r[0], r[1], r[2], r[3], r[4], r[5], r[6]};
+  }
+}
+
+// host environment values + metadata -> one pair's block table
+void host_pair(PairSrc& p, const QMeta& Ro, const void* rv, const QMeta& Lo, const void* lv) {
+  p.rvals = (const double*)rv;
+  p.lvals = (const double*)lv;
+  p.roff = Ro.block_offsets();
+  p.loff = Lo.block_offsets();
+  p.rsize.resize(Ro.syms.size());
+  p.lsize.resize(Lo.syms.size());
+  for (size_t b = 0; b < p.rsize.size(); b++) p.rsize[b] = Ro.block_size((int)b);
+  for (size_t b = 0; b < p.lsize.size(); b++) p.lsize[b] = Lo.block_size((int)b);
+}
+
+// block sizes as the caller gives them -> packed offsets; false on a negative size
+bool sized_pair(const int64_t* sz, int nb, std::vector<int64_t>& size, std::vector<int64_t>& off) {
+  size.assign(sz, sz + nb);
+  off.assign(nb + 1, 0);
+  for (int b = 0; b < nb; b++) {
+    if (size[b] < 0) return false;
+    off[b + 1] = off[b] + size[b];
+  }
+  return true;
+}
+
+int plan_build_common(dmrgx_ctx* c, const int* lenv_meta, const void* lenv_vals,
+                      const int* renv_meta, const void* renv_vals, const int* ledge_meta,
+                      const void* ledge_vals, const int* redge_meta, const void* redge_vals,
+                      int l_num, int r_num, int sector, int group_n, int fermion,
+                      const char* who) {
+  const std::string w = who;
+  ARG_CHECK(c, "null context");
+  ARG_CHECK(lenv_vals && renv_vals, w + ": null environment values");
+  const bool pbc = ledge_meta || redge_meta;
+  ARG_CHECK(!pbc || (ledge_meta && redge_meta && ledge_vals && redge_vals),
+            w + ": null edge metadata or values");
+  Group G;
+  ARG_CHECK(make_group(group_n, fermion, G), w + ": group_n out of range");
+  QMeta L, R, Le, Re;
+  std::string e = L.parse(lenv_meta);
+  ARG_CHECK(e.empty(), w + ": lenv metadata: " + e);
+  e = R.parse(renv_meta);
+  ARG_CHECK(e.empty(), w + ": renv metadata: " + e);
+  if (pbc) {
+    e = Le.parse(ledge_meta);
+    ARG_CHECK(e.empty(), w + ": ledge metadata: " + e);
+    e = Re.parse(redge_meta);
+    ARG_CHECK(e.empty(), w + ": redge metadata: " + e);
+    ARG_CHECK(Le.nleg() >= l_num && Re.nleg() >= r_num, w + ": edge legs out of range");
+  }
+  ARG_CHECK(l_num >= 2 && l_num <= L.nleg() && r_num >= 1 && r_num <= R.nleg(),
+            w + ": l_num/r_num out of range");
+  std::vector<PairSrc> pairs(pbc ? 2 : 1);
+  std::vector<std::vector<int>> dim, sym;
+  std::vector<MapRow> erm, elm;
+  int64_t es = 0;
+  e = step_maps(G, L, R, pbc ? &Le : nullptr, pbc ? &Re : nullptr, l_num, r_num, sector, dim,
+                sym, pairs[0].rmap, pairs[0].lmap, pairs[0].store, erm, elm, es);
+  ARG_CHECK(e.empty(), w + ": " + e);
+  c->n = get_dimension(dim, sym);
+  c->psi_dim = dim;
+  c->psi_sym = sym;
+  host_pair(pairs[0], R, renv_vals, L, lenv_vals);
+  if (pbc) {
+    pairs[1].rmap = erm;
+    pairs[1].lmap = elm;
+    pairs[1].store = es;
+    host_pair(pairs[1], Re, redge_vals, Le, ledge_vals);
+  }
+  return finalize_plan(c, pairs);
+}
+
+int build_maps_common(const int* lenv_meta, const int* renv_meta, const int* ledge_meta,
+                      const int* redge_meta, int l_num, int r_num, int sector, int group_n,
+                      int fermion, int64_t* info, int* rmap, int64_t rmap_cap, int* lmap,
+                      int64_t lmap_cap, int* remap, int64_t remap_cap, int* lemap,
+                      int64_t lemap_cap, const char* who) {
+  const std::string w = who;
+  ARG_CHECK(info, w + ": null info");
+  const bool pbc = ledge_meta || redge_meta;
+  ARG_CHECK(!pbc || (ledge_meta && redge_meta), w + ": null edge metadata");
+  Group G;
+  ARG_CHECK(make_group(group_n, fermion, G), w + ": group_n out of range");
+  QMeta L, R, Le, Re;
+  std::string e = L.parse(lenv_meta);
+  ARG_CHECK(e.empty(), w + ": lenv metadata: " + e);
+  e = R.parse(renv_meta);
+  ARG_CHECK(e.empty(), w + ": renv metadata: " + e);
+  if (pbc) {
+    e = Le.parse(ledge_meta);
+    ARG_CHECK(e.empty(), w + ": ledge metadata: " + e);
+    e = Re.parse(redge_meta);
+    ARG_CHECK(e.empty(), w + ": redge metadata: " + e);
+    ARG_CHECK(Le.nleg() >= l_num && Re.nleg() >= r_num, w + ": edge legs out of range");
+  }
+  ARG_CHECK(l_num >= 2 && l_num <= L.nleg() && r_num >= 1 && r_num <= R.nleg(),
+            w + ": l_num/r_num out of range");
+  std::vector<std::vector<int>> dim, sym;
+  std::vector<MapRow> rr, lr, er, el;
+  int64_t ds = 0, es = 0;
+  e = step_maps(G, L, R, pbc ? &Le : nullptr, pbc ? &Re : nullptr, l_num, r_num, sector, dim,
+                sym, rr, lr, ds, er, el, es);
+  ARG_CHECK(e.empty(), w + ": " + e);
+  info[0] = get_dimension(dim, sym);
+  info[1] = ds;
+  info[2] = (int64_t)rr.size();
+  info[3] = (int64_t)lr.size();
+  if (pbc) {
+    info[4] = es;
+    info[5] = (int64_t)er.size();
+    info[6] = (int64_t)el.size();
+  }
+  if (!rmap || !lmap) return 0;
+  ARG_CHECK(rmap_cap >= (int64_t)rr.size() && lmap_cap >= (int64_t)lr.size(),
+            w + ": map buffer too small");
+  put_rows(rr.data(), (int64_t)rr.size(), rmap);
+  put_rows(lr.data(), (int64_t)lr.size(), lmap);
+  if (pbc && remap && lemap) {
+    ARG_CHECK(remap_cap >= (int64_t)er.size() && lemap_cap >= (int64_t)el.size(),
+              w + ": map buffer too small");
+    put_rows(er.data(), (int64_t)er.size(), remap);
+    put_rows(el.data(), (int64_t)el.size(), lemap);
+  }
+  return 0;
+}
+
+int from_maps_common(dmrgx_ctx* c, int64_t n, int64_t d_store, const int* rmap, int n_rmap,
+                     const void* renv_vals, const int64_t* renv_sizes, int n_renv_blocks,
+                     const int* lmap, int n_lmap, const void* lenv_vals,
+                     const int64_t* lenv_sizes, int n_lenv_blocks, bool pbc, int64_t e_store,
+                     const int* remap, int n_remap, const void* redge_vals,
+                     const int64_t* redge_sizes, int n_redge_blocks, const int* lemap,
+                     int n_lemap, const void* ledge_vals, const int64_t* ledge_sizes,
+                     int n_ledge_blocks, const char* who) {
+  const std::string w = who;
+  ARG_CHECK(c, "null context");
+  ARG_CHECK(n >= 0 && d_store >= 0 && e_store >= 0, w + ": negative length");
+  ARG_CHECK((n_rmap == 0 || rmap) && (n_lmap == 0 || lmap), w + ": null map");
+  ARG_CHECK(n_rmap >= 0 && n_lmap >= 0 && n_renv_blocks >= 0 && n_lenv_blocks >= 0,
+            w + ": negative count");
+  ARG_CHECK(renv_vals && lenv_vals && renv_sizes && lenv_sizes,
+            w + ": null environment arrays");
+  std::vector<PairSrc> pairs(pbc ? 2 : 1);
+  rows_of(rmap, n_rmap, pairs[0].rmap);
+  rows_of(lmap, n_lmap, pairs[0].lmap);
+  pairs[0].store = d_store;
+  pairs[0].rvals = (const double*)renv_vals;
+  pairs[0].lvals = (const double*)lenv_vals;
+  ARG_CHECK(sized_pair(renv_sizes, n_renv_blocks, pairs[0].rsize, pairs[0].roff) &&
+                sized_pair(lenv_sizes, n_lenv_blocks, pairs[0].lsize, pairs[0].loff),
+            w + ": negative block size");
+  if (pbc) {
+    ARG_CHECK((n_remap == 0 || remap) && (n_lemap == 0 || lemap), w + ": null edge map");
+    ARG_CHECK(n_remap >= 0 && n_lemap >= 0 && n_redge_blocks >= 0 && n_ledge_blocks >= 0,
+              w + ": negative count");
+    ARG_CHECK(redge_vals && ledge_vals && redge_sizes && ledge_sizes,
+              w + ": null edge arrays");
+    rows_of(remap, n_remap, pairs[1].rmap);
+    rows_of(lemap, n_lemap, pairs[1].lmap);
+    pairs[1].store = e_store;
+    pairs[1].rvals = (const double*)redge_vals;
+    pairs[1].lvals = (const double*)ledge_vals;
+    ARG_CHECK(sized_pair(redge_sizes, n_redge_blocks, pairs[1].rsize, pairs[1].roff) &&
+                  sized_pair(ledge_sizes, n_ledge_blocks, pairs[1].lsize, pairs[1].loff),
+              w + ": negative block size");
+  }
+  c->n = n;
+  c->psi_dim.clear();
+  c->psi_sym.clear();
+  return finalize_plan(c, pairs);
+}
+}  // namespace
+
+int dmrgx_set_boundary(dmrgx_ctx* c, int boundary) {
+  ARG_CHECK(c, "null context");
+  ARG_CHECK(boundary == DMRGX_BOUNDARY_OPEN || boundary == DMRGX_BOUNDARY_PERIODIC,
+            "set_boundary: unknown boundary");
+  c->boundary = boundary;
+  return 0;
+}
+
 int dmrgx_plan_build(dmrgx_ctx* c, const int* lenv_meta, const void* lenv_vals,
                      const int* renv_meta, const void* renv_vals, int l_num, int r_num,
                      int sector, int group_n, int fermion) {
-  ARG_CHECK(c, "null context");
-  ARG_CHECK(lenv_vals && renv_vals, "plan_build: null environment values");
-  Group G;
-  ARG_CHECK(make_group(group_n, fermion, G), "plan_build: group_n out of range");
-  QMeta L, R;
-  std::string e = L.parse(lenv_meta);
-  ARG_CHECK(e.empty(), "plan_build: lenv metadata: " + e);
-  e = R.parse(renv_meta);
-  ARG_CHECK(e.empty(), "plan_build: renv metadata: " + e);
-  ARG_CHECK(l_num >= 2 && l_num <= L.nleg() && r_num >= 1 && r_num <= R.nleg(),
-            "plan_build: l_num/r_num out of range");
-  std::vector<std::vector<int>> dim, sym, dim_ret, sym_ret;
-  generate_dim_sym(G, L, l_num - 1, R, r_num, sector, dim, sym);
-  c->n = get_dimension(dim, sym);
-  e = get_map(G, R, dim, sym, r_num, 0, false, dim_ret, sym_ret, c->rmap);
-  ARG_CHECK(e.empty(), "plan_build: rmap: " + e);
-  c->d_store = get_dimension(dim_ret, sym_ret);
-  e = get_map(G, L, dim_ret, sym_ret, l_num, 0, true, dim, sym, c->lmap);
-  ARG_CHECK(e.empty(), "plan_build: lmap: " + e);
-  c->psi_dim = dim;
-  c->psi_sym = sym;
-  auto roff = R.block_offsets(), loff = L.block_offsets();
-  std::vector<int64_t> rsize(R.syms.size()), lsize(L.syms.size());
-  for (size_t b = 0; b < rsize.size(); b++) rsize[b] = R.block_size((int)b);
-  for (size_t b = 0; b < lsize.size(); b++) lsize[b] = L.block_size((int)b);
-  return finalize_plan(c, (const double*)renv_vals, roff, rsize, (const double*)lenv_vals, loff,
-                       lsize);
+  return plan_build_common(c, lenv_meta, lenv_vals, renv_meta, renv_vals, nullptr, nullptr,
+                           nullptr, nullptr, l_num, r_num, sector, group_n, fermion,
+                           "plan_build");
+}
+
+int dmrgx_plan_build_pbc(dmrgx_ctx* c, const int* lenv_meta, const void* lenv_vals,
+                         const int* renv_meta, const void* renv_vals, const int* ledge_meta,
+                         const void* ledge_vals, const int* redge_meta, const void* redge_vals,
+                         int l_num, int r_num, int sector, int group_n, int fermion) {
+  ARG_CHECK(ledge_meta && redge_meta, "plan_build_pbc: null edge metadata");
+  return plan_build_common(c, lenv_meta, lenv_vals, renv_meta, renv_vals, ledge_meta,
+                           ledge_vals, redge_meta, redge_vals, l_num, r_num, sector, group_n,
+                           fermion, "plan_build_pbc");
 }
 
 int dmrgx_build_maps(const int* lenv_meta, const int* renv_meta, int l_num, int r_num,
                      int sector, int group_n, int fermion, int64_t* info, int* rmap,
                      int64_t rmap_cap, int* lmap, int64_t lmap_cap) {
-  ARG_CHECK(info, "build_maps: null info");
-  Group G;
-  ARG_CHECK(make_group(group_n, fermion, G), "build_maps: group_n out of range");
-  QMeta L, R;
-  std::string e = L.parse(lenv_meta);
-  ARG_CHECK(e.empty(), "build_maps: lenv metadata: " + e);
-  e = R.parse(renv_meta);
-  ARG_CHECK(e.empty(), "build_maps: renv metadata: " + e);
-  ARG_CHECK(l_num >= 2 && l_num <= L.nleg() && r_num >= 1 && r_num <= R.nleg(),
-            "build_maps: l_num/r_num out of range");
-  std::vector<std::vector<int>> dim, sym, dim_ret, sym_ret;
-  std::vector<MapRow> rr, lr;
-  generate_dim_sym(G, L, l_num - 1, R, r_num, sector, dim, sym);
-  e = get_map(G, R, dim, sym, r_num, 0, false, dim_ret, sym_ret, rr);
-  ARG_CHECK(e.empty(), "build_maps: rmap: " + e);
-  e = get_map(G, L, dim_ret, sym_ret, l_num, 0, true, dim, sym, lr);
-  ARG_CHECK(e.empty(), "build_maps: lmap: " + e);
-  info[0] = get_dimension(dim, sym);
-  info[1] = get_dimension(dim_ret, sym_ret);
-  info[2] = (int64_t)rr.size();
-  info[3] = (int64_t)lr.size();
-  if (!rmap || !lmap) return 0;
-  ARG_CHECK(rmap_cap >= (int64_t)rr.size() && lmap_cap >= (int64_t)lr.size(),
-            "build_maps: map buffer too small");
-  auto put = [](const std::vector<MapRow>& rows, int* o) {
-    for (size_t i = 0; i < rows.size(); i++) {
-      const MapRow& r = rows[i];
-      int* p = o + 7 * i;
-      p[0] = r.blk;
-      p[1] = (int)r.in_beg;
-      p[2] = (int)r.out_beg;
-      p[3] = r.rows;
-      p[4] = r.cols;
-      p[5] = r.beta;
-      p[6] = r.alpha;
-    }
-  };
-  put(rr, rmap);
-  put(lr, lmap);
-  return 0;
+  return build_maps_common(lenv_meta, renv_meta, nullptr, nullptr, l_num, r_num, sector,
+                           group_n, fermion, info, rmap, rmap_cap, lmap, lmap_cap, nullptr, 0,
+                           nullptr, 0, "build_maps");
+}
+
+int dmrgx_build_maps_pbc(const int* lenv_meta, const int* renv_meta, const int* ledge_meta,
+                         const int* redge_meta, int l_num, int r_num, int sector, int group_n,
+                         int fermion, int64_t* info, int* rmap, int64_t rmap_cap, int* lmap,
+                         int64_t lmap_cap, int* remap, int64_t remap_cap, int* lemap,
+                         int64_t lemap_cap) {
+  ARG_CHECK(ledge_meta && redge_meta, "build_maps_pbc: null edge metadata");
+  return build_maps_common(lenv_meta, renv_meta, ledge_meta, redge_meta, l_num, r_num, sector,
+                           group_n, fermion, info, rmap, rmap_cap, lmap, lmap_cap, remap,
+                           remap_cap, lemap, lemap_cap, "build_maps_pbc");
 }
 
 int dmrgx_plan_from_maps(dmrgx_ctx* c, int64_t n, int64_t d_store, const int* rmap, int n_rmap,
                          const void* renv_vals, const int64_t* renv_sizes, int n_renv_blocks,
                          const int* lmap, int n_lmap, const void* lenv_vals,
                          const int64_t* lenv_sizes, int n_lenv_blocks) {
-  ARG_CHECK(c, "null context");
-  ARG_CHECK(n >= 0 && d_store >= 0, "plan_from_maps: negative length");
-  ARG_CHECK((n_rmap == 0 || rmap) && (n_lmap == 0 || lmap), "plan_from_maps: null map");
-  ARG_CHECK(renv_vals && lenv_vals && renv_sizes && lenv_sizes,
-            "plan_from_maps: null environment arrays");
-  c->n = n;
-  c->d_store = d_store;
-  auto rows_of = [](const int* m, int nr, std::vector<MapRow>& out) {
-    out.resize(nr);
-    for (int i = 0; i < nr; i++) {
-      const int* r = m + 7 * i;
-      out[i] = MapRow{r[0], r[1], r[2], r[3], r[4], r[5], r[6]};
-    }
-  };
-  rows_of(rmap, n_rmap, c->rmap);
-  rows_of(lmap, n_lmap, c->lmap);
-  c->psi_dim.clear();
-  c->psi_sym.clear();
-  std::vector<int64_t> rsize(renv_sizes, renv_sizes + n_renv_blocks);
-  std::vector<int64_t> lsize(lenv_sizes, lenv_sizes + n_lenv_blocks);
-  std::vector<int64_t> roff(n_renv_blocks + 1, 0), loff(n_lenv_blocks + 1, 0);
-  for (int b = 0; b < n_renv_blocks; b++) {
-    ARG_CHECK(rsize[b] >= 0, "plan_from_maps: negative block size");
-    roff[b + 1] = roff[b] + rsize[b];
-  }
-  for (int b = 0; b < n_lenv_blocks; b++) {
-    ARG_CHECK(lsize[b] >= 0, "plan_from_maps: negative block size");
-    loff[b + 1] = loff[b] + lsize[b];
-  }
-  return finalize_plan(c, (const double*)renv_vals, roff, rsize, (const double*)lenv_vals, loff,
-                       lsize);
+  return from_maps_common(c, n, d_store, rmap, n_rmap, renv_vals, renv_sizes, n_renv_blocks,
+                          lmap, n_lmap, lenv_vals, lenv_sizes, n_lenv_blocks, false, 0, nullptr,
+                          0, nullptr, nullptr, 0, nullptr, 0, nullptr, nullptr, 0,
+                          "plan_from_maps");
+}
+
+int dmrgx_plan_from_maps_pbc(dmrgx_ctx* c, int64_t n, int64_t d_store, const int* rmap,
+                             int n_rmap, const void* renv_vals, const int64_t* renv_sizes,
+                             int n_renv_blocks, const int* lmap, int n_lmap,
+                             const void* lenv_vals, const int64_t* lenv_sizes, int n_lenv_blocks,
+                             int64_t e_store, const int* remap, int n_remap,
+                             const void* redge_vals, const int64_t* redge_sizes,
+                             int n_redge_blocks, const int* lemap, int n_lemap,
+                             const void* ledge_vals, const int64_t* ledge_sizes,
+                             int n_ledge_blocks) {
+  return from_maps_common(c, n, d_store, rmap, n_rmap, renv_vals, renv_sizes, n_renv_blocks,
+                          lmap, n_lmap, lenv_vals, lenv_sizes, n_lenv_blocks, true, e_store,
+                          remap, n_remap, redge_vals, redge_sizes, n_redge_blocks, lemap,
+                          n_lemap, ledge_vals, ledge_sizes, n_ledge_blocks,
+                          "plan_from_maps_pbc");
 }
 
 int dmrgx_plan_info(dmrgx_ctx* c, int64_t* out) {
@@ -640,12 +898,24 @@ int dmrgx_plan_info(dmrgx_ctx* c, int64_t* out) {
     return DMRGX_E_STATE;
   }
   out[0] = c->n;
-  out[1] = c->d_store;
-  out[2] = (int64_t)c->rmap.size();
-  out[3] = (int64_t)c->lmap.size();
+  out[1] = c->d_store_main;
+  out[2] = c->n_rmap_main;
+  out[3] = c->n_lmap_main;
   out[4] = c->flops;
   out[5] = (int64_t)c->psi_sym.size();
   out[6] = c->n_store_blocks;
+  return 0;
+}
+
+int dmrgx_plan_edge_info(dmrgx_ctx* c, int64_t* out) {
+  ARG_CHECK(c && out, "null argument");
+  if (!c->has_plan) {
+    set_error("plan_edge_info: no plan");
+    return DMRGX_E_STATE;
+  }
+  out[0] = c->d_store - c->d_store_main;
+  out[1] = (int64_t)c->rmap.size() - c->n_rmap_main;
+  out[2] = (int64_t)c->lmap.size() - c->n_lmap_main;
   return 0;
 }
 
@@ -655,21 +925,30 @@ int dmrgx_plan_maps(dmrgx_ctx* c, int* rmap, int* lmap) {
     set_error("plan_maps: no plan");
     return DMRGX_E_STATE;
   }
-  auto put = [](const std::vector<MapRow>& rows, int* o) {
-    for (size_t i = 0; i < rows.size(); i++) {
-      const MapRow& r = rows[i];
-      int* p = o + 7 * i;
-      p[0] = r.blk;
-      p[1] = (int)r.in_beg;
-      p[2] = (int)r.out_beg;
-      p[3] = r.rows;
-      p[4] = r.cols;
-      p[5] = r.beta;
-      p[6] = r.alpha;
-    }
-  };
-  put(c->rmap, rmap);
-  put(c->lmap, lmap);
+  put_rows(c->rmap.data(), c->n_rmap_main, rmap);
+  put_rows(c->lmap.data(), c->n_lmap_main, lmap);
+  return 0;
+}
+
+int dmrgx_plan_edge_maps(dmrgx_ctx* c, int* remap, int* lemap) {
+  ARG_CHECK(c && remap && lemap, "null argument");
+  if (!c->has_plan) {
+    set_error("plan_edge_maps: no plan");
+    return DMRGX_E_STATE;
+  }
+  // undo the merge shifts: edge rows against the edge pair's own blocks and store
+  std::vector<MapRow> er(c->rmap.begin() + c->n_rmap_main, c->rmap.end());
+  std::vector<MapRow> el(c->lmap.begin() + c->n_lmap_main, c->lmap.end());
+  for (auto& r : er) {
+    r.blk -= c->r_blocks_main;
+    r.out_beg -= c->d_store_main;
+  }
+  for (auto& r : el) {
+    r.blk -= c->l_blocks_main;
+    r.in_beg -= c->d_store_main;
+  }
+  put_rows(er.data(), (int64_t)er.size(), remap);
+  put_rows(el.data(), (int64_t)el.size(), lemap);
   return 0;
 }
 

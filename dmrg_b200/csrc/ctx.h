@@ -104,7 +104,14 @@ struct dmrgx_ctx {
 
   bool has_plan = false;
   int64_t n = 0, d_store = 0, flops = 0;
+  // task lists the stages run: the main pair's rows (the reference's rmap / lmap)
+  // followed, on a periodic chain, by the edge pair's remap / lemap rows with
+  // block indices shifted past the main environments' blocks and store offsets
+  // past the main store (src/core.cpp:27-30, :241-247)
   std::vector<dmrgx::MapRow> rmap, lmap;
+  int64_t n_rmap_main = 0, n_lmap_main = 0, d_store_main = 0;
+  int r_blocks_main = 0, l_blocks_main = 0;
+  int boundary = 0;    // DMRGX_BOUNDARY_* of dmrgx_dmrg
   std::vector<std::vector<int>> psi_dim, psi_sym;
   int n_store_blocks = 0;
   dmrgx::Stage st1, st2;

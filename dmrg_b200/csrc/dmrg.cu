@@ -25,7 +25,8 @@
 namespace dmrgx {
 
 int plan_build_device(dmrgx_ctx* c, const QTensor& L, const QTensor& R, int l_num, int r_num,
-                      int sector, const Group& G);
+                      int sector, const Group& G, const QTensor* Le = nullptr,
+                      const QTensor* Re = nullptr);
 
 namespace {
 
@@ -197,6 +198,30 @@ bool build_mpo(int model, const double* par, HostQT& W) {
   return false;
 }
 
+// qtensor::id(bulk_mpo) (src/qtensor.cpp:157-184): the operator that carries an
+// edge environment across a bulk site on a periodic chain.  Legs and directions
+// of the bulk MPO W, except legs 0 and 2, which take the edge environment's MPO
+// leg (leg 1); one block (s0, s1, s0, s1) per pair of sectors with
+// delta(i0, i2) delta(i1, i3).  Blocks of zero size are left out (they hold no
+// values).
+HostQT edge_identity(const QMeta& edge, const QMeta& W) {
+  HostQT R;
+  R.m.dims = W.dims;
+  R.m.dirs = W.dirs;
+  R.m.dims[0] = R.m.dims[2] = edge.dims[1];
+  R.m.dirs[0] = R.m.dirs[2] = edge.dirs[1];
+  for (int s0 = 0; s0 < (int)R.m.dims[0].size(); s0++)
+    for (int s1 = 0; s1 < (int)R.m.dims[1].size(); s1++) {
+      const int a = R.m.dims[0][s0], b = R.m.dims[1][s1];
+      if (a == 0 || b == 0) continue;
+      R.add_block({s0, s1, s0, s1}, {a, b, a, b});
+      for (int i0 = 0; i0 < a; i0++)
+        for (int i1 = 0; i1 < b; i1++)
+          R.blocks.back()[(((size_t)i0 * b + i1) * a + i0) * b + i1] = cplx(1, 0);
+    }
+  return R;
+}
+
 QTPtr upload(const HostQT& H, int f, cudaStream_t s, std::string& err) {
   auto T = std::make_shared<QTensor>();
   T->m = H.m;
@@ -232,6 +257,11 @@ struct Run {
   QTPtr cpsi;
   int model = 0;
   std::vector<double> par;   // model parameters of the MPO in use
+  // periodic chain (the reference's PBC build): edge environments mps.edge(i),
+  // seeded at 0 and L-1 with the drivers' edge operators (src/mps.h add_edge)
+  bool pbc = false;
+  std::vector<QTPtr> edge;
+  std::map<std::pair<std::vector<int>, int>, QTPtr> edge_ids;  // id(W) by (dims, dir) of leg 1
   // per-step records
   std::vector<int> lr;
   std::vector<double> energies, trunc;
@@ -247,10 +277,11 @@ struct Run {
         .count();
   }
 
-  // plan of a step (timed)
-  int plan(const QTensor& Lop, const QTensor& Rop, int ln, int rn, int sec, const Group& G) {
+  // plan of a step (timed); Le / Re: the edge pair of a periodic chain
+  int plan(const QTensor& Lop, const QTensor& Rop, int ln, int rn, int sec, const Group& G,
+           const QTensor* Le = nullptr, const QTensor* Re = nullptr) {
     const double t0 = now();
-    const int rc = plan_build_device(c, Lop, Rop, ln, rn, sec, G);
+    const int rc = plan_build_device(c, Lop, Rop, ln, rn, sec, G, Le, Re);
     t_plan += now() - t0;
     return rc;
   }
@@ -342,17 +373,50 @@ struct Run {
     return o;
   }
 
+  // periodic chain: the edge environment carried across a bulk site,
+  //   ledge = (edge(l-1) ._1 ope).exchange(3,4)          (src/core.cpp:193-197)
+  //   redge = (edge(r+1) ._1 ope, change).exchange(0,1)   (src/core.cpp:198-199)
+  // ope = e.id(W) of the edge environment e the step names: edge(l-1) for both
+  // sides in update_two and move2right, edge(r+1) in move2left (:302, :418)
+  QTPtr edge_op(const QTensor& e) {
+    auto key = std::make_pair(e.m.dims[1], e.m.dirs[1]);
+    auto it = edge_ids.find(key);
+    if (it != edge_ids.end()) return it->second;
+    QTPtr o = upload(edge_identity(e.m, bulk->m), c->f(), E.stream, err);
+    if (o) edge_ids[key] = o;
+    return o;
+  }
+  QTPtr fuse_edge_left(int l, const QTPtr& ope) {
+    const double t0 = now();
+    QTPtr o = ope ? qt_contract_legs(E, *edge[l - 1], 1, *ope, 0, false, 3, 4, err) : nullptr;
+    t_fuse += now() - t0;
+    return o;
+  }
+  QTPtr fuse_edge_right(int r, const QTPtr& ope) {
+    const double t0 = now();
+    QTPtr o = ope ? qt_contract_legs(E, *edge[r + 1], 1, *ope, 0, true, 0, 1, err) : nullptr;
+    t_fuse += now() - t0;
+    return o;
+  }
+
   // src/core.cpp:88-172
   int two_sites(int l, int r, int cutoff) {
     const QTensor& le = mpo(l);
     const QTensor& re = mpo(r);
-    int rc = plan(le, re, 2, 1, sector, E.G);
+    // on a periodic chain the edge pair is edge(l), edge(r) (src/core.cpp:96-99)
+    QTPtr lx = pbc ? edge[l] : nullptr, rx = pbc ? edge[r] : nullptr;
+    int rc = plan(le, re, 2, 1, sector, E.G, lx.get(), rx.get());
     if (rc) return fail(rc);
     QTPtr psi, U, V;
     if ((rc = solve(l, r, psi))) return rc;
     if ((rc = svd(*psi, 1, cutoff, U, V))) return rc;
     env[l] = left_update(le, *U, 1);
     env[r] = right_update(re, *V, 1);
+    if (pbc) {
+      edge[l] = left_update(*lx, *U, 1);   // src/core.cpp:161-170
+      edge[r] = right_update(*rx, *V, 1);
+      if (!edge[l] || !edge[r]) return DMRGX_E_CUDA;
+    }
     site[l] = U;
     site[r] = V;
     center = -1;
@@ -362,13 +426,25 @@ struct Run {
   int update_two(int l, int r, int cutoff) {
     QTPtr le = fuse_left(l), re = fuse_right(r);
     if (!le || !re) return DMRGX_E_CUDA;
-    int rc = plan(*le, *re, 3, 2, sector, E.G);
+    QTPtr lx, rx;
+    if (pbc) {
+      QTPtr ope = edge_op(*edge[l - 1]);
+      lx = fuse_edge_left(l, ope);
+      rx = fuse_edge_right(r, ope);
+      if (!lx || !rx) return DMRGX_E_CUDA;
+    }
+    int rc = plan(*le, *re, 3, 2, sector, E.G, lx.get(), rx.get());
     if (rc) return fail(rc);
     QTPtr psi, U, V;
     if ((rc = solve(l, r, psi))) return rc;
     if ((rc = svd(*psi, 2, cutoff, U, V))) return rc;
     env[l] = left_update(*le, *U, 2);
     env[r] = right_update(*re, *V, 2);
+    if (pbc) {
+      edge[l] = left_update(*lx, *U, 2);   // src/core.cpp:272-281
+      edge[r] = right_update(*rx, *V, 2);
+      if (!edge[l] || !edge[r]) return DMRGX_E_CUDA;
+    }
     site[l] = U;
     site[r] = V;
     center = -1;
@@ -378,12 +454,19 @@ struct Run {
   int move2right(int l, int r, int cutoff) {
     QTPtr le = fuse_left(l);
     if (!le) return DMRGX_E_CUDA;
-    int rc = plan(*le, *env[r], 3, 1, sector, E.G);
+    QTPtr lx, rx;
+    if (pbc) {  // src/core.cpp:302-307
+      lx = fuse_edge_left(l, edge_op(*edge[l - 1]));
+      rx = edge[r];
+      if (!lx || !rx) return DMRGX_E_CUDA;
+    }
+    int rc = plan(*le, *env[r], 3, 1, sector, E.G, lx.get(), rx.get());
     if (rc) return fail(rc);
     QTPtr psi, U, V;
     if ((rc = solve(l, r, psi))) return rc;
     if ((rc = svd(*psi, 2, cutoff, U, V))) return rc;
     env[l] = left_update(*le, *U, 2);
+    if (pbc && !(edge[l] = left_update(*lx, *U, 2))) return DMRGX_E_CUDA;  // :371-376
     site[l] = U;
     center = l;  // psi[a_{l-1}, s_l, b_r]: centre at l, right block from r = l + 1
     cpsi = psi;
@@ -393,12 +476,19 @@ struct Run {
   int move2left(int l, int r, int cutoff) {
     QTPtr re = fuse_right(r);
     if (!re) return DMRGX_E_CUDA;
-    int rc = plan(*env[l], *re, 2, 2, sector, E.G);
+    QTPtr lx, rx;
+    if (pbc) {  // src/core.cpp:398-403
+      lx = edge[l];
+      rx = fuse_edge_right(r, edge_op(*edge[r + 1]));
+      if (!lx || !rx) return DMRGX_E_CUDA;
+    }
+    int rc = plan(*env[l], *re, 2, 2, sector, E.G, lx.get(), rx.get());
     if (rc) return fail(rc);
     QTPtr psi, U, V;
     if ((rc = solve(l, r, psi))) return rc;
     if ((rc = svd(*psi, 1, cutoff, U, V))) return rc;
     env[r] = right_update(*re, *V, 2);
+    if (pbc && !(edge[r] = right_update(*rx, *V, 2))) return DMRGX_E_CUDA;  // :467-472
     site[r] = V;
     center = r;  // psi[b_l, s_r, a_{r+1}]: centre at r, left block through l = r - 1
     cpsi = psi;
@@ -618,6 +708,10 @@ struct Run {
   // [2] max_k |<dE/dW_k, W_k> - E0| (E is linear in each W_k), [3] max discarded weight.
   int adjoint(bool recompute, const std::vector<double>& w_host,
               std::vector<std::vector<double>>& gw, double* checks) {
+    if (pbc) {
+      err = "adjoint: periodic chains are not supported";
+      return DMRGX_E_STATE;
+    }
     if (center < 0 || !cpsi) {
       err = "adjoint: the last step left no one-site centre (the schedule must end with a move)";
       return DMRGX_E_STATE;
@@ -677,6 +771,10 @@ struct Run {
 
   // <Psi|H(W)|Psi> of the current state for another MPO of the same shape
   int expect(const QTPtr& W, const QTPtr& le, const QTPtr& re, double& value) {
+    if (pbc) {
+      err = "expect: periodic chains are not supported";
+      return DMRGX_E_STATE;
+    }
     if (center < 0 || !cpsi) {
       err = "expect: no state (run dmrg first)";
       return DMRGX_E_STATE;
@@ -811,6 +909,29 @@ extern "C" int dmrgx_dmrg(dmrgx_ctx* c, int model, int L, int m, int sweeps, int
   }
   R->env.assign(L, nullptr);
   R->site.assign(L, nullptr);
+  if (c->boundary == DMRGX_BOUNDARY_PERIODIC) {
+    // the drivers' edge operators: kitaev.cpp:42-45 H_Kitaev(t, -p, 0),
+    // xyz.cpp:39-42 H_XYZ(jx, jy, jz) (no field), potts.cpp:44-47 H_Potts3(0, j, p, t)
+    std::vector<double> ep(R->par);
+    if (model == 0) {
+      ep[1] = -ep[1];
+      ep[2] = 0.0;
+    } else if (model == 2) {
+      ep[0] = 0.0;
+    } else {
+      ep[3] = 0.0;
+    }
+    QTPtr eb, el, er;
+    if (!mpo_set(model, ep.data(), c->f(), c->stream, eb, el, er, nullptr, err)) {
+      delete R;
+      set_error("dmrg: edge operators: " + err);
+      return DMRGX_E_CUDA;
+    }
+    R->pbc = true;
+    R->edge.assign(L, nullptr);
+    R->edge[0] = el;
+    R->edge[L - 1] = er;
+  }
   const double t0 = Run::now();
   int rc = R->dmrg(m, sweeps);
   const double t1 = Run::now();

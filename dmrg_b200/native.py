@@ -19,6 +19,7 @@ PREC_FP64, PREC_BF16X3, PREC_TF32X3 = 0, 1, 2
 SCHED_GROUPED, SCHED_PER_BLOCK = 0, 1
 GROUP_Z2CUBED = -8  # group_n of the Z2 x Z2 x Z2 (S4E) fusion rule
 MEM_HOST, MEM_DEVICE = 0, 1
+BOUNDARY_OPEN, BOUNDARY_PERIODIC = 0, 1
 
 # every entry point declared in include/dmrgx.h, with (restype, argtypes)
 _vp, _ip, _i, _i64 = C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_int64
@@ -33,8 +34,18 @@ SIGNATURES = {
     "dmrgx_build_maps": (_i, [_ip, _ip, _i, _i, _i, _i, _i, _i64p, _ip, _i64, _ip, _i64]),
     "dmrgx_plan_from_maps": (_i, [_vp, _i64, _i64, _ip, _i, _vp, _i64p, _i, _ip, _i, _vp,
                                   _i64p, _i]),
+    "dmrgx_plan_build_pbc": (_i, [_vp, _ip, _vp, _ip, _vp, _ip, _vp, _ip, _vp, _i, _i, _i, _i,
+                                  _i]),
+    "dmrgx_build_maps_pbc": (_i, [_ip, _ip, _ip, _ip, _i, _i, _i, _i, _i, _i64p, _ip, _i64, _ip,
+                                  _i64, _ip, _i64, _ip, _i64]),
+    "dmrgx_plan_from_maps_pbc": (_i, [_vp, _i64, _i64, _ip, _i, _vp, _i64p, _i, _ip, _i, _vp,
+                                      _i64p, _i, _i64, _ip, _i, _vp, _i64p, _i, _ip, _i, _vp,
+                                      _i64p, _i]),
     "dmrgx_plan_info": (_i, [_vp, _i64p]),
+    "dmrgx_plan_edge_info": (_i, [_vp, _i64p]),
     "dmrgx_plan_maps": (_i, [_vp, _ip, _ip]),
+    "dmrgx_plan_edge_maps": (_i, [_vp, _ip, _ip]),
+    "dmrgx_set_boundary": (_i, [_vp, _i]),
     "dmrgx_plan_psi_layout": (_i, [_vp, _ip, _i64]),
     "dmrgx_av": (_i, [_vp, _vp, _vp, _i]),
     "dmrgx_av_noalloc": (_i, [_i, _i64, _i64, _ip, _i, _vp, _i64p, _i, _ip, _i, _vp, _i64p, _i,
@@ -102,6 +113,23 @@ def build_maps(lenv_meta, renv_meta, l_num, r_num, sector, group_n, fermion):
                                   _i64p(info), _ip(rmap), rmap.shape[0], _ip(lmap),
                                   lmap.shape[0]))
     return int(info[0]), int(info[1]), rmap[: info[2]], lmap[: info[3]]
+
+
+def build_maps_pbc(lenv_meta, renv_meta, ledge_meta, redge_meta, l_num, r_num, sector, group_n,
+                   fermion):
+    """build_maps with the periodic edge pair: (n, d_store, rmap, lmap, e_store, remap, lemap)."""
+    m = [np.ascontiguousarray(x, np.int32) for x in (lenv_meta, renv_meta, ledge_meta, redge_meta)]
+    info = np.zeros(7, np.int64)
+    _check(lib().dmrgx_build_maps_pbc(*[_ip(x) for x in m], l_num, r_num, sector, group_n,
+                                      fermion, _i64p(info), None, 0, None, 0, None, 0, None, 0))
+    maps = [np.zeros((max(1, int(info[k])), 7), np.int32) for k in (2, 3, 5, 6)]
+    args = []
+    for a in maps:
+        args += [_ip(a), a.shape[0]]
+    _check(lib().dmrgx_build_maps_pbc(*[_ip(x) for x in m], l_num, r_num, sector, group_n,
+                                      fermion, _i64p(info), *args))
+    rmap, lmap, remap, lemap = (a[: int(info[k])] for a, k in zip(maps, (2, 3, 5, 6)))
+    return int(info[0]), int(info[1]), rmap, lmap, int(info[4]), remap, lemap
 
 
 def av_noalloc(dtype, n, d_store, rmap, renv_dev, renv_sizes, lmap, lenv_dev, lenv_sizes,
@@ -172,6 +200,54 @@ class Context:
         _check(lib().dmrgx_plan_build(self.ptr, _ip(lm), lv.ctypes.data, _ip(rm), rv.ctypes.data,
                                       l_num, r_num, sector, group_n, fermion))
         self._refresh()
+
+    def plan_build_pbc(self, lenv, renv, ledge, redge, l_num, r_num, sector, group_n,
+                       fermion=0):
+        """Periodic chain: (meta, values) of lenv, renv and the edge pair ledge, redge."""
+        ms = [np.ascontiguousarray(t[0], np.int32) for t in (lenv, renv, ledge, redge)]
+        vs = [np.ascontiguousarray(t[1], self._np) for t in (lenv, renv, ledge, redge)]
+        args = []
+        for m, v in zip(ms, vs):
+            args += [_ip(m), v.ctypes.data]
+        _check(lib().dmrgx_plan_build_pbc(self.ptr, *args, l_num, r_num, sector, group_n,
+                                          fermion))
+        self._refresh()
+
+    def plan_from_maps_pbc(self, n, d_store, rmap, renv_vals, renv_sizes, lmap, lenv_vals,
+                           lenv_sizes, e_store, remap, redge_vals, redge_sizes, lemap,
+                           ledge_vals, ledge_sizes):
+        """The drop-in for a PBC build's lanczos<T>: both pairs' task lists and blocks."""
+        keep = []
+
+        def m7(a):
+            a = np.ascontiguousarray(a, np.int32).reshape(-1, 7)
+            keep.append(a)
+            return _ip(a), a.shape[0]
+
+        def vals(v, sz):
+            v = np.ascontiguousarray(v, self._np)
+            sz = np.ascontiguousarray(sz, np.int64)
+            keep.extend([v, sz])
+            return v.ctypes.data, _i64p(sz), sz.size
+
+        _check(lib().dmrgx_plan_from_maps_pbc(
+            self.ptr, n, d_store, *m7(rmap), *vals(renv_vals, renv_sizes), *m7(lmap),
+            *vals(lenv_vals, lenv_sizes), e_store, *m7(remap), *vals(redge_vals, redge_sizes),
+            *m7(lemap), *vals(ledge_vals, ledge_sizes)))
+        self._refresh()
+
+    def edge_maps(self):
+        """(e_store, remap, lemap) of the current plan's edge pair."""
+        info = np.zeros(3, np.int64)
+        _check(lib().dmrgx_plan_edge_info(self.ptr, _i64p(info)))
+        r = np.zeros((max(1, int(info[1])), 7), np.int32)
+        l = np.zeros((max(1, int(info[2])), 7), np.int32)
+        _check(lib().dmrgx_plan_edge_maps(self.ptr, _ip(r), _ip(l)))
+        return int(info[0]), r[: int(info[1])], l[: int(info[2])]
+
+    def set_boundary(self, boundary):
+        """BOUNDARY_OPEN (default) or BOUNDARY_PERIODIC for the next dmrg()."""
+        _check(lib().dmrgx_set_boundary(self.ptr, boundary))
 
     def plan_from_maps(self, n, d_store, rmap, renv_vals, renv_sizes, lmap, lenv_vals,
                        lenv_sizes):

@@ -64,6 +64,9 @@ enum { DMRGX_MEM_HOST = 0, DMRGX_MEM_DEVICE = 1 };
 /* group_n value selecting the Z2 x Z2 x Z2 fusion rule (S4E, src/useful.cpp:4-27) */
 enum { DMRGX_GROUP_Z2CUBED = -8 };
 
+/* chain boundary of dmrgx_dmrg (the reference's PBC switch, global.h:14) */
+enum { DMRGX_BOUNDARY_OPEN = 0, DMRGX_BOUNDARY_PERIODIC = 1 };
+
 typedef struct dmrgx_ctx dmrgx_ctx;
 
 const char* dmrgx_last_error(void);
@@ -136,13 +139,56 @@ int dmrgx_build_maps(const int* lenv_meta, const int* renv_meta, int l_num, int 
                      int sector, int group_n, int fermion, int64_t* info, int* rmap,
                      int64_t rmap_cap, int* lmap, int64_t lmap_cap);
 
-/* Plan facts: out[0]=n, out[1]=d_store, out[2]=rows of rmap, out[3]=rows of lmap,
- * out[4]=useful real flops of one matvec (2*M*N*K per task, x4 for complex),
- * out[5]=psi blocks, out[6]=store blocks. */
+/* Periodic chains: the edge pair of av() (src/core.cpp:27-30, PBC build).  The
+ * matvec becomes
+ *   out = lenv (x) (renv (x) in) + ledge (x) (redge (x) in)
+ * with the edge pair's task lists built as the step functions build them
+ * (src/core.cpp:241-247): remap = redge.get_map(psi layout, 'N','T', r_num, 0)
+ * with its own intermediate (e_store elements), lemap = ledge.get_map(...,
+ * l_num, beta = 1, back = true).  The reference shares one store of
+ * max(d_store, e_store) between the pairs and runs them one after the other;
+ * here each pair has its own intermediate and both run in the same two
+ * launches (the edge rows are further tasks of each stage).  Arguments as for
+ * the open-chain calls; ledge/redge have the legs of lenv/renv. */
+int dmrgx_plan_build_pbc(dmrgx_ctx* ctx, const int* lenv_meta, const void* lenv_vals,
+                         const int* renv_meta, const void* renv_vals, const int* ledge_meta,
+                         const void* ledge_vals, const int* redge_meta, const void* redge_vals,
+                         int l_num, int r_num, int sector, int group_n, int fermion);
+
+/* dmrgx_build_maps with the edge pair: info (7 slots) adds info[4]=e_store,
+ * info[5]=rows of remap, info[6]=rows of lemap. */
+int dmrgx_build_maps_pbc(const int* lenv_meta, const int* renv_meta, const int* ledge_meta,
+                         const int* redge_meta, int l_num, int r_num, int sector, int group_n,
+                         int fermion, int64_t* info, int* rmap, int64_t rmap_cap, int* lmap,
+                         int64_t lmap_cap, int* remap, int64_t remap_cap, int* lemap,
+                         int64_t lemap_cap);
+
+/* dmrgx_plan_from_maps with the edge pair: the drop-in for a PBC build's
+ * lanczos<T> (include/val_for_lanczos.h:18-23: ledge, redge, lemap, remap). */
+int dmrgx_plan_from_maps_pbc(dmrgx_ctx* ctx, int64_t n, int64_t d_store, const int* rmap,
+                             int n_rmap, const void* renv_vals, const int64_t* renv_sizes,
+                             int n_renv_blocks, const int* lmap, int n_lmap,
+                             const void* lenv_vals, const int64_t* lenv_sizes, int n_lenv_blocks,
+                             int64_t e_store, const int* remap, int n_remap,
+                             const void* redge_vals, const int64_t* redge_sizes,
+                             int n_redge_blocks, const int* lemap, int n_lemap,
+                             const void* ledge_vals, const int64_t* ledge_sizes,
+                             int n_ledge_blocks);
+
+/* Plan facts: out[0]=n, out[1]=d_store, out[2]=rows of rmap, out[3]=rows of lmap
+ * (the main pair), out[4]=useful real flops of one matvec (2*M*N*K per task, x4
+ * for complex, both pairs), out[5]=psi blocks, out[6]=store blocks. */
 int dmrgx_plan_info(dmrgx_ctx* ctx, int64_t* out);
+
+/* Edge pair of the current plan: out[0]=e_store, out[1]=rows of remap,
+ * out[2]=rows of lemap (all 0 on an open chain). */
+int dmrgx_plan_edge_info(dmrgx_ctx* ctx, int64_t* out);
 
 /* Copy out the task lists of the current plan, reference row format. */
 int dmrgx_plan_maps(dmrgx_ctx* ctx, int* rmap, int* lmap);
+
+/* Copy out the edge pair's task lists (remap, lemap), reference row format. */
+int dmrgx_plan_edge_maps(dmrgx_ctx* ctx, int* remap, int* lemap);
 
 /* Copy out the psi layout: nleg, nblk, nsec[], dims..., sym[blk][leg]. */
 int dmrgx_plan_psi_layout(dmrgx_ctx* ctx, int* out, int64_t cap);
@@ -211,6 +257,17 @@ int dmrgx_eigsolve(dmrgx_ctx* ctx, int nev, int ncv, double tol, int maxiter, co
 int dmrgx_dmrg(dmrgx_ctx* ctx, int model, int L, int m, int sweeps, int sector,
                const double* params, int nparams, double* energies, double* trunc, int* steps_lr,
                int64_t* matvecs, int64_t cap, int64_t* nsteps, double* seconds);
+
+/* Boundary condition of the next dmrgx_dmrg: DMRGX_BOUNDARY_OPEN (default) or
+ * DMRGX_BOUNDARY_PERIODIC, the reference's PBC build (global.h:14): the MPS
+ * carries edge environments seeded with the edge operators the drivers give
+ * (kitaev.cpp:42-45 H_Kitaev(t, -p, 0), xyz.cpp:39-42 H_XYZ(jx, jy, jz),
+ * potts.cpp:44-47 H_Potts3(0, j, p, t); left() / right()), carried across the
+ * chain by the identity operator id(W) (src/qtensor.cpp:157-184) and updated
+ * with the bulk environments (src/core.cpp:93-97, :193-199, :272-282, ...);
+ * every step's matvec adds the edge pair.  dmrgx_adjoint and dmrgx_expect
+ * refuse a periodic run. */
+int dmrgx_set_boundary(dmrgx_ctx* ctx, int boundary);
 /* XYZ (models 1 and 3) accept a fourth parameter h: a field h sum_i sigma^z_i,
  * absent from the reference (nparams = 3, or h = 0, is the reference's MPO).
  * The final state of dmrgx_dmrg (MPS site tensors, environments and the one-site

@@ -41,24 +41,28 @@ def _kron_chain(ops):
     return out
 
 
-def xyz_ed(L: int, jx: float, jy: float, jz: float, sector: int = 0) -> float:
+def xyz_ed(L: int, jx: float, jy: float, jz: float, sector: int = 0,
+           periodic: bool = False) -> float:
+    """periodic adds the bond (L-1, 0), the reference's PBC build (xyz.cpp:39-42)."""
     X = np.array([[0, 1], [1, 0]], complex)
     Y = np.array([[0, -1j], [1j, 0]], complex)
     Z = np.array([[1, 0], [0, -1]], complex)
     I = np.eye(2)
     H = np.zeros((2 ** L, 2 ** L), complex)
-    for i in range(L - 1):
+    for i in range(L if periodic else L - 1):
         for J, P in ((jx, X), (jy, Y), (jz, Z)):
             ops = [I] * L
             ops[i] = P
-            ops[i + 1] = P
+            ops[(i + 1) % L] = P
             H += J * _kron_chain(ops)
     # basis state index bits: label 1 = down spin; keep even/odd count of 1s
     idx = [s for s in range(2 ** L) if bin(s).count("1") % 2 == sector]
     return float(np.linalg.eigvalsh(H[np.ix_(idx, idx)])[0])
 
 
-def potts_ed(L: int, f: float, j: float, sector: int = 0) -> float:
+def potts_ed(L: int, f: float, j: float, sector: int = 0, periodic: bool = False) -> float:
+    """periodic adds the bond (L-1, 0) without a second field term, the reference's
+    PBC build (potts.cpp:44-47: edge operators H_Potts3(0, j, p, t))."""
     w = np.exp(2j * np.pi / 3)
     T = np.diag([1, w, w * w])
     S = np.zeros((3, 3), complex)
@@ -71,10 +75,10 @@ def potts_ed(L: int, f: float, j: float, sector: int = 0) -> float:
         ops = [I] * L
         ops[i] = T + T.conj().T
         H += -f * _kron_chain(ops)
-    for i in range(L - 1):
+    for i in range(L if periodic else L - 1):
         ops = [I] * L
         ops[i] = S
-        ops[i + 1] = S.conj().T
+        ops[(i + 1) % L] = S.conj().T
         M = _kron_chain(ops)
         H += -j * (M + M.conj().T)
     charge = []

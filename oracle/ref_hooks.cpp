@@ -102,6 +102,8 @@ extern "C" void oref_av(int is_complex, void* pv, const void* in, void* out)
     av<double>((double*)in, (double*)out, *(lanczos<double>*)pv);
 }
 
+/* out: l_num, r_num, rows of rmap, rows of lmap, rows of remap, rows of lemap
+   (the last two 0 unless built with PBC) */
 template <typename T>
 static void pv_info_t(lanczos<T>* pv, int* out)
 {
@@ -109,6 +111,13 @@ static void pv_info_t(lanczos<T>* pv, int* out)
   out[1] = pv->r_num;
   out[2] = (int)pv->rmap.size();
   out[3] = (int)pv->lmap.size();
+#ifdef PBC
+  out[4] = (int)pv->remap.size();
+  out[5] = (int)pv->lemap.size();
+#else
+  out[4] = 0;
+  out[5] = 0;
+#endif
 }
 
 extern "C" void oref_pv_info(int is_complex, void* pv, int* out)
@@ -132,15 +141,50 @@ extern "C" void oref_pv_maps(int is_complex, void* pv, int* rmap, int* lmap)
   else pv_maps_t((lanczos<double>*)pv, rmap, lmap);
 }
 
-/* which: 0 = lenv, 1 = renv */
+/* edge task lists of a PBC build (include/val_for_lanczos.h:18-23) */
+template <typename T>
+static void pv_edge_maps_t(lanczos<T>* pv, int* remap, int* lemap)
+{
+#ifdef PBC
+  for (size_t i = 0; i < pv->remap.size(); i++)
+    for (int j = 0; j < 7; j++) remap[i * 7 + j] = pv->remap[i][j];
+  for (size_t i = 0; i < pv->lemap.size(); i++)
+    for (int j = 0; j < 7; j++) lemap[i * 7 + j] = pv->lemap[i][j];
+#endif
+}
+
+extern "C" void oref_pv_edge_maps(int is_complex, void* pv, int* remap, int* lemap)
+{
+  if (is_complex) pv_edge_maps_t((lanczos<complex<double> >*)pv, remap, lemap);
+  else pv_edge_maps_t((lanczos<double>*)pv, remap, lemap);
+}
+
+extern "C" int oref_pbc()
+{
+#ifdef PBC
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+/* which: 0 = lenv, 1 = renv, 2 = ledge, 3 = redge (PBC builds) */
+template <typename T>
+static void* pv_env_t(lanczos<T>* p, int which)
+{
+  if (which == 0) return (void*)&p->lenv;
+  if (which == 1) return (void*)&p->renv;
+#ifdef PBC
+  if (which == 2) return (void*)&p->ledge;
+  if (which == 3) return (void*)&p->redge;
+#endif
+  return 0;
+}
+
 extern "C" void* oref_pv_env(int is_complex, void* pv, int which)
 {
-  if (is_complex) {
-    lanczos<complex<double> >* p = (lanczos<complex<double> >*)pv;
-    return which ? (void*)&p->renv : (void*)&p->lenv;
-  }
-  lanczos<double>* p = (lanczos<double>*)pv;
-  return which ? (void*)&p->renv : (void*)&p->lenv;
+  if (is_complex) return pv_env_t((lanczos<complex<double> >*)pv, which);
+  return pv_env_t((lanczos<double>*)pv, which);
 }
 
 /* ---- qtensor (de)serialisation ---- */
@@ -289,6 +333,62 @@ static void* pv_build_t(const qtensor<T>* le, const qtensor<T>* re, int l_num, i
   info[2] = (int)b->pv.rmap.size();
   info[3] = (int)b->pv.lmap.size();
   return (void*)b;
+}
+
+#ifdef PBC
+/* the same with the edge pair, as update_two builds it (src/core.cpp:241-247):
+   info out: n, d_store, n_rmap, n_lmap, e_store, n_remap, n_lemap; the store
+   holds max(d_store, e_store) elements, shared by both pairs as in av() */
+template <typename T>
+static void* pv_build_pbc_t(const qtensor<T>* le, const qtensor<T>* re, const qtensor<T>* lx,
+                            const qtensor<T>* rx, int l_num, int r_num, int sector, int* info)
+{
+  OrefBox<T>* b = new OrefBox<T>();
+  b->pv.lenv = *le;
+  b->pv.renv = *re;
+  b->pv.ledge = *lx;
+  b->pv.redge = *rx;
+  generate_dim_sym(b->dim, b->sym, b->pv.lenv, l_num - 1, b->pv.renv, r_num, sector);
+  b->n = get_dimension(b->dim, b->sym);
+  b->pv.r_num = r_num;
+  b->pv.l_num = l_num;
+  b->pv.renv.get_map(b->pv.rmap, b->dim_ret, b->sym_ret, b->dim, b->sym, 'N', 'T', r_num, 0);
+  b->d_store = get_dimension(b->dim_ret, b->sym_ret);
+  b->pv.lenv.get_map(b->pv.lmap, b->dim, b->sym, b->dim_ret, b->sym_ret, 'N', 'T', l_num, 0,
+                     true);
+  b->pv.redge.get_map(b->pv.remap, b->dim_ret, b->sym_ret, b->dim, b->sym, 'N', 'T', r_num, 0);
+  int e_store = get_dimension(b->dim_ret, b->sym_ret);
+  b->pv.ledge.get_map(b->pv.lemap, b->dim, b->sym, b->dim_ret, b->sym_ret, 'N', 'T', l_num, 1,
+                      true);
+  int s = b->d_store > e_store ? b->d_store : e_store;
+  b->pv.store = new T[s > 0 ? s : 1];
+  info[0] = b->n;
+  info[1] = b->d_store;
+  info[2] = (int)b->pv.rmap.size();
+  info[3] = (int)b->pv.lmap.size();
+  info[4] = e_store;
+  info[5] = (int)b->pv.remap.size();
+  info[6] = (int)b->pv.lemap.size();
+  return (void*)b;
+}
+#endif
+
+extern "C" void* oref_pv_build_pbc(int is_complex, const void* le, const void* re,
+                                   const void* lx, const void* rx, int l_num, int r_num,
+                                   int sector, int* info)
+{
+#ifdef PBC
+  if (is_complex)
+    return pv_build_pbc_t((const qtensor<complex<double> >*)le,
+                          (const qtensor<complex<double> >*)re,
+                          (const qtensor<complex<double> >*)lx,
+                          (const qtensor<complex<double> >*)rx, l_num, r_num, sector, info);
+  return pv_build_pbc_t((const qtensor<double>*)le, (const qtensor<double>*)re,
+                        (const qtensor<double>*)lx, (const qtensor<double>*)rx, l_num, r_num,
+                        sector, info);
+#else
+  return 0;
+#endif
 }
 
 extern "C" void* oref_pv_build(int is_complex, const void* le, const void* re, int l_num,
@@ -475,6 +575,10 @@ extern "C" int oref_run(int model, int L, int m, int n, int sector, const double
     for (int i = 0; i < L; i++) o[i] = H_Kitaev(par[0], par[1], par[2]);
     o.edge(H_Kitaev(par[0], par[1], par[2]).left(), H_Kitaev(par[0], par[1], par[2]).right());
     mps<double> s(o);
+#ifdef PBC
+    s.add_edge(H_Kitaev(par[0], -par[1], 0.0).left(),
+               H_Kitaev(par[0], -par[1], 0.0).right());   /* kitaev.cpp:42-45 */
+#endif
     run_sched(s, o, m, n, sector, t, schedule);
     return 0;
   }
@@ -484,6 +588,10 @@ extern "C" int oref_run(int model, int L, int m, int n, int sector, const double
     mpo<complex<double> > o(L, H_XYZ(par[0], par[1], par[2]));
     o.edge();
     mps<complex<double> > s(o);
+#ifdef PBC
+    s.add_edge(H_XYZ(par[0], par[1], par[2]).left(),
+               H_XYZ(par[0], par[1], par[2]).right());   /* xyz.cpp:39-42 */
+#endif
     run_sched(s, o, m, n, sector, t, schedule);
     return 0;
   }
@@ -492,6 +600,10 @@ extern "C" int oref_run(int model, int L, int m, int n, int sector, const double
     mpo<complex<double> > o(L, H_Potts3(par[0], par[1], par[2], par[3]));
     o.edge();
     mps<complex<double> > s(o);
+#ifdef PBC
+    s.add_edge(H_Potts3(0, par[1], par[2], par[3]).left(),
+               H_Potts3(0, par[1], par[2], par[3]).right());   /* potts.cpp:44-47 */
+#endif
     run_sched(s, o, m, n, sector, t, schedule);
     return 0;
   }

@@ -23,7 +23,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REFDIR = os.path.join(HERE, "_ref")
-VARIANTS = ("kitaev", "xyz", "potts", "u1", "s4e")
+VARIANTS = ("kitaev", "xyz", "potts", "u1", "s4e", "kitaev_pbc", "xyz_pbc", "potts_pbc")
 MODEL = {"kitaev": 0, "xyz": 1, "potts": 2}
 
 _EIG_CB = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double),
@@ -68,6 +68,7 @@ class Ref:
         self.variant = variant
         self.N = self.lib.oref_symmetry()
         self.fermion = bool(self.lib.oref_fermion())
+        self.pbc = bool(self.lib.oref_pbc())
         self.capture: StepCapture | None = None
         self._cb = _EIG_CB(self._eig_cb)
         _keep.append(self._cb)
@@ -82,6 +83,9 @@ class Ref:
         lib.oref_av.argtypes = [i, vp, vp, vp]
         lib.oref_pv_info.argtypes = [i, vp, ip]
         lib.oref_pv_maps.argtypes = [i, vp, ip, ip]
+        lib.oref_pv_edge_maps.argtypes = [i, vp, ip, ip]
+        lib.oref_pv_build_pbc.argtypes = [i, vp, vp, vp, vp, i, i, i, ip]
+        lib.oref_pv_build_pbc.restype = vp
         lib.oref_pv_env.argtypes = [i, vp, i]
         lib.oref_pv_env.restype = vp
         lib.oref_qt_serialize.argtypes = [i, vp, ip, l, vp, l]
@@ -142,9 +146,17 @@ class Ref:
 
     # ------------------------------------------------------------------ helpers
     def pv_info(self, is_complex, pv):
-        out = (C.c_int * 4)()
+        out = (C.c_int * 6)()
         self.lib.oref_pv_info(is_complex, pv, out)
-        return dict(l_num=out[0], r_num=out[1], n_rmap=out[2], n_lmap=out[3])
+        return dict(l_num=out[0], r_num=out[1], n_rmap=out[2], n_lmap=out[3], n_remap=out[4],
+                    n_lemap=out[5])
+
+    def pv_edge_maps(self, is_complex, pv, info):
+        r = np.zeros((max(info["n_remap"], 1), 7), np.int32)
+        lm = np.zeros((max(info["n_lemap"], 1), 7), np.int32)
+        self.lib.oref_pv_edge_maps(is_complex, pv, r.ctypes.data_as(C.POINTER(C.c_int)),
+                                   lm.ctypes.data_as(C.POINTER(C.c_int)))
+        return r[: info["n_remap"]], lm[: info["n_lemap"]]
 
     def pv_maps(self, is_complex, pv, info):
         r = np.zeros((max(info["n_rmap"], 1), 7), np.int32)
@@ -181,8 +193,13 @@ class Ref:
             x = x + 1j * rng.standard_normal(n)
         y = np.zeros(n, x.dtype)
         self.lib.oref_av(is_complex, pv, x.ctypes.data, y.ctypes.data)
-        return dict(info=info, rmap=rmap, lmap=lmap, lenv=le, renv=re, evec=v.copy(),
+        snap = dict(info=info, rmap=rmap, lmap=lmap, lenv=le, renv=re, evec=v.copy(),
                     evals=np.array(w), x=x, ax=y)
+        if self.pbc:
+            snap["remap"], snap["lemap"] = self.pv_edge_maps(is_complex, pv, info)
+            snap["ledge"] = self.qt_to_py(is_complex, self.lib.oref_pv_env(is_complex, pv, 2))
+            snap["redge"] = self.qt_to_py(is_complex, self.lib.oref_pv_env(is_complex, pv, 3))
+        return snap
 
     # ------------------------------------------------------------------ runs
     def run(self, model: str, L: int, m: int, n: int, sector: int, params, schedule=0,

@@ -9,6 +9,7 @@
  *   -DORACLE_SYMMETRY=<N>   Z_N fusion rule (2 Kitaev/XYZ, 3 Potts, 32 U(1) embedding)
  *   -DORACLE_FERMION        fermionic operators and signs (Kitaev, S4E)
  *   -DORACLE_S4E            Z2 x Z2 x Z2 fusion rule and parity table (with SYMMETRY 8)
+ *   -DORACLE_PBC            periodic boundary: edge environments (global.h:14 PBC)
  * The numerical constants (TOL, NEV, ...) keep the values the reference ships
  * with, because the reference's ARPACK wrapper and printers read them.
  */
@@ -34,6 +35,9 @@
 #endif
 #ifdef ORACLE_S4E
 #define S4E
+#endif
+#ifdef ORACLE_PBC
+#define PBC
 #endif
 
 #define TOL 1e-10

@@ -273,23 +273,39 @@ class MatvecContext:
     sym_ret: list
     n: int
     d_store: int
+    # periodic chains (PBC build, include/val_for_lanczos.h:18-23): the edge pair
+    ledge: QT | None = None
+    redge: QT | None = None
+    remap: np.ndarray | None = None
+    lemap: np.ndarray | None = None
+    e_store: int = 0
 
 
-def build_context(G: Group, lenv: QT, renv: QT, l_num: int, r_num: int, sector: int):
+def build_context(G: Group, lenv: QT, renv: QT, l_num: int, r_num: int, sector: int,
+                  ledge: QT | None = None, redge: QT | None = None):
     """What a reference step function does before the eigensolve
-    (src/core.cpp:201-202 and :236-247 for update_two)."""
+    (src/core.cpp:201-202 and :236-247 for update_two); with ledge/redge the
+    edge pair of a periodic chain (:241-247): remap against the same psi layout
+    with its own store layout, lemap with beta = 1 into psi."""
     dim, sym = generate_dim_sym(G, lenv.dims, l_num - 1, renv.dims, r_num, sector)
     n = get_dimension(dim, sym)
     rmap, dim_ret, sym_ret = get_map(G, renv, dim, sym, "N", "T", r_num, 0)
     d_store = get_dimension(dim_ret, sym_ret)
     # input = the store layout, output = the fixed wavefunction layout (back=True)
     lmap, _, _ = get_map(G, lenv, dim_ret, sym_ret, "N", "T", l_num, 0, True, dim, sym)
-    return MatvecContext(lenv, renv, l_num, r_num, rmap, lmap, dim, sym, dim_ret, sym_ret,
-                         n, d_store)
+    ctx = MatvecContext(lenv, renv, l_num, r_num, rmap, lmap, dim, sym, dim_ret, sym_ret,
+                        n, d_store)
+    if ledge is not None:
+        remap, edim, esym = get_map(G, redge, dim, sym, "N", "T", r_num, 0)
+        ctx.e_store = get_dimension(edim, esym)
+        ctx.lemap, _, _ = get_map(G, ledge, edim, esym, "N", "T", l_num, 1, True, dim, sym)
+        ctx.remap, ctx.ledge, ctx.redge = remap, ledge, redge
+    return ctx
 
 
 def av(ctx: MatvecContext, x):
-    """out = lenv (x)_{l_num} (renv (x)_{r_num} x)   (src/core.cpp:22-31).
+    """out = lenv (x)_{l_num} (renv (x)_{r_num} x)   (src/core.cpp:22-31), plus
+    ledge (x) (redge (x) x) on a periodic chain (:27-30).
 
     Output sectors that no task writes are zero here (the reference leaves them
     untouched)."""
@@ -297,4 +313,8 @@ def av(ctx: MatvecContext, x):
     contract_map(ctx.renv, store, x, ctx.rmap, ctx.r_num)
     out = np.zeros(ctx.n, store.dtype)
     contract_map(ctx.lenv, out, store, ctx.lmap, ctx.l_num)
+    if ctx.ledge is not None:
+        est = np.zeros(ctx.e_store, store.dtype)
+        contract_map(ctx.redge, est, x, ctx.remap, ctx.r_num)
+        contract_map(ctx.ledge, out, est, ctx.lemap, ctx.l_num)
     return out

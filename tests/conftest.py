@@ -14,21 +14,27 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
 
 
-def load_steps(model):
-    """Golden per-step matvec fixtures of one model (see tests/golden/make_golden.py)."""
-    z = np.load(os.path.join(GOLDEN, f"steps_{model}.npz"))
+def load_steps(model, pbc=False):
+    """Golden per-step matvec fixtures of one model (see tests/golden/make_golden.py);
+    pbc: the periodic-chain fixtures, each step with its edge pair."""
+    z = np.load(os.path.join(GOLDEN, f"steps_{model}{'_pbc' if pbc else ''}.npz"))
     gn, ferm, sector = (int(v) for v in z["group"])
     out = []
     for k in range(int(z["nsteps"])):
         p = f"s{k}_"
-        out.append(dict(
+        st = dict(
             lenv=(z[p + "lenv_meta"], z[p + "lenv_vals"]),
             renv=(z[p + "renv_meta"], z[p + "renv_vals"]),
             l_num=int(z[p + "nums"][0]), r_num=int(z[p + "nums"][1]),
             rmap=z[p + "rmap"], lmap=z[p + "lmap"], x=z[p + "x"], ax=z[p + "ax"],
             evals=z[p + "evals"], evec=z[p + "evec"],
             group_n=gn, fermion=ferm, sector=sector,
-            complex=np.iscomplexobj(z[p + "lenv_vals"])))
+            complex=np.iscomplexobj(z[p + "lenv_vals"]))
+        if pbc:
+            st.update(ledge=(z[p + "ledge_meta"], z[p + "ledge_vals"]),
+                      redge=(z[p + "redge_meta"], z[p + "redge_vals"]),
+                      remap=z[p + "remap"], lemap=z[p + "lemap"])
+        out.append(st)
     return out
 
 

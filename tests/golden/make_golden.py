@@ -22,8 +22,13 @@ oracle/_ref by oracle/Makefile) and records:
                       task lists and av(x) of the reference's S4E build
                       (SYMMETRY 8, FERMION, src/useful.cpp:4-27).
 
+  steps_<model>_pbc.npz, energies_pbc.json
+                      the same for periodic chains (the reference's PBC build,
+                      global.h:14), each step with its edge pair: ledge/redge
+                      and the task lists remap/lemap (src/core.cpp:241-247).
+
 ``python tests/golden/make_golden.py z2cubed`` regenerates only the named
-fixtures (steps, microbench, z2cubed); no argument regenerates all of them.
+fixtures (steps, microbench, z2cubed, pbc); no argument regenerates all of them.
 
 The files are small (tens of KB) and committed; the GPU box never needs the
 reference tree.
@@ -54,6 +59,16 @@ RUNS = {
 }
 
 
+# periodic chains (the reference's PBC build); Kitaev has no closed form here
+RUNS_PBC = {
+    "kitaev": ("kitaev_pbc", 8, 16, 2, [1.0, 1.0, 0.25], 2, 1, lambda: None),
+    "xyz": ("xyz_pbc", 8, 16, 2, [1.0, 0.8, 0.5], 2, 0,
+            lambda: exact.xyz_ed(8, 1.0, 0.8, 0.5, 0, periodic=True)),
+    "potts": ("potts_pbc", 6, 27, 2, [1.0, 1.0, 0.0, 0.0], 3, 0,
+              lambda: exact.potts_ed(6, 1.0, 1.0, 0, periodic=True)),
+}
+
+
 def pick_steps(steps):
     """Last captured step of each (l_num, r_num) kind (largest bond dimension)."""
     out = {}
@@ -63,9 +78,9 @@ def pick_steps(steps):
     return [out[k] for k in sorted(out)]
 
 
-def make_steps():
+def make_steps(runs=RUNS, suffix=""):
     energies = {}
-    for model, (variant, L, m, n, par, gn, ferm, exact_fn) in RUNS.items():
+    for model, (variant, L, m, n, par, gn, ferm, exact_fn) in runs.items():
         R = refbind.Ref(variant)
         cap = refbind.StepCapture(want=lambda i, info: True)
         res = R.run(model, L, m, n, 0, par, capture=cap)
@@ -82,9 +97,14 @@ def make_steps():
             arrs[p + "ax"] = st["ax"]
             arrs[p + "evals"] = st["evals"]
             arrs[p + "evec"] = st["evec"]
+            if "ledge" in st:
+                arrs[p + "ledge_meta"], arrs[p + "ledge_vals"] = st["ledge"]
+                arrs[p + "redge_meta"], arrs[p + "redge_vals"] = st["redge"]
+                arrs[p + "remap"] = st["remap"]
+                arrs[p + "lemap"] = st["lemap"]
         arrs["nsteps"] = np.array(len(chosen))
         arrs["group"] = np.array([gn, ferm, 0], np.int32)  # group_n, fermion, sector
-        np.savez_compressed(os.path.join(HERE, f"steps_{model}.npz"), **arrs)
+        np.savez_compressed(os.path.join(HERE, f"steps_{model}{suffix}.npz"), **arrs)
         e_exact = exact_fn()
         energies[model] = dict(
             args=dict(L=L, m=m, n=n, params=par, sector=0),
@@ -92,9 +112,15 @@ def make_steps():
             energy_rows=res["energy"][:, :3].tolist(),
             trunc_err_rows=res["singular"][:, [0, 1, -1]].tolist(),
             exact=e_exact)
-        print(model, "steps", len(cap.steps), "E", res["energy"][-1, 2], "exact", e_exact)
-    with open(os.path.join(HERE, "energies.json"), "w") as fh:
+        print(model + suffix, "steps", len(cap.steps), "E", res["energy"][-1, 2], "exact",
+              e_exact)
+    with open(os.path.join(HERE, f"energies{suffix}.json"), "w") as fh:
         json.dump(energies, fh, indent=1)
+
+
+def make_steps_pbc():
+    """Per-step fixtures of periodic chains, with the edge pair of every step."""
+    make_steps(RUNS_PBC, "_pbc")
 
 
 def make_microbench():
@@ -147,7 +173,8 @@ def make_z2cubed():
     np.savez_compressed(os.path.join(HERE, "z2cubed.npz"), **arrs)
 
 
-PARTS = {"steps": make_steps, "microbench": make_microbench, "z2cubed": make_z2cubed}
+PARTS = {"steps": make_steps, "microbench": make_microbench, "z2cubed": make_z2cubed,
+         "pbc": make_steps_pbc}
 
 
 def main(parts):

@@ -60,6 +60,40 @@ def test_av_microbench_m64():
     assert close(ctx.av(mb["x"]), mb["ax"])
 
 
+@pytest.mark.parametrize("model", MODELS)
+def test_av_periodic_edge_pair(model):
+    """PBC: both pairs in one plan, from metadata and from the reference's own maps."""
+    for st in load_steps(model, pbc=True):
+        dt = native.C128 if st["complex"] else native.F64
+        ctx = native.Context(dt)
+        ctx.plan_build_pbc(st["lenv"], st["renv"], st["ledge"], st["redge"], st["l_num"],
+                           st["r_num"], st["sector"], st["group_n"], st["fermion"])
+        r, l = ctx.maps()
+        es, re_, le_ = ctx.edge_maps()
+        assert np.array_equal(r, st["rmap"]) and np.array_equal(l, st["lmap"])
+        assert np.array_equal(re_, st["remap"]) and np.array_equal(le_, st["lemap"])
+        assert close(ctx.av(st["x"]), st["ax"])
+        ctx.close()
+        # the drop-in: the reference's task lists and blocks of both pairs
+        def d_store_of(rmap, sizes):
+            d = 0
+            for row in rmap:
+                d = max(d, row[2] + sizes[row[0]] // row[4] * row[3])
+            return d
+        rs, ls = block_sizes(st["renv"][0]), block_sizes(st["lenv"][0])
+        rxs, lxs = block_sizes(st["redge"][0]), block_sizes(st["ledge"][0])
+        ctx = native.Context(dt)
+        ctx.plan_from_maps_pbc(st["x"].size, d_store_of(st["rmap"], rs), st["rmap"],
+                               st["renv"][1], rs, st["lmap"], st["lenv"][1], ls,
+                               d_store_of(st["remap"], rxs), st["remap"], st["redge"][1], rxs,
+                               st["lemap"], st["ledge"][1], lxs)
+        assert close(ctx.av(st["x"]), st["ax"])
+        for prec in (native.PREC_BF16X3, native.PREC_TF32X3):
+            ctx.set_precision(prec)
+            assert close(ctx.av(st["x"]), st["ax"], 5e-5)
+        ctx.close()
+
+
 def test_av_z2cubed():
     """Z2 x Z2 x Z2 (S4E) plans, real and complex, FP64 and split precision."""
     for z in load_z2cubed():

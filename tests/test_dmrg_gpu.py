@@ -40,6 +40,48 @@ def test_dmrg_small_chain_matches_reference_steps(gold, model, dtype):
     print(model, r["seconds"], r["energies"][-1, 0])
 
 
+with open(os.path.join(GOLDEN, "energies_pbc.json")) as fh:
+    GOLD_PBC = json.load(fh)
+
+
+@pytest.mark.parametrize("gold,model,dtype", CASES)
+def test_dmrg_periodic_matches_reference_steps(gold, model, dtype):
+    """PBC build: edge environments carried through every step (src/core.cpp:27-30 and
+    the PBC blocks of the step functions); step energies equal the reference's, the
+    final energy the periodic chain's exact value (XYZ, Potts)."""
+    g = GOLD_PBC[gold]
+    a = g["args"]
+    ctx = native.Context(dtype)
+    ctx.set_boundary(native.BOUNDARY_PERIODIC)
+    r = ctx.dmrg(model, a["L"], a["m"], a["n"], a["params"])
+    ref = np.array(g["energy_rows"])
+    assert len(r["energies"]) == len(ref)
+    assert np.array_equal(r["lr"], ref[:, :2].astype(int))
+    err = np.abs(r["energies"][:, 0] - ref[:, 2]).max()
+    print(model, "pbc", r["energies"][-1, 0], ref[-1, 2], err)
+    assert err < 2e-10 * np.abs(ref[:, 2]).max() + 6e-11
+    if g["exact"] is not None:
+        assert abs(r["energies"][-1, 0] - g["exact"]) < 1e-10 * abs(g["exact"])
+    tr = np.array(g["trunc_err_rows"])
+    assert np.abs(r["trunc"] - tr[:, 2]).max() < 1e-9
+    with pytest.raises(native.DmrgxError, match="periodic"):
+        ctx.adjoint()
+
+
+def test_dmrg_periodic_split_precision():
+    """Split-precision matvecs on a periodic chain reach the FP64 energy."""
+    c64 = native.Context(native.F64)
+    c64.set_boundary(native.BOUNDARY_PERIODIC)
+    r64 = c64.dmrg("xyz_real", 16, 32, 2, [1.0, 0.8, 0.5])
+    ctx = native.Context(native.F64)
+    ctx.set_boundary(native.BOUNDARY_PERIODIC)
+    ctx.set_precision(native.PREC_BF16X3)
+    r = ctx.dmrg("xyz_real", 16, 32, 2, [1.0, 0.8, 0.5])
+    e64, e = r64["energies"][-1, 0], r["energies"][-1, 0]
+    print("pbc split", e, e64)
+    assert abs(e - e64) <= 1e-9 * abs(e64)
+
+
 def test_kitaev_L32_m64_matches_bdg():
     """Config 1: Kitaev chain L=32, t=Delta=1, mu=0.5 (u=0.25), m=64, 6 sweeps."""
     ctx = native.Context(native.F64)

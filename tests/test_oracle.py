@@ -13,7 +13,9 @@ def _ctx(st):
     G = restate.Group(st["group_n"], bool(st["fermion"]))
     le = restate.QT.from_ibuf(*st["lenv"])
     re_ = restate.QT.from_ibuf(*st["renv"])
-    return restate.build_context(G, le, re_, st["l_num"], st["r_num"], st["sector"])
+    lx = restate.QT.from_ibuf(*st["ledge"]) if "ledge" in st else None
+    rx = restate.QT.from_ibuf(*st["redge"]) if "redge" in st else None
+    return restate.build_context(G, le, re_, st["l_num"], st["r_num"], st["sector"], lx, rx)
 
 
 @pytest.mark.parametrize("model", MODELS)
@@ -36,6 +38,36 @@ def test_reference_ritz_pair(model):
         e = np.vdot(v, hv).real
         assert abs(e - st["evals"][0]) < 1e-8 * max(1.0, abs(e))
         assert np.linalg.norm(hv - e * v) < 1e-6 * max(1.0, abs(e))
+
+
+@pytest.mark.parametrize("model", MODELS)
+def test_restatement_periodic_edge_pair(model):
+    """PBC build: remap/lemap of the edge pair and av with both pairs (src/core.cpp:27-30)."""
+    for st in load_steps(model, pbc=True):
+        ctx = _ctx(st)
+        assert np.array_equal(ctx.rmap, st["rmap"]) and np.array_equal(ctx.lmap, st["lmap"])
+        assert np.array_equal(ctx.remap, st["remap"])
+        assert np.array_equal(ctx.lemap, st["lemap"])
+        assert len(st["remap"]) and len(st["lemap"])
+        y = restate.av(ctx, st["x"])
+        assert np.allclose(y, st["ax"], rtol=0, atol=1e-13 * np.abs(st["ax"]).max())
+        # the captured Ritz vector is an eigenvector of the operator with both pairs
+        v = st["evec"] / np.linalg.norm(st["evec"])
+        hv = restate.av(ctx, v)
+        e = np.vdot(v, hv).real
+        assert abs(e - st["evals"][0]) < 1e-8 * max(1.0, abs(e))
+
+
+def test_periodic_energies_pin_reference_runs():
+    """The PBC reference runs end at the periodic chain's exact energy."""
+    with open(os.path.join(GOLDEN, "energies_pbc.json")) as fh:
+        en = json.load(fh)
+    ex = {"xyz": exact.xyz_ed(8, 1.0, 0.8, 0.5, 0, periodic=True),
+          "potts": exact.potts_ed(6, 1.0, 1.0, 0, periodic=True)}
+    for m, e in ex.items():
+        assert abs(en[m]["exact"] - e) < 1e-12
+        assert abs(en[m]["final_energy"] - e) < 2e-10 * abs(e) + 1e-10
+    assert en["kitaev"]["exact"] is None
 
 
 def test_restatement_microbench_m64():

@@ -45,6 +45,19 @@ def test_native_maps_microbench_m64():
     assert np.array_equal(rmap, mb["rmap"]) and np.array_equal(lmap, mb["lmap"])
 
 
+@pytest.mark.parametrize("model", MODELS)
+def test_native_maps_periodic_equal_reference(model):
+    """The edge pair's task lists (src/core.cpp:241-247) of the reference's PBC build."""
+    for st in load_steps(model, pbc=True):
+        n, ds, rmap, lmap, es, remap, lemap = native.build_maps_pbc(
+            st["lenv"][0], st["renv"][0], st["ledge"][0], st["redge"][0], st["l_num"],
+            st["r_num"], st["sector"], st["group_n"], st["fermion"])
+        assert n == st["x"].size
+        assert np.array_equal(rmap, st["rmap"]) and np.array_equal(lmap, st["lmap"])
+        assert np.array_equal(remap, st["remap"]) and np.array_equal(lemap, st["lemap"])
+        assert set(np.unique(lemap[:, 5])) <= {1}  # lemap accumulates (beta = 1)
+
+
 def test_native_maps_z2cubed():
     """group_n = GROUP_Z2CUBED: the reference's S4E fusion rule and parity table."""
     for z in load_z2cubed():
