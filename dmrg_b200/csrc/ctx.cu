@@ -820,6 +820,19 @@ int from_maps_common(dmrgx_ctx* c, int64_t n, int64_t d_store, const int* rmap, 
 }
 }  // namespace
 
+int dmrgx_set_solver(dmrgx_ctx* c, int nev, int ncv, int predict) {
+  ARG_CHECK(c, "null context");
+  ARG_CHECK(nev >= 1 && nev <= 6, "set_solver: nev must be 1..6");
+  ARG_CHECK(ncv == 0 || (ncv > nev && ncv <= 64), "set_solver: ncv must be 0 or nev < ncv <= 64");
+  // a start vector close to the lowest eigenvector spans the other eigenvectors
+  // only weakly: excited values can come out missing or wrong
+  ARG_CHECK(!predict || nev == 1, "set_solver: prediction needs nev = 1");
+  c->eig_nev = nev;
+  c->eig_ncv = ncv;
+  c->predict = predict != 0;
+  return 0;
+}
+
 int dmrgx_set_boundary(dmrgx_ctx* c, int boundary) {
   ARG_CHECK(c, "null context");
   ARG_CHECK(boundary == DMRGX_BOUNDARY_OPEN || boundary == DMRGX_BOUNDARY_PERIODIC,

@@ -112,6 +112,8 @@ struct dmrgx_ctx {
   int64_t n_rmap_main = 0, n_lmap_main = 0, d_store_main = 0;
   int r_blocks_main = 0, l_blocks_main = 0;
   int boundary = 0;    // DMRGX_BOUNDARY_* of dmrgx_dmrg
+  int eig_nev = 6, eig_ncv = 0;  // site-step eigensolver of dmrgx_dmrg (dmrgx_set_solver)
+  bool predict = false;
   std::vector<std::vector<int>> psi_dim, psi_sym;
   int n_store_blocks = 0;
   dmrgx::Stage st1, st2;

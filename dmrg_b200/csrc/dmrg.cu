@@ -27,6 +27,8 @@ namespace dmrgx {
 int plan_build_device(dmrgx_ctx* c, const QTensor& L, const QTensor& R, int l_num, int r_num,
                       int sector, const Group& G, const QTensor* Le = nullptr,
                       const QTensor* Re = nullptr);
+int eigsolve_device(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const double* v0,
+                    double* evals, double* evec, int64_t* info);
 
 namespace {
 
@@ -261,6 +263,13 @@ struct Run {
   // seeded at 0 and L-1 with the drivers' edge operators (src/mps.h add_edge)
   bool pbc = false;
   std::vector<QTPtr> edge;
+  // eigensolver of the site steps: eigenvalues wanted (the reference's NEV = 6,
+  // global.h:21), Krylov basis (0: the reference's 4 nev / 6 nev), prediction
+  int eig_nev = 6, eig_ncv = 0;
+  bool predict = false;
+  QTPtr guess;                               // start vector of the next solve
+  int last_kind = 0, last_center = -1;       // 1 move2right, 2 move2left
+  QTPtr last_psi, last_U, last_V;
   std::map<std::pair<std::vector<int>, int>, QTPtr> edge_ids;  // id(W) by (dims, dir) of leg 1
   // per-step records
   std::vector<int> lr;
@@ -286,17 +295,13 @@ struct Run {
     return rc;
   }
 
-  // lowest state of the current plan -> psi tensor; records energies
+  // lowest state of the current plan -> psi tensor (written by the eigensolver on
+  // the device); records energies.  With a predicted centre (guess) the solve
+  // starts from it, else from the solver's fixed pattern.
   int solve(int l, int r, QTPtr& psi) {
     const double t0 = now();
-    std::vector<double> ev(6);
-    std::vector<double> vec((size_t)c->n * c->f());
+    std::vector<double> ev(std::max(6, eig_nev), 0.0);
     int64_t info[6];
-    int rc = dmrgx_eigsolve(c, 6, 0, 1e-10, 0, nullptr, ev.data(), vec.data(), info);
-    if (rc) {
-      err = std::string("eigsolve: ") + dmrgx_last_error();
-      return rc;
-    }
     psi = std::make_shared<QTensor>();
     psi->m.dims = c->psi_dim;
     psi->m.syms = c->psi_sym;
@@ -310,15 +315,68 @@ struct Run {
       err = "psi layout mismatch";
       return DMRGX_E_STATE;
     }
-    cudaMemcpyAsync(psi->d, vec.data(), sizeof(double) * vec.size(), cudaMemcpyHostToDevice,
-                    E.stream);
-    cudaStreamSynchronize(E.stream);
+    double* v0 = nullptr;
+    if (guess) {
+      // a guess whose blocks do not fit this plan is dropped, not an error
+      if (dalloc(&v0, (size_t)std::max<int64_t>(1, c->n * c->f()), E.stream) != cudaSuccess) {
+        v0 = nullptr;
+      } else if (to_plan(*guess, v0)) {
+        dfree(v0, E.stream);
+        v0 = nullptr;
+        err.clear();
+      }
+      guess.reset();
+    }
+    int rc = eigsolve_device(c, eig_nev, eig_ncv, 1e-10, 0, v0, ev.data(), psi->d, info);
+    if (v0) dfree(v0, E.stream);
+    if (rc) {
+      err = std::string("eigsolve: ") + dmrgx_last_error();
+      return rc;
+    }
     lr.push_back(l);
     lr.push_back(r);
-    for (int q = 0; q < 6; q++) energies.push_back(q < (int)std::min<int64_t>(6, c->n) ? ev[q] : 0.0);
+    const int nrec = (int)std::min<int64_t>(std::min(6, eig_nev), c->n);
+    for (int q = 0; q < 6; q++) energies.push_back(q < nrec ? ev[q] : 0.0);
     matvecs.push_back(info[0]);
     t_eig += now() - t0;
     return 0;
+  }
+
+  // White's wavefunction prediction of the next step's one-site centre from the
+  // last step's psi = U S V (the reference starts every solve from ARPACK's
+  // random vector instead, src/dsaupd.cpp:97):
+  //   right move after a right move (centre c -> c+1):  (U^+ psi) . B_{c+1}
+  //   left move after a left move (centre c -> c-1):    A_{c-1} . (psi V^+)
+  //   turn at a chain end (same centre site):           psi
+  // B_{c+1} / A_{c-1}: the site tensors the previous sweep left there.
+  void remember(int kind, const QTPtr& psi, const QTPtr& U, const QTPtr& V) {
+    last_kind = kind;
+    last_center = center;
+    last_psi = predict ? psi : nullptr;
+    last_U = predict ? U : nullptr;
+    last_V = predict ? V : nullptr;
+  }
+  void predict_center(int kind, int next_center) {
+    guess.reset();
+    if (!predict || !last_psi) return;
+    const double t0 = now();
+    if (kind != last_kind && next_center == last_center) {
+      guess = last_psi;
+    } else if (kind == 1 && last_kind == 1 && next_center == last_center + 1 &&
+               site[next_center]) {
+      auto Uc = qt_copy(E, *last_U);
+      qt_conjugate(E, *Uc);
+      QTPtr sv = qt_contract_mat(E, *Uc, *last_psi, 'T', 'N', 2, err);
+      if (sv) guess = qt_contract_mat(E, *sv, *site[next_center], 'N', 'N', 1, err);
+    } else if (kind == 2 && last_kind == 2 && next_center == last_center - 1 &&
+               site[next_center]) {
+      auto Vc = qt_copy(E, *last_V);
+      qt_conjugate(E, *Vc);
+      QTPtr us = qt_contract_mat(E, *last_psi, *Vc, 'N', 'T', 2, err);
+      if (us) guess = qt_contract_mat(E, *site[next_center], *us, 'N', 'N', 1, err);
+    }
+    if (!guess) err.clear();  // no prediction: the solve starts from the default
+    t_eig += now() - t0;
   }
 
   int svd(const QTensor& psi, int num, int cutoff, QTPtr& U, QTPtr& V) {
@@ -420,6 +478,7 @@ struct Run {
     site[l] = U;
     site[r] = V;
     center = -1;
+    remember(0, nullptr, nullptr, nullptr);
     return env[l] && env[r] ? 0 : DMRGX_E_CUDA;
   }
   // src/core.cpp:182-283
@@ -448,6 +507,7 @@ struct Run {
     site[l] = U;
     site[r] = V;
     center = -1;
+    remember(0, nullptr, nullptr, nullptr);
     return env[l] && env[r] ? 0 : DMRGX_E_CUDA;
   }
   // src/core.cpp:293-378
@@ -462,6 +522,7 @@ struct Run {
     }
     int rc = plan(*le, *env[r], 3, 1, sector, E.G, lx.get(), rx.get());
     if (rc) return fail(rc);
+    predict_center(1, l);
     QTPtr psi, U, V;
     if ((rc = solve(l, r, psi))) return rc;
     if ((rc = svd(*psi, 2, cutoff, U, V))) return rc;
@@ -470,6 +531,7 @@ struct Run {
     site[l] = U;
     center = l;  // psi[a_{l-1}, s_l, b_r]: centre at l, right block from r = l + 1
     cpsi = psi;
+    remember(1, psi, U, V);
     return env[l] ? 0 : DMRGX_E_CUDA;
   }
   // src/core.cpp:388-474
@@ -484,6 +546,7 @@ struct Run {
     }
     int rc = plan(*env[l], *re, 2, 2, sector, E.G, lx.get(), rx.get());
     if (rc) return fail(rc);
+    predict_center(2, r);
     QTPtr psi, U, V;
     if ((rc = solve(l, r, psi))) return rc;
     if ((rc = svd(*psi, 1, cutoff, U, V))) return rc;
@@ -492,6 +555,7 @@ struct Run {
     site[r] = V;
     center = r;  // psi[b_l, s_r, a_{r+1}]: centre at r, left block through l = r - 1
     cpsi = psi;
+    remember(2, psi, U, V);
     return env[r] ? 0 : DMRGX_E_CUDA;
   }
   int fail(int rc) {
@@ -909,6 +973,9 @@ extern "C" int dmrgx_dmrg(dmrgx_ctx* c, int model, int L, int m, int sweeps, int
   }
   R->env.assign(L, nullptr);
   R->site.assign(L, nullptr);
+  R->eig_nev = c->eig_nev;
+  R->eig_ncv = c->eig_ncv;
+  R->predict = c->predict;
   if (c->boundary == DMRGX_BOUNDARY_PERIODIC) {
     // the drivers' edge operators: kitaev.cpp:42-45 H_Kitaev(t, -p, 0),
     // xyz.cpp:39-42 H_XYZ(jx, jy, jz) (no field), potts.cpp:44-47 H_Potts3(0, j, p, t)

@@ -435,6 +435,7 @@ struct Lanczos {
   unsigned* ticket;
   int nblk2;       // blocks of the fused step kernels
   int64_t matvecs = 0, matvecs64 = 0;
+  bool force64 = false;  // this solve runs its Krylov steps on the FP64 matvec
 
   double* col(double* M, int j) { return M + (int64_t)j * len; }
 
@@ -486,7 +487,7 @@ struct Lanczos {
   // one Lanczos step j on the device: v_{j+1}, T[j][j], T[j][j+1]
   // (classical Gram-Schmidt against the whole basis, twice)
   int step(int j) {
-    if (matvec(col(V, j), w, false)) return DMRGX_E_CUDA;
+    if (matvec(col(V, j), w, force64)) return DMRGX_E_CUDA;
     const int k = j + 1;
     if (cplx) {
       lz_dots<true><<<nblk2, RB, 0, s>>>(V, n, k, w, n, part2, ticket, coef, T, tdim, j);
@@ -503,8 +504,24 @@ struct Lanczos {
   }
 };
 
+// the default start vector: a fixed xorshift pattern in [-0.5, 0.5)
+int eigsolve_start_pattern(Lanczos& L) {
+  std::vector<double> hv(L.len);
+  uint64_t x = 0x9E3779B97F4A7C15ull;
+  for (int64_t i = 0; i < L.len; i++) {
+    x ^= x << 13;
+    x ^= x >> 7;
+    x ^= x << 17;
+    hv[i] = (double)(x >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+  }
+  EIG_TRY(cudaMemcpyAsync(L.V, hv.data(), sizeof(double) * L.len, cudaMemcpyHostToDevice, L.s));
+  EIG_TRY(cudaStreamSynchronize(L.s));  // hv is a host temporary
+  return 0;
+}
+
+// v0 / evec: host arrays, or device arrays on the context's device when dev_vecs
 int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const void* v0,
-                  double* evals, void* evec, int64_t* info) {
+                  double* evals, void* evec, int64_t* info, bool dev_vecs) {
   const int64_t n = c->n;
   const bool cplx = c->dtype == DMRGX_C128;
   const int nev_out = nev;
@@ -519,7 +536,7 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
   }
   if (tol <= 0) tol = 1e-10;
   if (maxiter <= 0) maxiter = (int)std::min<int64_t>(3 * n, 1000000);
-  const bool split = c->prec != DMRGX_PREC_FP64;
+  bool split = c->prec != DMRGX_PREC_FP64;
 
   Lanczos L;
   L.c = c;
@@ -537,27 +554,46 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
   const int m = L.m, td = L.tdim;
 
   // start vector: the caller's guess, else a fixed deterministic pattern
+  if (v0 && dev_vecs) {
+    EIG_TRY(cudaMemcpyAsync(L.V, v0, sizeof(double) * L.len, cudaMemcpyDeviceToDevice, L.s));
+  } else if (v0) {
+    EIG_TRY(cudaMemcpyAsync(L.V, v0, sizeof(double) * L.len, cudaMemcpyHostToDevice, L.s));
+    EIG_TRY(cudaStreamSynchronize(L.s));  // the caller's array may go away after the call
+  } else if ((rc = eigsolve_start_pattern(L))) {
+    return rc;
+  }
   {
-    std::vector<double> hv(L.len);
-    if (v0) {
-      std::memcpy(hv.data(), v0, sizeof(double) * L.len);
-    } else {
-      uint64_t x = 0x9E3779B97F4A7C15ull;
-      for (int64_t i = 0; i < L.len; i++) {
-        x ^= x << 13;
-        x ^= x >> 7;
-        x ^= x << 17;
-        hv[i] = (double)(x >> 11) * (1.0 / 9007199254740992.0) - 0.5;
-      }
-    }
-    EIG_TRY(cudaMemcpyAsync(L.V, hv.data(), sizeof(double) * L.len, cudaMemcpyHostToDevice, L.s));
     double nn;
     if ((rc = L.norm2(L.V, nn))) return rc;
+    if (!(nn > 0) && dev_vecs && v0) {
+      // a device guess with no weight in this layout: the default pattern instead
+      if ((rc = eigsolve_start_pattern(L))) return rc;
+      if ((rc = L.norm2(L.V, nn))) return rc;
+    }
     if (!(nn > 0)) {
       set_error("eigsolve: zero start vector");
       return DMRGX_E_ARG;
     }
     vscale<<<L.grid, RB, 0, L.s>>>(L.V, nullptr, 1.0 / std::sqrt(nn), L.V, L.len);
+  }
+  // Split precision from a caller's start vector: when its FP64 residual is
+  // already below kSplitGain, the split Krylov steps (floor ~1e-6) would gain
+  // little before the FP64 defect corrections take over, and every Krylov step
+  // costs its orthogonalisation besides the matvec: run this solve in FP64.
+  if (split && v0) {
+    constexpr double kSplitGain = 1e-3;
+    if (L.matvec(L.V, L.w, true)) return DMRGX_E_CUDA;
+    L.dots(L.V, 1, L.w, -1);
+    double hth[2];
+    EIG_TRY(cudaMemcpyAsync(hth, L.coef, sizeof(hth), cudaMemcpyDeviceToHost, L.s));
+    EIG_TRY(cudaStreamSynchronize(L.s));
+    vresid<<<L.grid, RB, 0, L.s>>>(L.w, L.V, hth[0], L.w, L.len);
+    double rr;
+    if ((rc = L.norm2(L.w, rr))) return rc;
+    if (std::sqrt(std::max(rr, 0.0)) <= kSplitGain * std::fabs(hth[0])) {
+      split = false;
+      L.force64 = true;
+    }
   }
 
   std::vector<double> Th((size_t)td * td, 0.0);
@@ -727,7 +763,8 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
   double nn;
   if ((rc = L.norm2(L.V2, nn))) return rc;
   vscale<<<L.grid, RB, 0, L.s>>>(L.V2, nullptr, 1.0 / std::sqrt(std::max(nn, 1e-300)), L.V2, L.len);
-  EIG_TRY(cudaMemcpyAsync(evec, L.V2, sizeof(double) * L.len, cudaMemcpyDeviceToHost, L.s));
+  EIG_TRY(cudaMemcpyAsync(evec, L.V2, sizeof(double) * L.len,
+                          dev_vecs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, L.s));
   EIG_TRY(cudaStreamSynchronize(L.s));
   if (info) {
     info[0] = L.matvecs;
@@ -745,6 +782,16 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
 }
 
 }  // namespace
+
+// the eigensolver with device start and result vectors (the site steps)
+int eigsolve_device(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const double* v0,
+                    double* evals, double* evec, int64_t* info) {
+  if (!c->has_plan || nev < 1 || c->n < 1) {
+    set_error("eigsolve: no plan, or nev < 1, or empty psi");
+    return DMRGX_E_STATE;
+  }
+  return eigsolve_impl(c, nev, ncv, tol, maxiter, v0, evals, evec, info, true);
+}
 }  // namespace dmrgx
 
 extern "C" int dmrgx_eigsolve(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter,
@@ -766,5 +813,5 @@ extern "C" int dmrgx_eigsolve(dmrgx_ctx* c, int nev, int ncv, double tol, int ma
     dmrgx::set_error(std::string("eigsolve: ") + cudaGetErrorString(e));
     return DMRGX_E_CUDA;
   }
-  return dmrgx::eigsolve_impl(c, nev, ncv, tol, maxiter, v0, evals, evec, info);
+  return dmrgx::eigsolve_impl(c, nev, ncv, tol, maxiter, v0, evals, evec, info, false);
 }

@@ -46,6 +46,7 @@ SIGNATURES = {
     "dmrgx_plan_maps": (_i, [_vp, _ip, _ip]),
     "dmrgx_plan_edge_maps": (_i, [_vp, _ip, _ip]),
     "dmrgx_set_boundary": (_i, [_vp, _i]),
+    "dmrgx_set_solver": (_i, [_vp, _i, _i, _i]),
     "dmrgx_plan_psi_layout": (_i, [_vp, _ip, _i64]),
     "dmrgx_av": (_i, [_vp, _vp, _vp, _i]),
     "dmrgx_av_noalloc": (_i, [_i, _i64, _i64, _ip, _i, _vp, _i64p, _i, _ip, _i, _vp, _i64p, _i,
@@ -245,6 +246,11 @@ class Context:
         _check(lib().dmrgx_plan_edge_maps(self.ptr, _ip(r), _ip(l)))
         return int(info[0]), r[: int(info[1])], l[: int(info[2])]
 
+    def set_solver(self, nev=6, ncv=0, predict=False):
+        """Site-step eigensolver of the next dmrg(): eigenvalues per step, Krylov basis
+        (0: the reference's), White's wavefunction prediction."""
+        _check(lib().dmrgx_set_solver(self.ptr, nev, ncv, int(bool(predict))))
+
     def set_boundary(self, boundary):
         """BOUNDARY_OPEN (default) or BOUNDARY_PERIODIC for the next dmrg()."""
         _check(lib().dmrgx_set_boundary(self.ptr, boundary))
@@ -275,11 +281,13 @@ class Context:
         _check(lib().dmrgx_plan_maps(self.ptr, _ip(r), _ip(l)))
         return r[: self.n_rmap], l[: self.n_lmap]
 
-    def av(self, x):
-        """Host arrays in/out (the reference-facing call)."""
+    def av(self, x, out=None):
+        """Host arrays in/out (the reference-facing call); ``out``: a host array of n
+        elements to write (e.g. page-locked), else a new one."""
         x = np.ascontiguousarray(x, self._np)
         assert x.size == self.n
-        y = np.empty(self.n, self._np)
+        y = np.empty(self.n, self._np) if out is None else out
+        assert y.dtype == self._np and y.size == self.n and y.flags.c_contiguous
         _check(lib().dmrgx_av(self.ptr, x.ctypes.data, y.ctypes.data, MEM_HOST))
         return y
 

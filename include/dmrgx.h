@@ -268,6 +268,20 @@ int dmrgx_dmrg(dmrgx_ctx* ctx, int model, int L, int m, int sweeps, int sector,
  * every step's matvec adds the edge pair.  dmrgx_adjoint and dmrgx_expect
  * refuse a periodic run. */
 int dmrgx_set_boundary(dmrgx_ctx* ctx, int boundary);
+
+/* Eigensolver of the next dmrgx_dmrg's site steps.  New options; the defaults
+ * (6, 0, 0) are the reference's settings.
+ *   nev      1..6 eigenvalues converged per step (the reference's NEV = 6,
+ *            global.h:21); energies past nev are reported as 0
+ *   ncv      Krylov basis size (0: the reference's 4 nev real / 6 nev complex,
+ *            src/dsaupd.cpp:76, src/znaupd.cpp:94)
+ *   predict  1: start every sweep step from White's prediction of the new
+ *            centre (the last step's state carried one site on through the
+ *            site tensors, or the same state at a turn), where the reference
+ *            starts from a random vector (src/dsaupd.cpp:97).  Needs nev = 1: a
+ *            start this close to the lowest eigenvector spans the excited ones
+ *            too weakly for their values to be trusted. */
+int dmrgx_set_solver(dmrgx_ctx* ctx, int nev, int ncv, int predict);
 /* XYZ (models 1 and 3) accept a fourth parameter h: a field h sum_i sigma^z_i,
  * absent from the reference (nparams = 3, or h = 0, is the reference's MPO).
  * The final state of dmrgx_dmrg (MPS site tensors, environments and the one-site

@@ -82,6 +82,42 @@ def test_dmrg_periodic_split_precision():
     assert abs(e - e64) <= 1e-9 * abs(e64)
 
 
+@pytest.mark.parametrize("gold,model,dtype", CASES)
+def test_dmrg_lowest_only_and_prediction_keep_reference_energies(gold, model, dtype):
+    """nev=1 (lowest value only), with and without White's prediction as the start
+    vector: every step's lowest energy is still the reference's; prediction cuts
+    the matvecs."""
+    g = GOLD[gold]
+    a = g["args"]
+    ref = np.array(g["energy_rows"])
+    tol = 2e-10 * np.abs(ref[:, 2]).max() + 6e-11
+    runs = {}
+    for name, kw in (("nev1", dict(nev=1, ncv=12)), ("pred", dict(nev=1, ncv=12, predict=True))):
+        ctx = native.Context(dtype)
+        ctx.set_solver(**kw)
+        r = ctx.dmrg(model, a["L"], a["m"], a["n"], a["params"])
+        assert np.abs(r["energies"][:, 0] - ref[:, 2]).max() < tol, name
+        assert not r["energies"][:, 1:].any()
+        runs[name] = int(r["matvecs"].sum())
+    print(model, "matvecs", runs)
+    assert runs["pred"] < runs["nev1"]
+    with pytest.raises(native.DmrgxError, match="nev = 1"):
+        native.Context(dtype).set_solver(nev=6, predict=True)
+
+
+def test_kitaev_L32_m64_prediction():
+    """Config 1 with the fast solver settings: the BdG energy, far fewer matvecs."""
+    ex = exact.kitaev_bdg(32, 1.0, 1.0, 0.25)
+    ctx = native.Context(native.F64)
+    ctx.set_solver(nev=1, ncv=12, predict=True)
+    r = ctx.dmrg("kitaev", 32, 64, 6, [1.0, 1.0, 0.25])
+    base = native.Context(native.F64).dmrg("kitaev", 32, 64, 6, [1.0, 1.0, 0.25])
+    print("kitaev L32 m64 predicted", r["energies"][-1, 0], ex, r["matvecs"].sum(),
+          base["matvecs"].sum(), r["seconds"], base["seconds"])
+    assert abs(r["energies"][-1, 0] - ex) < 1e-9 * abs(ex)
+    assert r["matvecs"].sum() < 0.5 * base["matvecs"].sum()
+
+
 def test_kitaev_L32_m64_matches_bdg():
     """Config 1: Kitaev chain L=32, t=Delta=1, mu=0.5 (u=0.25), m=64, 6 sweeps."""
     ctx = native.Context(native.F64)
