@@ -203,16 +203,24 @@ def sweep_compare(native, args):
     L = args.sweep_L
     out = {"workload": f"XYZ chain L={L}, m={args.sweep_m}, {args.sweep_n} sweep(s), "
                        "reference dmrg() schedule, real MPO", "runs": {}}
-    arms = [("plain_fp64", native.SCHED_PER_BLOCK, native.PREC_FP64),
-            ("fp64", native.SCHED_GROUPED, native.PREC_FP64)]
+    # the reference's site-step eigensolver (nev=6 from a fixed start), then the
+    # fast settings: lowest value only (nev=1, ncv=12) from White's prediction
+    fast = {"nev": 1, "ncv": 12, "predict": True}
+    arms = [("plain_fp64", native.SCHED_PER_BLOCK, native.PREC_FP64, None),
+            ("fp64", native.SCHED_GROUPED, native.PREC_FP64, None)]
     if args.prec != "fp64":
-        arms.append((args.prec, native.SCHED_GROUPED, prec))
+        arms.append((args.prec, native.SCHED_GROUPED, prec, None))
+    arms.append(("fp64_predicted", native.SCHED_GROUPED, native.PREC_FP64, fast))
+    if args.prec != "fp64":
+        arms.append((args.prec + "_predicted", native.SCHED_GROUPED, prec, fast))
     half = L // 2 - 1          # steps of the closing half sweep
     full = 2 * (L - 2)         # steps of one full sweep
-    for name, sched, p in arms:
+    for name, sched, p, solver in arms:
         c = native.Context(native.F64)
         c.set_schedule(sched)
         c.set_precision(p)
+        if solver:
+            c.set_solver(**solver)
         r = c.dmrg("xyz_real", L, args.sweep_m, args.sweep_n, [1.0, 0.8, 0.5])
         st = c.step_seconds()
         ns = len(st)
@@ -228,6 +236,15 @@ def sweep_compare(native, args):
     out["speedup_vs_plain_fp64"] = runs["plain_fp64"]["sweep_s"] / runs[head]["sweep_s"]
     out["speedup_vs_grouped_fp64"] = runs["fp64"]["sweep_s"] / runs[head]["sweep_s"]
     out["dE_rel_vs_fp64"] = abs(runs[head]["energy"] - runs["fp64"]["energy"]) / abs(runs["fp64"]["energy"])
+    # the fast solver settings against the reference's, same precision, whole schedule
+    fh = head + "_predicted"
+    out["predicted"] = {"solver": fast,
+                        "schedule_speedup_vs_reference_solver":
+                            runs[head]["schedule_s"] / runs[fh]["schedule_s"],
+                        "sweep_speedup_vs_reference_solver":
+                            runs[head]["sweep_s"] / runs[fh]["sweep_s"],
+                        "dE_rel_vs_fp64": abs(runs[fh]["energy"] - runs["fp64"]["energy"])
+                        / abs(runs["fp64"]["energy"])}
     return out
 
 

@@ -322,6 +322,8 @@ int launch_stage(dmrgx_ctx* c, int which) {
 
 }  // namespace
 
+constexpr double kTuneMinFlops = 2e8;  // useful flops of a stage worth tuning
+
 int tune_stage(dmrgx_ctx* c, int which) {
   SplitPlan& sp = c->sp;
   SplitStage& st = which == 1 ? sp.s1 : sp.s2;
@@ -340,33 +342,52 @@ int tune_stage(dmrgx_ctx* c, int which) {
       return configure_stage(c, st, it->second.cfg, it->second.halve, it->second.cap_scale);
     }
   }
+  // a stage this small runs in a few microseconds whatever the tiling: measuring
+  // 18 tilings would cost more than it could save (the small-bond steps near
+  // the chain ends), so it keeps the default
+  {
+    const Stage& fs = which == 1 ? c->st1 : c->st2;
+    double fl = 0;
+    for (const PlainRow& r : fs.rows) fl += 2.0 * r.M * r.N * r.K;
+    if (fl < kTuneMinFlops) {
+      st.tuned = false;
+      return configure_stage(c, st, 0, def_halve, 1.0);
+    }
+  }
   cudaEvent_t e0, e1;
   SP_TRY(cudaEventCreate(&e0));
   SP_TRY(cudaEventCreate(&e1));
   TuneVal best{0, def_halve, 1.0};
   float best_ms = 1e30f;
   int rc = 0;
+  auto trial = [&](int cfg, bool hv, double cs) {
+    rc = configure_stage(c, st, cfg, hv, cs);
+    if (rc) return;
+    rc = launch_stage(c, which);  // warm-up
+    float ms = 1e30f;
+    for (int r = 0; r < 2 && !rc; r++) {
+      cudaEventRecord(e0, c->stream);
+      rc = launch_stage(c, which);
+      cudaEventRecord(e1, c->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = DMRGX_E_CUDA;
+      float t = 0;
+      cudaEventElapsedTime(&t, e0, e1);
+      ms = std::min(ms, t);
+    }
+    if (!rc && ms < best_ms) {
+      best_ms = ms;
+      best = TuneVal{cfg, hv, cs};
+    }
+  };
+  // every configuration and halving with the K-split threshold at its default
+  // and off (1e9), then the other thresholds for the best of those
   for (int cfg = 0; cfg < tc_configs() && !rc; cfg++)
     for (int hv = 0; hv < 2 && !rc; hv++)
-      for (double cs : {1.0, 2.0, 4.0, 1e9}) {  // 1e9: no K-split
-        rc = configure_stage(c, st, cfg, hv != 0, cs);
-        if (rc) break;
-        rc = launch_stage(c, which);  // warm-up
-        float ms = 1e30f;
-        for (int r = 0; r < 3 && !rc; r++) {
-          cudaEventRecord(e0, c->stream);
-          rc = launch_stage(c, which);
-          cudaEventRecord(e1, c->stream);
-          if (cudaEventSynchronize(e1) != cudaSuccess) rc = DMRGX_E_CUDA;
-          float t = 0;
-          cudaEventElapsedTime(&t, e0, e1);
-          ms = std::min(ms, t);
-        }
-        if (!rc && ms < best_ms) {
-          best_ms = ms;
-          best = TuneVal{cfg, hv != 0, cs};
-        }
-      }
+      for (double cs : {1.0, 1e9})
+        if (!rc) trial(cfg, hv != 0, cs);
+  const TuneVal b1 = best;
+  for (double cs : {2.0, 4.0})
+    if (!rc) trial(b1.cfg, b1.halve, cs);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
