@@ -53,6 +53,8 @@ __global__ void __launch_bounds__(64 * RPB) pad_split_kernel(const double* __res
                                                              const PadJob* __restrict__ jobs,
                                                              const PadRow* __restrict__ rows,
                                                              int nrows) {
+  pdl_wait();
+  pdl_launch_dependents();
   const int r = blockIdx.x * RPB + (int)(threadIdx.x >> 6);
   if (r >= nrows) return;
   const PadRow pr = rows[r];
@@ -98,12 +100,14 @@ cudaError_t launch_pad_split(int eb, const double* src, void* dst, const PadJob*
   for (int r0 = 0; r0 < nrows; r0 += 1 << 28) {
     const int n = std::min(nrows - r0, 1 << 28);
     const int blocks = (n + RPB - 1) / RPB;
-    if (eb == 2)
-      pad_split_kernel<2><<<blocks, 64 * RPB, 0, st>>>(src, (uint8_t*)dst, jobs, rows + r0, n);
-    else
-      pad_split_kernel<4><<<blocks, 64 * RPB, 0, st>>>(src, (uint8_t*)dst, jobs, rows + r0, n);
+    const cudaError_t e =
+        eb == 2 ? launch_pdl(pad_split_kernel<2>, blocks, 64 * RPB, 0, st, src, (uint8_t*)dst,
+                             jobs, rows + r0, n)
+                : launch_pdl(pad_split_kernel<4>, blocks, 64 * RPB, 0, st, src, (uint8_t*)dst,
+                             jobs, rows + r0, n);
+    if (e != cudaSuccess) return e;
   }
-  return cudaGetLastError();
+  return cudaSuccess;
 }
 
 }  // namespace dmrgx

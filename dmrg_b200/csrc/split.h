@@ -111,6 +111,33 @@ cudaError_t prepare_tc_gemm();
 // One stage: the warp-specialized TMA/tcgen05 kernel of configuration cfg, CTA c
 // running units [cta_begin[c], cta_begin[c+1]) in order, then the reduction of
 // K-split tiles.
+// Programmatic dependent launch (sm_90+): a kernel launched with launch_pdl may
+// start while the previous kernel on the stream drains; pdl_wait() blocks until
+// that kernel has completed and its writes are visible (a no-op for a plain
+// launch), pdl_launch_dependents() lets the next such kernel start.
+__device__ __forceinline__ void pdl_wait() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
+__device__ __forceinline__ void pdl_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), int grid, int block, size_t smem,
+                       cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 cudaError_t launch_tc_gemm(int eb, bool out_split, int cfg, const CUtensorMap* maps,
                            const SUnit* units, const int* cta_begin, int nctas, const SOut* outs,
                            const SSeg2* segs, void* c_pair, double* c64, float* ws,

@@ -290,6 +290,10 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
+  // programmatic dependent launch: the set-up above may overlap the previous
+  // kernel's tail; operands and outputs are touched only after it completed
+  pdl_wait();
+  pdl_launch_dependents();
   const uint32_t tmem = *tmem_slot;
   const int ubeg = cta_begin[blockIdx.x], uend = cta_begin[blockIdx.x + 1];
 
@@ -497,6 +501,8 @@ __global__ void __launch_bounds__(256)
 split_reduce(const SRed* __restrict__ reds, const SRedBlk* __restrict__ blks,
              const SOut* __restrict__ outs, const float* __restrict__ ws,
              uint8_t* __restrict__ c_pair, double* __restrict__ c64) {
+  pdl_wait();
+  pdl_launch_dependents();
   const SRedBlk b = blks[blockIdx.x];
   const SRed rd = reds[b.red];
   const SOut o = outs[rd.out];
@@ -569,11 +575,13 @@ cudaError_t launch_tc_gemm(int eb, bool out_split, int cfg, const CUtensorMap* m
   const int sm = tc_smem_bytes(cfg);
 #define DMRGX_TC_LAUNCH(EB, OS, TN, STG)                                                      \
   do {                                                                                        \
-    tc_grouped_gemm<EB, OS, TN, STG><<<nctas, THREADS, sm, st>>>(                              \
-        maps, units, cta_begin, outs, segs, (uint8_t*)c_pair, c64, ws, err);                  \
-    if (nredblk > 0)                                                                          \
-      split_reduce<EB, OS><<<nredblk, 256, 0, st>>>(reds, redblk, outs, ws, (uint8_t*)c_pair, \
-                                                   c64);                                      \
+    cudaError_t e_ = launch_pdl(tc_grouped_gemm<EB, OS, TN, STG>, nctas, THREADS, sm, st,      \
+                                maps, units, cta_begin, outs, segs, (uint8_t*)c_pair, c64, ws, \
+                                err);                                                         \
+    if (e_ == cudaSuccess && nredblk > 0)                                                     \
+      e_ = launch_pdl(split_reduce<EB, OS>, nredblk, 256, 0, st, reds, redblk, outs,          \
+                      (const float*)ws, (uint8_t*)c_pair, c64);                               \
+    if (e_ != cudaSuccess) return e_;                                                         \
   } while (0)
   if (cfg == 0) {
     if (eb == 2) {
