@@ -578,8 +578,7 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
   if (rc) return rc;
   rc = run_jobs(eb, (const double*)c->lenv.p, a2, a2_jobs, s);
   if (rc) return rc;
-  // the stage kernels read these images before they wait on the kernel launched
-  // just before them: the images must be complete before any stage launch
+  // images complete before the tuner's timed launches
   SP_TRY(cudaStreamSynchronize(s));
   // ---- operand blocks of the tensor maps
   auto to_req = [&](const std::vector<MapReq>& req, SplitStage& st) {
