@@ -12,7 +12,9 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <fstream>
 #include <map>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -924,31 +926,19 @@ bool mpo_set(int model, const double* par, int f, cudaStream_t st, QTPtr& bulk, 
 
 void free_run(void* p) { delete static_cast<Run*>(p); }
 
-}  // namespace
-}  // namespace dmrgx
-
-using namespace dmrgx;
-
-extern "C" int dmrgx_dmrg(dmrgx_ctx* c, int model, int L, int m, int sweeps, int sector,
-                          const double* params, int nparams, double* energies, double* trunc,
-                          int* steps_lr, int64_t* matvecs, int64_t cap, int64_t* nsteps,
-                          double* seconds) {
-  if (!c || !params || !nsteps || L < 4) {
-    set_error("dmrg: bad arguments (need a context, parameters and L >= 4)");
-    return DMRGX_E_ARG;
-  }
+// A run with the model's MPO on the context's device: what dmrgx_dmrg and
+// dmrgx_load_state share.  nullptr (err set) on bad arguments.
+Run* make_run(dmrgx_ctx* c, int model, int L, int m, int sector, const double* params,
+              int nparams, std::string& err) {
   if (model < 0 || model > 3) {
-    set_error("dmrg: unknown model");
-    return DMRGX_E_ARG;
+    err = "unknown model";
+    return nullptr;
   }
   const bool real_model = model == 0 || model == 3;
   if (real_model != (c->dtype == DMRGX_F64)) {
-    set_error("dmrg: Kitaev and real XYZ run on F64 contexts, XYZ and Potts on C128");
-    return DMRGX_E_ARG;
+    err = "Kitaev and real XYZ run on F64 contexts, XYZ and Potts on C128";
+    return nullptr;
   }
-  if (c->run_free) c->run_free(c->run);
-  c->run = nullptr;
-  c->run_free = nullptr;
   Run* R = new Run;
   R->c = c;
   R->L = L;
@@ -963,16 +953,159 @@ extern "C" int dmrgx_dmrg(dmrgx_ctx* c, int model, int L, int m, int sweeps, int
   for (int i = 0; i < nparams && i < 8; i++) R->par[i] = params[i];
   R->E.G.n = model == 2 ? 3 : 2;
   R->E.G.fermion = model == 0;
-  std::string err;
   cudaSetDevice(c->device);
   if (!mpo_set(model, R->par.data(), c->f(), c->stream, R->bulk, R->ledge, R->redge, nullptr,
                err)) {
     delete R;
-    set_error("dmrg: " + err);
-    return DMRGX_E_CUDA;
+    return nullptr;
   }
   R->env.assign(L, nullptr);
   R->site.assign(L, nullptr);
+  return R;
+}
+
+// ---------------------------------------------------------------- checkpoint
+// Text form of a block-sparse tensor: metadata lines (legs and blocks; sector
+// sizes per leg; directions; block labels), then one line per block in the
+// reference's tensor::write_file format (src/tensor.cpp:249-257: the number of
+// indices, the extents, the values, 32 significant digits; complex values as
+// "(re,im)", std::complex's stream form), which tensor::read_file
+// (src/tensor.cpp:260-271) reads back.
+bool write_qt(std::ostream& o, const QTensor& T, cudaStream_t st) {
+  const QMeta& m = T.m;
+  std::vector<double> v((size_t)T.total() * T.f);
+  if (!v.empty() &&
+      (cudaMemcpyAsync(v.data(), T.d, sizeof(double) * v.size(), cudaMemcpyDeviceToHost, st) !=
+           cudaSuccess ||
+       cudaStreamSynchronize(st) != cudaSuccess))
+    return false;
+  o << m.nleg() << " " << m.syms.size() << "\n";
+  for (auto& d : m.dims) {
+    o << d.size();
+    for (int x : d) o << " " << x;
+    o << "\n";
+  }
+  for (int l = 0; l < m.nleg(); l++) o << (l ? " " : "") << m.dirs[l];
+  o << "\n";
+  for (auto& sy : m.syms) {
+    for (int l = 0; l < m.nleg(); l++) o << (l ? " " : "") << sy[l];
+    o << "\n";
+  }
+  o.precision(32);
+  for (size_t b = 0; b < m.syms.size(); b++) {
+    o << m.nleg();
+    for (int l = 0; l < m.nleg(); l++) o << " " << m.dims[l][m.syms[b][l]];
+    for (int64_t i = T.off[b]; i < T.off[b + 1]; i++) {
+      if (T.f == 2) o << " " << std::complex<double>(v[2 * i], v[2 * i + 1]);
+      else o << " " << v[i];
+    }
+    o << "\n";
+  }
+  return (bool)o;
+}
+
+QTPtr read_qt(std::istream& in, int f, cudaStream_t st, std::string& err) {
+  auto T = std::make_shared<QTensor>();
+  QMeta& m = T->m;
+  int nleg = 0;
+  int64_t nblk = 0;
+  if (!(in >> nleg >> nblk) || nleg < 1 || nleg > 8 || nblk < 0 || nblk > (1 << 24)) {
+    err = "bad tensor header";
+    return nullptr;
+  }
+  m.dims.resize(nleg);
+  for (auto& d : m.dims) {
+    int ns = 0;
+    if (!(in >> ns) || ns < 0 || ns > 4096) {
+      err = "bad sector count";
+      return nullptr;
+    }
+    d.resize(ns);
+    for (int& x : d)
+      if (!(in >> x) || x < 0) {
+        err = "bad sector size";
+        return nullptr;
+      }
+  }
+  m.dirs.resize(nleg);
+  for (int& x : m.dirs)
+    if (!(in >> x)) {
+      err = "bad direction";
+      return nullptr;
+    }
+  m.syms.assign((size_t)nblk, std::vector<int>(nleg));
+  for (auto& sy : m.syms)
+    for (int l = 0; l < nleg; l++)
+      if (!(in >> sy[l]) || sy[l] < 0 || sy[l] >= (int)m.dims[l].size()) {
+        err = "bad block label";
+        return nullptr;
+      }
+  T->f = f;
+  if (T->alloc(st) != cudaSuccess) {
+    err = "allocation failed";
+    return nullptr;
+  }
+  std::vector<double> v((size_t)T->total() * f);
+  for (int64_t b = 0; b < nblk; b++) {
+    int n = 0;
+    if (!(in >> n) || n != nleg) {
+      err = "block index count differs from the tensor's legs";
+      return nullptr;
+    }
+    for (int l = 0; l < nleg; l++) {
+      int e = 0;
+      if (!(in >> e) || e != m.dims[l][m.syms[b][l]]) {
+        err = "block extent differs from its sector size";
+        return nullptr;
+      }
+    }
+    for (int64_t i = T->off[b]; i < T->off[b + 1]; i++) {
+      if (f == 2) {
+        std::complex<double> z;
+        if (!(in >> z)) {
+          err = "bad complex value";
+          return nullptr;
+        }
+        v[2 * i] = z.real();
+        v[2 * i + 1] = z.imag();
+      } else if (!(in >> v[i])) {
+        err = "bad value";
+        return nullptr;
+      }
+    }
+  }
+  if (!v.empty() &&
+      (cudaMemcpyAsync(T->d, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, st) !=
+           cudaSuccess ||
+       cudaStreamSynchronize(st) != cudaSuccess)) {
+    err = "upload failed";
+    return nullptr;
+  }
+  return T;
+}
+
+}  // namespace
+}  // namespace dmrgx
+
+using namespace dmrgx;
+
+extern "C" int dmrgx_dmrg(dmrgx_ctx* c, int model, int L, int m, int sweeps, int sector,
+                          const double* params, int nparams, double* energies, double* trunc,
+                          int* steps_lr, int64_t* matvecs, int64_t cap, int64_t* nsteps,
+                          double* seconds) {
+  if (!c || !params || !nsteps || L < 4) {
+    set_error("dmrg: bad arguments (need a context, parameters and L >= 4)");
+    return DMRGX_E_ARG;
+  }
+  if (c->run_free) c->run_free(c->run);
+  c->run = nullptr;
+  c->run_free = nullptr;
+  std::string err;
+  Run* R = make_run(c, model, L, m, sector, params, nparams, err);
+  if (!R) {
+    set_error("dmrg: " + err);
+    return DMRGX_E_ARG;
+  }
   R->eig_nev = c->eig_nev;
   R->eig_ncv = c->eig_ncv;
   R->predict = c->predict;
@@ -1151,5 +1284,136 @@ extern "C" int dmrgx_run_seconds(dmrgx_ctx* c, double* out, int cap) {
   out[3] = R->t_env;
   out[4] = R->t_fuse;
   out[5] = R->t_plan;
+  return 0;
+}
+
+extern "C" int dmrgx_save_state(dmrgx_ctx* c, const char* path) {
+  if (!c || !path) {
+    set_error("save_state: null argument");
+    return DMRGX_E_ARG;
+  }
+  if (!c->run) {
+    set_error("save_state: no state (run dmrgx_dmrg or dmrgx_load_state first)");
+    return DMRGX_E_STATE;
+  }
+  Run* R = static_cast<Run*>(c->run);
+  if (R->pbc) {
+    set_error("save_state: periodic chains are not supported");
+    return DMRGX_E_STATE;
+  }
+  if (R->center < 0 || !R->cpsi) {
+    set_error("save_state: the last step left no one-site centre");
+    return DMRGX_E_STATE;
+  }
+  std::ofstream o(path);
+  if (!o) {
+    set_error(std::string("save_state: cannot open ") + path);
+    return DMRGX_E_ARG;
+  }
+  const double e0 = R->energies.empty() ? 0.0 : R->energies[R->energies.size() - 6];
+  o.precision(17);
+  o << "dmrgx-mps 1\n";
+  o << "model " << R->model << " L " << R->L << " sector " << R->sector << " m " << R->m_cut
+    << " center " << R->center << " f " << c->f() << " energy " << e0 << "\n";
+  o << "params " << R->par.size();
+  for (double p : R->par) o << " " << p;
+  o << "\n";
+  bool ok = true;
+  for (int k = 0; k < R->L && ok; k++) {
+    if (k == R->center || !R->site[k]) continue;
+    o << "site " << k << "\n";
+    ok = write_qt(o, *R->site[k], c->stream);
+    o.precision(17);
+  }
+  if (ok) {
+    o << "centre\n";
+    ok = write_qt(o, *R->cpsi, c->stream);
+  }
+  o << "end\n";
+  if (!ok || !o) {
+    set_error(std::string("save_state: writing ") + path + " failed");
+    return DMRGX_E_CUDA;
+  }
+  return 0;
+}
+
+extern "C" int dmrgx_load_state(dmrgx_ctx* c, const char* path) {
+  if (!c || !path) {
+    set_error("load_state: null argument");
+    return DMRGX_E_ARG;
+  }
+  std::ifstream in(path);
+  if (!in) {
+    set_error(std::string("load_state: cannot open ") + path);
+    return DMRGX_E_ARG;
+  }
+  std::string tag, k1, k2, k3, k4, k5, k6, k7;
+  int ver = 0, model = -1, L = 0, sector = 0, m = 0, center = -1, f = 0, np = 0;
+  double e0 = 0;
+  if (!(in >> tag >> ver) || tag != "dmrgx-mps" || ver != 1 ||
+      !(in >> k1 >> model >> k2 >> L >> k3 >> sector >> k4 >> m >> k5 >> center >> k6 >> f >>
+        k7 >> e0) ||
+      k1 != "model" || k2 != "L" || k5 != "center" || !(in >> tag >> np) || tag != "params" ||
+      np < 0 || np > 8 || L < 4 || center < 0 || center >= L) {
+    set_error("load_state: not a dmrgx state file (bad header)");
+    return DMRGX_E_ARG;
+  }
+  if (f != c->f()) {
+    set_error("load_state: element type of the file differs from the context's");
+    return DMRGX_E_ARG;
+  }
+  std::vector<double> par((size_t)np);
+  for (double& p : par)
+    if (!(in >> p)) {
+      set_error("load_state: bad parameters");
+      return DMRGX_E_ARG;
+    }
+  std::string err;
+  Run* R = make_run(c, model, L, m, sector, par.data(), np, err);
+  if (!R) {
+    set_error("load_state: " + err);
+    return DMRGX_E_ARG;
+  }
+  int rc = 0;
+  for (;;) {
+    if (!(in >> tag)) {
+      err = "truncated file";
+      break;
+    }
+    if (tag == "end") break;
+    if (tag == "site") {
+      int k = -1;
+      if (!(in >> k) || k < 0 || k >= L) {
+        err = "bad site index";
+        break;
+      }
+      R->site[k] = read_qt(in, f, c->stream, err);
+      if (!R->site[k]) break;
+    } else if (tag == "centre") {
+      R->cpsi = read_qt(in, f, c->stream, err);
+      if (!R->cpsi) break;
+    } else {
+      err = "unknown record " + tag;
+      break;
+    }
+  }
+  if (tag == "end" && err.empty() && !R->cpsi) err = "no centre tensor";
+  if (tag == "end" && err.empty()) {
+    R->center = center;
+    R->energies.assign(6, 0.0);
+    R->energies[0] = e0;
+    std::vector<QTPtr> ev;
+    rc = R->rebuild(R->bulk, R->ledge, R->redge, ev);
+    if (!rc) R->env = ev;
+    else err = R->err;
+  }
+  if (!err.empty() || rc) {
+    delete R;
+    set_error("load_state: " + (err.empty() ? std::string("environment rebuild failed") : err));
+    return rc ? rc : DMRGX_E_ARG;
+  }
+  if (c->run_free) c->run_free(c->run);
+  c->run = R;
+  c->run_free = free_run;
   return 0;
 }

@@ -47,6 +47,8 @@ SIGNATURES = {
     "dmrgx_plan_edge_maps": (_i, [_vp, _ip, _ip]),
     "dmrgx_set_boundary": (_i, [_vp, _i]),
     "dmrgx_set_solver": (_i, [_vp, _i, _i, _i]),
+    "dmrgx_save_state": (_i, [_vp, C.c_char_p]),
+    "dmrgx_load_state": (_i, [_vp, C.c_char_p]),
     "dmrgx_plan_psi_layout": (_i, [_vp, _ip, _i64]),
     "dmrgx_av": (_i, [_vp, _vp, _vp, _i]),
     "dmrgx_av_noalloc": (_i, [_i, _i64, _i64, _ip, _i, _vp, _i64p, _i, _ip, _i, _vp, _i64p, _i,
@@ -245,6 +247,14 @@ class Context:
         l = np.zeros((max(1, int(info[2])), 7), np.int32)
         _check(lib().dmrgx_plan_edge_maps(self.ptr, _ip(r), _ip(l)))
         return int(info[0]), r[: int(info[1])], l[: int(info[2])]
+
+    def save_state(self, path):
+        """Write the state of the last dmrg() (site tensors, centre) to a text file."""
+        _check(lib().dmrgx_save_state(self.ptr, os.fsencode(path)))
+
+    def load_state(self, path):
+        """Read a state written by save_state; adjoint() and expect() then apply to it."""
+        _check(lib().dmrgx_load_state(self.ptr, os.fsencode(path)))
 
     def set_solver(self, nev=6, ncv=0, predict=False):
         """Site-step eigensolver of the next dmrg(): eigenvalues per step, Krylov basis

@@ -322,6 +322,20 @@ int dmrgx_adjoint(dmrgx_ctx* ctx, int recompute, double* dE_dparams, int nparams
                   double* dE_dW, int64_t w_cap, int64_t* w_len, double* checks,
                   double* seconds);
 
+/* Checkpoint of the state after dmrgx_dmrg (new work; the reference has no MPS
+ * file format, only tensor::write_file / read_file for one dense tensor,
+ * src/tensor.cpp:249-296).  Text file: a header (model, L, sector, m, centre
+ * site, element type, final energy, model parameters), then every site tensor
+ * left and right of the one-site centre and the centre tensor, each as its
+ * block metadata followed by one line per block in tensor::write_file's format
+ * (index count, extents, values at 32 significant digits; complex "(re,im)").
+ * dmrgx_load_state reads such a file into a context of the same element type,
+ * builds the model's MPO and the environments from the site tensors, and
+ * leaves the state for dmrgx_adjoint / dmrgx_expect / dmrgx_save_state.  Open
+ * chains only. */
+int dmrgx_save_state(dmrgx_ctx* ctx, const char* path);
+int dmrgx_load_state(dmrgx_ctx* ctx, const char* path);
+
 /* <Psi|H(params)|Psi> of the current state of the last dmrgx_dmrg for the same
  * model with other parameters (the reference's calc(mps, mpo),
  * src/functions.cpp:469-511, on the device): environments rebuilt from the MPS

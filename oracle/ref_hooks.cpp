@@ -187,6 +187,30 @@ extern "C" void* oref_pv_env(int is_complex, void* pv, int which)
   return pv_env_t((lanczos<double>*)pv, which);
 }
 
+/* ---- one dense tensor through the reference's own reader (src/tensor.cpp:285-296):
+   reads the first tensor of the file at path; returns the number of values read
+   (extents in idx, up to icap; values in vals, up to vcap), or -1 ---- */
+template <typename T>
+static long tensor_read_t(const char* path, int* idx, int icap, T* vals, long vcap)
+{
+  ifstream f(path);
+  if (!f.is_open()) return -1;
+  tensor<T> t;
+  t.read_file(f);
+  if (f.fail()) return -1;
+  for (int i = 0; i < (int)t.index_.size() && i < icap; i++) idx[i] = t.index_[i];
+  for (long i = 0; i < (long)t.val_.size() && i < vcap; i++) vals[i] = t.val_[i];
+  return (long)t.val_.size();
+}
+
+extern "C" long oref_tensor_read(int is_complex, const char* path, int* idx, int icap, void* vals,
+                                 long vcap)
+{
+  if (is_complex)
+    return tensor_read_t(path, idx, icap, (complex<double>*)vals, vcap);
+  return tensor_read_t(path, idx, icap, (double*)vals, vcap);
+}
+
 /* ---- qtensor (de)serialisation ---- */
 template <typename T>
 static long qt_ser_t(const qtensor<T>* q, int* ibuf, long ilen, T* vbuf, long vlen)

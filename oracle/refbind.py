@@ -108,6 +108,8 @@ class Ref:
         lib.oref_mpo_tensor.argtypes = [i, dp, i, ip]
         lib.oref_mpo_tensor.restype = vp
         lib.oref_run.argtypes = [i, i, i, i, i, dp, C.c_char_p, i]
+        lib.oref_tensor_read.argtypes = [i, C.c_char_p, ip, i, vp, l]
+        lib.oref_tensor_read.restype = l
 
     # ------------------------------------------------------------------ eigensolver hook
     def _eig_cb(self, n, nev, is_complex, evals_p, evecs_p, pv):
@@ -230,6 +232,18 @@ class Ref:
             sg = np.loadtxt(os.path.join(td, "singular_oracle_.txt"), ndmin=2)
         self.capture = None
         return dict(energy=en, singular=sg, step_e0=list(self.energies_by_step))
+
+    def tensor_read(self, is_complex, path, icap=8, vcap=1 << 20):
+        """The first dense tensor of a text file, read by the reference's
+        tensor<T>::read_file: (extents, values)."""
+        idx = np.zeros(icap, np.int32)
+        vals = np.zeros(vcap, np.complex128 if is_complex else np.float64)
+        n = self.lib.oref_tensor_read(is_complex, os.fsencode(path),
+                                      idx.ctypes.data_as(C.POINTER(C.c_int)), icap,
+                                      vals.ctypes.data, vcap)
+        if n < 0:
+            raise RuntimeError(f"reference read_file failed on {path}")
+        return idx, vals[:n]
 
     def mpo_tensor(self, model: str, params, part=0):
         par = (C.c_double * 8)(*([float(p) for p in params] + [0.0] * (8 - len(params))))

@@ -318,3 +318,77 @@ def av(ctx: MatvecContext, x):
         contract_map(ctx.redge, est, x, ctx.remap, ctx.r_num)
         contract_map(ctx.ledge, out, est, ctx.lemap, ctx.l_num)
     return out
+
+
+# ----------------------------------------------------------------------------- text files
+def _value(tok: str, is_complex: bool):
+    if is_complex:
+        re_, im = tok.strip("()").split(",")
+        return complex(float(re_), float(im))
+    return float(tok)
+
+
+def read_tensor_text(tokens, pos: int, is_complex: bool):
+    """tensor<T>::read_file (src/tensor.cpp:260-271) on a token stream: the number
+    of indices, the extents, then prod(extents) values (std::complex's stream
+    form "(re,im)" for complex).  Returns (extents, values, next position)."""
+    n = int(tokens[pos])
+    ext = [int(t) for t in tokens[pos + 1: pos + 1 + n]]
+    pos += 1 + n
+    cnt = int(np.prod(ext)) if ext else 1
+    vals = np.array([_value(t, is_complex) for t in tokens[pos: pos + cnt]],
+                    np.complex128 if is_complex else np.float64)
+    return ext, vals, pos + cnt
+
+
+def format_tensor_text(ext, vals, is_complex: bool) -> str:
+    """tensor<T>::write_file (src/tensor.cpp:249-257): the same fields, values at 32
+    significant digits."""
+    def fmt(x):
+        return f"{x:.32g}"
+    parts = [str(len(ext))] + [str(e) for e in ext]
+    for v in np.ravel(vals):
+        parts.append(f"({fmt(v.real)},{fmt(v.imag)})" if is_complex else fmt(float(v)))
+    return " ".join(parts)
+
+
+def read_state(path: str):
+    """Parse a dmrgx state file (dmrgx_save_state): header fields, parameters, and
+    every tensor as (QT, per-block extents)."""
+    tok = open(path).read().split()
+    assert tok[0] == "dmrgx-mps" and tok[1] == "1", "not a dmrgx state file"
+    head = {tok[i]: tok[i + 1] for i in range(2, 16, 2)}  # model L sector m center f energy
+    f = int(head["f"])
+    i = 16
+    assert tok[i] == "params"
+    npar = int(tok[i + 1])
+    params = [float(t) for t in tok[i + 2: i + 2 + npar]]
+    i += 2 + npar
+    tensors = {}
+    while tok[i] != "end":
+        if tok[i] == "site":
+            name, i = f"site{int(tok[i + 1])}", i + 2
+        else:
+            name, i = "centre", i + 1
+        nleg, nblk = int(tok[i]), int(tok[i + 1])
+        i += 2
+        dims = []
+        for _ in range(nleg):
+            ns = int(tok[i])
+            dims.append([int(t) for t in tok[i + 1: i + 1 + ns]])
+            i += 1 + ns
+        dirs = [int(t) for t in tok[i: i + nleg]]
+        i += nleg
+        syms = []
+        for _ in range(nblk):
+            syms.append(tuple(int(t) for t in tok[i: i + nleg]))
+            i += nleg
+        blocks = []
+        for b in range(nblk):
+            ext, vals, i = read_tensor_text(tok, i, f == 2)
+            assert ext == [dims[l][syms[b][l]] for l in range(nleg)]
+            blocks.append(vals.reshape(ext))
+        tensors[name] = QT(dims=dims, dirs=dirs, syms=syms, blocks=blocks)
+    return dict(header={k: (float(v) if k == "energy" else int(v)) for k, v in head.items()},
+                params=params, tensors=tensors)
+

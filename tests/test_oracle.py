@@ -100,6 +100,29 @@ def test_z2cubed_rule():
     assert restate.Group(-8, False).ff(3) == 0
 
 
+def test_tensor_text_format_pinned_to_reference_reader(tmp_path):
+    """The restated tensor::write_file / read_file pair against the reference's own
+    read_file (src/tensor.cpp:260-296), real and complex, including a zero extent."""
+    from oracle import refbind
+    if not refbind.available("xyz"):
+        pytest.skip("oracle/_ref not built in this checkout")
+    R = refbind.Ref("xyz")
+    rng = np.random.default_rng(4)
+    for cplx in (0, 1):
+        for ext in ([3, 1, 4], [2, 5], [1, 0, 2]):
+            v = rng.standard_normal(int(np.prod(ext)))
+            if cplx:
+                v = v + 1j * rng.standard_normal(v.size)
+            v = v * 10.0 ** rng.integers(-12, 12, v.size)
+            line = restate.format_tensor_text(ext, v, bool(cplx))
+            path = tmp_path / f"t{cplx}_{len(ext)}.txt"
+            path.write_text(line + "\n")
+            idx, ref_vals = R.tensor_read(cplx, str(path))
+            e2, mine, _ = restate.read_tensor_text(line.split(), 0, bool(cplx))
+            assert list(idx[: len(ext)]) == ext == e2
+            assert np.array_equal(ref_vals, v) and np.array_equal(mine, v)
+
+
 def test_exact_energies_pin_reference_runs():
     with open(os.path.join(GOLDEN, "energies.json")) as fh:
         en = json.load(fh)
