@@ -1353,7 +1353,8 @@ extern "C" int dmrgx_load_state(dmrgx_ctx* c, const char* path) {
   if (!(in >> tag >> ver) || tag != "dmrgx-mps" || ver != 1 ||
       !(in >> k1 >> model >> k2 >> L >> k3 >> sector >> k4 >> m >> k5 >> center >> k6 >> f >>
         k7 >> e0) ||
-      k1 != "model" || k2 != "L" || k5 != "center" || !(in >> tag >> np) || tag != "params" ||
+      k1 != "model" || k2 != "L" || k3 != "sector" || k4 != "m" || k5 != "center" ||
+      k6 != "f" || k7 != "energy" || !(in >> tag >> np) || tag != "params" ||
       np < 0 || np > 8 || L < 4 || center < 0 || center >= L) {
     set_error("load_state: not a dmrgx state file (bad header)");
     return DMRGX_E_ARG;
