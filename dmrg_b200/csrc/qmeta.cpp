@@ -101,17 +101,29 @@ void generate_dim_sym(const Group& G, const QMeta& lenv, int lnum, const QMeta& 
     sym.push_back(std::vector<int>(dim.size(), 0));
     return;
   }
+  // the reference's order (src/useful.cpp:172-188): left charge s = 0..N-1, then
+  // left tuples, then right tuples, each lexicographic.  The tuples are bucketed
+  // by their charge (order kept within a bucket) instead of rescanning every
+  // pair for every s, which is N |lt| |rt| work (33 M pairs for U(1) in Z_32).
+  std::unordered_map<int, std::vector<int>> lby, rby;
+  for (size_t l = 0; l < lt.size(); l++) lby[lsum[l]].push_back((int)l);
+  for (size_t r = 0; r < rt.size(); r++) rby[rsum[r]].push_back((int)r);
+  size_t count = 0;
   for (int s = 0; s < G.n; s++) {
-    int t = G.ss(sector, -s);
-    for (size_t l = 0; l < lt.size(); l++) {
-      if (lsum[l] != s) continue;
-      for (size_t r = 0; r < rt.size(); r++) {
-        if (rsum[r] != t) continue;
+    auto li = lby.find(s), ri = rby.find(G.ss(sector, -s));
+    if (li != lby.end() && ri != rby.end()) count += li->second.size() * ri->second.size();
+  }
+  sym.reserve(count);
+  for (int s = 0; s < G.n; s++) {
+    const int t = G.ss(sector, -s);
+    auto li = lby.find(s), ri = rby.find(t);
+    if (li == lby.end() || ri == rby.end()) continue;
+    for (int l : li->second)
+      for (int r : ri->second) {
         std::vector<int> v = lt[l];
         v.insert(v.end(), rt[r].begin(), rt[r].end());
-        sym.push_back(v);
+        sym.push_back(std::move(v));
       }
-    }
   }
 }
 
