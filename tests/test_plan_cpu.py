@@ -58,6 +58,25 @@ def test_native_maps_periodic_equal_reference(model):
         assert set(np.unique(lemap[:, 5])) <= {1}  # lemap accumulates (beta = 1)
 
 
+def test_periodic_bookkeeping_errors():
+    st = load_steps("xyz", pbc=True)[0]
+    with pytest.raises(native.DmrgxError, match="out of range"):
+        native.build_maps_pbc(st["lenv"][0], st["renv"][0], st["ledge"][0], st["redge"][0], 9,
+                              st["r_num"], st["sector"], st["group_n"], st["fermion"])
+    bad = np.array(st["ledge"][0], np.int32)
+    bad[-1] = 999  # block label out of range
+    with pytest.raises(native.DmrgxError, match="ledge metadata"):
+        native.build_maps_pbc(st["lenv"][0], st["renv"][0], bad, st["redge"][0], st["l_num"],
+                              st["r_num"], st["sector"], st["group_n"], st["fermion"])
+    # with the edge pair equal to the main pair the edge task lists repeat the main ones,
+    # except that lemap accumulates (beta = 1)
+    n, ds, rmap, lmap, es, remap, lemap = native.build_maps_pbc(
+        st["lenv"][0], st["renv"][0], st["lenv"][0], st["renv"][0], st["l_num"], st["r_num"],
+        st["sector"], st["group_n"], st["fermion"])
+    assert es == ds and np.array_equal(remap, rmap)
+    assert np.array_equal(lemap[:, :5], lmap[:, :5]) and (lemap[:, 5] == 1).all()
+
+
 def test_native_maps_z2cubed():
     """group_n = GROUP_Z2CUBED: the reference's S4E fusion rule and parity table."""
     for z in load_z2cubed():
