@@ -221,7 +221,11 @@ def sweep_compare(native, args):
         c.set_precision(p)
         if solver:
             c.set_solver(**solver)
+        import torch
+        # ncu --nvtx --nvtx-include "sweep_<arm>/" selects one arm's launches
+        torch.cuda.nvtx.range_push("sweep_" + name)
         r = c.dmrg("xyz_real", L, args.sweep_m, args.sweep_n, [1.0, 0.8, 0.5])
+        torch.cuda.nvtx.range_pop()
         st = c.step_seconds()
         ns = len(st)
         last = st[ns - half - full: ns - half] if ns >= half + full else st
