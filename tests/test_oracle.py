@@ -123,6 +123,31 @@ def test_tensor_text_format_pinned_to_reference_reader(tmp_path):
             assert np.array_equal(ref_vals, v) and np.array_equal(mine, v)
 
 
+def test_state_file_reader(tmp_path):
+    """The oracle's reader of dmrgx state files on a hand-made file: header fields,
+    parameters, block metadata and one block line per block (tensor::write_file)."""
+    blk = restate.format_tensor_text([2, 1, 3], np.arange(6.0) - 2.5, False)
+    zero = restate.format_tensor_text([1, 0, 3], np.zeros(0), False)
+    text = "\n".join([
+        "dmrgx-mps 1",
+        "model 3 L 4 sector 0 m 8 center 1 f 1 energy -1.25",
+        "params 3 1 0.8 0.5",
+        "centre",
+        "3 2", "2 2 1", "2 1 0", "1 3", "0 0 0",
+        "0 0 0", "1 1 0",
+        blk, zero,
+        "end", ""])
+    path = tmp_path / "s.txt"
+    path.write_text(text)
+    st = restate.read_state(str(path))
+    assert st["header"] == dict(model=3, L=4, sector=0, m=8, center=1, f=1, energy=-1.25)
+    assert st["params"] == [1.0, 0.8, 0.5]
+    q = st["tensors"]["centre"]
+    assert q.dims == [[2, 1], [1, 0], [3]] and q.syms == [(0, 0, 0), (1, 1, 0)]
+    assert np.array_equal(q.blocks[0].ravel(), np.arange(6.0) - 2.5)
+    assert q.blocks[1].size == 0
+
+
 def test_exact_energies_pin_reference_runs():
     with open(os.path.join(GOLDEN, "energies.json")) as fh:
         en = json.load(fh)
