@@ -229,8 +229,12 @@ def sweep_compare(native, args):
         st = c.step_seconds()
         ns = len(st)
         last = st[ns - half - full: ns - half] if ns >= half + full else st
+        sp = c.step_split()
+        lsp = sp[ns - half - full: ns - half] if ns >= half + full else sp
         out["runs"][name] = {"schedule_s": float(r["seconds"]["total"]), "steps": ns,
                              "sweep_s": float(np.sum(last)),
+                             "sweep_split_s": dict(zip(("eig", "svd", "env", "fuse", "plan"),
+                                                       lsp.sum(axis=0).tolist())),
                              "energy": float(r["energies"][-1, 0]),
                              "matvecs": int(r["matvecs"].sum()),
                              "split_s": c.run_seconds()}

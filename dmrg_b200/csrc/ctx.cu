@@ -537,7 +537,11 @@ int dmrgx_ctx_create(dmrgx_ctx** out, int dtype, int device) {
     set_error("ctx_create: this library is built for sm_100a (Blackwell B200)");
     return DMRGX_E_CUDA;
   }
-  keep_pool(device);
+  if (e == cudaSuccess && !library_pool(device)) {
+    delete c;
+    set_error("ctx_create: cannot create the library's device memory pool");
+    return DMRGX_E_CUDA;
+  }
   e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete c;

@@ -246,6 +246,9 @@ QTPtr upload(const HostQT& H, int f, cudaStream_t s, std::string& err) {
   return T;
 }
 
+// singular values per step kept for dmrgx_singular (the reference's NSI, global.h)
+constexpr int kSingularRow = 20;
+
 struct Run {
   dmrgx_ctx* c;
   Engine E;
@@ -276,8 +279,12 @@ struct Run {
   // per-step records
   std::vector<int> lr;
   std::vector<double> energies, trunc;
+  std::vector<double> entropy;  // per step, print_singular's S
+  std::vector<double> sv;       // per step, the first 20 singular values (0 past |s|)
+  std::vector<int> nsv;         // per step, |s|
   std::vector<int64_t> matvecs;
   std::vector<double> step_s;  // wall seconds of every step
+  std::vector<double> step_split;  // per step: eigensolver, SVD, env update, fusion, plan
   double t_eig = 0, t_svd = 0, t_env = 0, t_fuse = 0, t_plan = 0;
   std::string err;
 
@@ -385,7 +392,15 @@ struct Run {
     const double t0 = now();
     std::vector<double> s;
     if (qt_svd(E, psi, num, cutoff, U, V, s, err)) return DMRGX_E_CUDA;
-    // truncation error of print_singular (src/useful.cpp:97-101)
+    // print_singular's figures (src/useful.cpp:75-102), same expressions and
+    // summation order: entropy S = -sum s^2 log(s^2 + TOL) over the whole
+    // spectrum (TOL = 1e-10, global.h), the first NSI = 20 values, and the
+    // truncation error 1 - sum_{i < min(cutoff, |s|)} s_i^2
+    double S = 0.0;
+    for (size_t i = 0; i < s.size(); i++) S += -s[i] * s[i] * std::log(s[i] * s[i] + 1e-10);
+    entropy.push_back(S);
+    for (int i = 0; i < kSingularRow; i++) sv.push_back(i < (int)s.size() ? s[i] : 0.0);
+    nsv.push_back((int)s.size());
     double e = 1.0;
     const int64_t k = std::min<int64_t>(cutoff, (int64_t)s.size());
     for (int64_t i = 0; i < k; i++) e -= s[i] * s[i];
@@ -859,8 +874,13 @@ struct Run {
   template <class F>
   int timed(F&& f) {
     const double t0 = now();
+    const double before[5] = {t_eig, t_svd, t_env, t_fuse, t_plan};
     const int r = f();
-    if (!r) step_s.push_back(now() - t0);
+    if (!r) {
+      step_s.push_back(now() - t0);
+      const double after[5] = {t_eig, t_svd, t_env, t_fuse, t_plan};
+      for (int q = 0; q < 5; q++) step_split.push_back(after[q] - before[q]);
+    }
     return r;
   }
 
@@ -1256,6 +1276,37 @@ extern "C" int dmrgx_expect(dmrgx_ctx* c, const double* params, int nparams, dou
     set_error("expect: " + R->err);
     return rc;
   }
+  return 0;
+}
+
+extern "C" int dmrgx_singular(dmrgx_ctx* c, double* entropy, double* s20, int* nsv, int64_t cap,
+                              int64_t* nsteps) {
+  if (!c || !c->run || !nsteps) {
+    set_error("singular: no finished dmrgx_dmrg run on this context");
+    return DMRGX_E_STATE;
+  }
+  Run* R = static_cast<Run*>(c->run);
+  const int64_t ns = (int64_t)R->entropy.size();
+  *nsteps = ns;
+  for (int64_t i = 0; i < ns && i < cap; i++) {
+    if (entropy) entropy[i] = R->entropy[i];
+    if (nsv) nsv[i] = R->nsv[i];
+    if (s20)
+      for (int q = 0; q < kSingularRow; q++) s20[kSingularRow * i + q] = R->sv[kSingularRow * i + q];
+  }
+  return 0;
+}
+
+extern "C" int dmrgx_step_split(dmrgx_ctx* c, double* out, int64_t cap, int64_t* nsteps) {
+  if (!c || !c->run || !nsteps) {
+    set_error("step_split: no finished dmrgx_dmrg run on this context");
+    return DMRGX_E_STATE;
+  }
+  Run* R = static_cast<Run*>(c->run);
+  const int64_t ns = (int64_t)R->step_s.size();
+  *nsteps = ns;
+  for (int64_t i = 0; i < ns && i < cap && out; i++)
+    for (int q = 0; q < 5; q++) out[5 * i + q] = R->step_split[5 * i + q];
   return 0;
 }
 

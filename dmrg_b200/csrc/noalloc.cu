@@ -26,11 +26,14 @@
 // stream, or one call at a time).
 //
 // The array's device address is looked up with cudaGetSymbolAddress once per
-// device, by the first call made while that device is current.  That first call
-// does this set-up, so it should come before any CUDA stream capture.
+// device, by the first call made while that device is current.  Every call
+// uploads its task descriptors from static host buffers that the next call
+// overwrites, so no call may be made while `stream` is being captured into a
+// CUDA graph: such a call returns DMRGX_E_STATE.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -220,6 +223,10 @@ std::string plan_stage(const int* map, int nrows, const int64_t* sizes, int nblk
     const int64_t M = S / K;
     if (in_beg < 0 || in_beg + N * K > in_len) return "task row: input range out of bounds";
     if (out_beg < 0 || out_beg + M * N > out_len) return "task row: output range out of bounds";
+    // descriptor fields are 32-bit: the caller's vector length is not capped
+    // by the scratch size, so a single block's extents are checked here
+    if (M * f > INT32_MAX || N * f > INT32_MAX || K * f > INT32_MAX)
+      return "task row: block extent too large";
     if (M == 0 || N == 0) continue;
     if (out_beg != prev_off) {
       DOut& o = st.outs[st.nouts++];
@@ -292,6 +299,15 @@ extern "C" int dmrgx_av_noalloc(int dtype, int64_t n, int64_t d_store, const int
     set_error("av_noalloc: intermediate of " + std::to_string(d_store * f * 8) +
               " bytes exceeds the fixed 32 MiB scratch; use dmrgx_av with a context");
     return DMRGX_E_ARG;
+  }
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t ce = cudaStreamIsCapturing((cudaStream_t)stream, &cs);
+    if (ce != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+      set_error("av_noalloc: not callable while the stream is being captured (descriptors "
+                "are uploaded from host buffers that the next call reuses)");
+      return ce != cudaSuccess ? DMRGX_E_CUDA : DMRGX_E_STATE;
+    }
   }
   std::lock_guard<std::mutex> lock(g_mu);
   int dev = 0;

@@ -284,13 +284,31 @@ __global__ void rev_cols(const double* __restrict__ src, double* __restrict__ ds
     dst[e] = src[(n - 1 - col) * n * f + rem];
   }
 }
-// Y[:, j] *= sc[j], j < k (real scale)
-__global__ void scale_cols(double* __restrict__ Y, int64_t rows, int k,
-                           const double* __restrict__ sc, int f) {
+// nrm[j] = ||Y[:, j]||_2, j < k (rows x k, column-major, ld rows): one block
+// per column, fixed summation order
+__global__ void col_norms(const double* __restrict__ Y, int64_t rows, int k,
+                          double* __restrict__ nrm, int f) {
+  const int j = blockIdx.x;
+  if (j >= k) return;
+  const double* c = Y + (int64_t)j * rows * f;
+  double acc = 0.0;
+  for (int64_t e = threadIdx.x; e < rows * f; e += blockDim.x) acc += c[e] * c[e];
+  __shared__ double red[256];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) nrm[j] = sqrt(red[0]);
+}
+// Y[:, j] /= nrm[j], j < k
+__global__ void unit_cols(double* __restrict__ Y, int64_t rows, int k,
+                          const double* __restrict__ nrm, int f) {
   const int64_t tot = rows * k * f;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot;
        e += (int64_t)gridDim.x * blockDim.x)
-    Y[e] *= sc[e / (rows * f)];
+    Y[e] /= nrm[e / (rows * f)];
 }
 // ph[j] = R_jj / |R_jj| from the upper triangle of a QR factorisation (ld rows)
 __global__ void qr_phase(const double* __restrict__ Y, int64_t ld, int k, double* __restrict__ ph,
@@ -920,9 +938,11 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
   // for s_j > 1e-13 s_0; a Householder QR of those derived columns makes them
   // orthonormal to working precision (phases restored from R's diagonal) and
   // completes them to a full unitary -- the complement columns the reference
-  // takes from LAPACK's full U / V (src/qtensor.cpp:1221-1252).  Singular values
-  // come out accurate to ~1e-16 s_0^2 / s_j absolutely, so the truncation weight
-  // sum_{discarded} s^2 is exact to ~1e-16 per value.
+  // takes from LAPACK's full U / V (src/qtensor.cpp:1221-1252).  The singular
+  // values are the norms of the derived columns, s_j = |X^H u_j| (or |X v_j|),
+  // computed for every j: a Gram eigenvector is accurate to ~1e-16 in angle,
+  // so the norm is accurate to ~1e-16 s_0 absolutely, where sqrt(lambda_j)
+  // would carry ~1e-16 s_0^2 / s_j (1e-8 s_0 for a zero singular value).
   std::vector<std::vector<double>> S(ns);
   std::vector<double*> Ux(ns, nullptr), Vx(ns, nullptr);
   std::vector<double*> Gm(ns, nullptr), Wd(ns, nullptr);
@@ -994,6 +1014,7 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
   // ---- phase 2: singular values, the derived side, QR completion
   std::vector<int> kk(ns, 0);
   std::vector<double*> taus(ns, nullptr), scs(ns, nullptr), phs(ns, nullptr);
+  std::vector<std::vector<double>> nrm_h(ns);
   if (!fail) {
     int lw2 = 1;
     for (int i = 0; i < ns && !fail; i++) {
@@ -1046,24 +1067,27 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
       double* other = C <= R ? Vx[i] : Ux[i];
       const double* full = C <= R ? Ux[i] : Vx[i];
       const double* X = dM + moff[i] * f;
+      if (dalloc(&scs[i], (size_t)p, E.stream) != cudaSuccess) {
+        fail = true;
+        break;
+      }
+      // derived columns X^H u_j (C <= R) or X v_j (C > R) of all p Gram vectors
+      // into the first p columns of `other` (q x q, ld q); their norms are the
+      // singular values
+      if (C <= R) fail = !gemm(OPH, CUBLAS_OP_N, R, p, C, X, C, full, C, other, R);
+      else fail = !gemm(CUBLAS_OP_N, CUBLAS_OP_N, C, p, R, X, C, full, R, other, C);
+      if (fail) break;
+      col_norms<<<p, 256, 0, E.stream>>>(other, q, p, scs[i], f);
       if (k == 0) {
         eye<<<gridfor((int64_t)q * q), 256, 0, E.stream>>>(other, q, f);
         continue;
       }
-      std::vector<double> inv_s(k);
-      for (int j = 0; j < k; j++) inv_s[j] = 1.0 / S[i][j];
-      if (dalloc(&scs[i], (size_t)k, E.stream) != cudaSuccess ||
-          dalloc(&taus[i], (size_t)k * f, E.stream) != cudaSuccess ||
+      if (dalloc(&taus[i], (size_t)k * f, E.stream) != cudaSuccess ||
           dalloc(&phs[i], (size_t)2 * k, E.stream) != cudaSuccess) {
         fail = true;
         break;
       }
-      cudaMemcpyAsync(scs[i], inv_s.data(), sizeof(double) * k, cudaMemcpyHostToDevice, E.stream);
-      // derived columns into the first k columns of `other` (q x q, ld q)
-      if (C <= R) fail = !gemm(OPH, CUBLAS_OP_N, R, k, C, X, C, full, C, other, R);
-      else fail = !gemm(CUBLAS_OP_N, CUBLAS_OP_N, C, k, R, X, C, full, R, other, C);
-      if (fail) break;
-      scale_cols<<<gridfor((int64_t)q * k * f), 256, 0, E.stream>>>(other, q, k, scs[i], f);
+      unit_cols<<<gridfor((int64_t)q * k * f), 256, 0, E.stream>>>(other, q, k, scs[i], f);
       cusolverStatus_t st =
           cx ? g_sol.z_qrf(t_sol.h, q, k, (cuDoubleComplex*)other, q, (cuDoubleComplex*)taus[i],
                            (cuDoubleComplex*)work, lmax, dinfo + 3 * i + 1)
@@ -1086,7 +1110,19 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
     if (!fail) {
       cudaMemcpyAsync(hinfo.data(), dinfo, sizeof(int) * hinfo.size(), cudaMemcpyDeviceToHost,
                       E.stream);
+      for (int i = 0; i < ns; i++) {
+        nrm_h[i].assign(S[i].size(), 0.0);
+        if (!nrm_h[i].empty() && scs[i])
+          cudaMemcpyAsync(nrm_h[i].data(), scs[i], sizeof(double) * nrm_h[i].size(),
+                          cudaMemcpyDeviceToHost, E.stream);
+      }
       if (cudaStreamSynchronize(E.stream) != cudaSuccess) fail = true;
+      // the column norms replace sqrt(lambda); a value is capped by the one
+      // before it so each sector's list stays descending (the order of the
+      // vectors), which moves a value only between near-equal neighbours
+      for (int i = 0; i < ns && !fail; i++)
+        for (size_t j = 0; j < nrm_h[i].size(); j++)
+          S[i][j] = j ? std::min(nrm_h[i][j], S[i][j - 1]) : nrm_h[i][j];
       for (int i = 0; i < 3 * ns && !fail; i++)
         if (hinfo[i] != 0) {
           err = "svd: cuSOLVER eigensolver / QR failed (info " + std::to_string(hinfo[i]) + ")";

@@ -60,6 +60,8 @@ SIGNATURES = {
     "dmrgx_split_tuning": (_i, [_vp, _ip, _i]),
     "dmrgx_matvec_launches": (_i, [_vp, _ip]),
     "dmrgx_step_seconds": (_i, [_vp, _dp, _i64, _i64p]),
+    "dmrgx_singular": (_i, [_vp, _dp, _dp, _ip, _i64, _i64p]),
+    "dmrgx_step_split": (_i, [_vp, _dp, _i64, _i64p]),
     "dmrgx_run_seconds": (_i, [_vp, _dp, _i]),
     "dmrgx_adjoint": (_i, [_vp, _i, _dp, _i, _dp, _i64, _i64p, _dp, _dp]),
     "dmrgx_expect": (_i, [_vp, _dp, _i, _dp]),
@@ -326,7 +328,9 @@ class Context:
     def dmrg(self, model, L, m, sweeps, params, sector=0, cap=100000):
         """Run the reference dmrg() schedule on the GPU.  model: 'kitaev' (F64
         context), 'xyz' or 'potts' (C128 context).  Returns a dict of per-step
-        arrays (lr, energies[:, 6], trunc, matvecs) and timings."""
+        arrays (lr, energies[:, 6], trunc, entropy, s20[:, 20], nsv, matvecs) and
+        timings: the rows of the reference's energy and singular-value files
+        (src/useful.cpp:54-102) in full precision."""
         code = {"kitaev": 0, "xyz": 1, "potts": 2, "xyz_real": 3}[model]
         par = np.ascontiguousarray(params, np.float64)
         en = np.zeros((cap, 6))
@@ -341,7 +345,13 @@ class Context:
         k = int(ns[0])
         self._L = L
         self._nparams = 3 if code == 0 else min(4, max(3, par.size))
-        return dict(lr=lr[:k], energies=en[:k], trunc=tr[:k], matvecs=mv[:k],
+        ent = np.zeros(max(k, 1))
+        s20 = np.zeros((max(k, 1), 20))
+        nsv = np.zeros(max(k, 1), np.int32)
+        _check(lib().dmrgx_singular(self.ptr, ent.ctypes.data_as(_dp), s20.ctypes.data_as(_dp),
+                                    _ip(nsv), k, _i64p(ns)))
+        return dict(lr=lr[:k], energies=en[:k], trunc=tr[:k], entropy=ent[:k], s20=s20[:k],
+                    nsv=nsv[:k], matvecs=mv[:k],
                     seconds=dict(total=sec[0], eig=sec[1], svd=sec[2], env=sec[3], fuse=sec[4]))
 
     def run_seconds(self):
@@ -356,6 +366,14 @@ class Context:
         _check(lib().dmrgx_step_seconds(self.ptr, None, 0, _i64p(ns)))
         out = np.zeros(max(1, int(ns[0])))
         _check(lib().dmrgx_step_seconds(self.ptr, out.ctypes.data_as(_dp), out.size, _i64p(ns)))
+        return out[:int(ns[0])]
+
+    def step_split(self):
+        """Per-step split of the last dmrg() run: rows (eig, svd, env, fuse, plan) seconds."""
+        ns = np.zeros(1, np.int64)
+        _check(lib().dmrgx_step_split(self.ptr, None, 0, _i64p(ns)))
+        out = np.zeros((max(1, int(ns[0])), 5))
+        _check(lib().dmrgx_step_split(self.ptr, out.ctypes.data_as(_dp), out.shape[0], _i64p(ns)))
         return out[:int(ns[0])]
 
     def adjoint(self, nparams=None, recompute=False, want_w=False):

@@ -208,9 +208,11 @@ int dmrgx_av(dmrgx_ctx* ctx, const void* in, void* out, int mem);
  * device memory, or a loop that cannot afford the device-wide synchronisation
  * that allocation may cause.  Same arithmetic as dmrgx_plan_from_maps followed
  * by dmrgx_av, without a context:
- *   renv/lenv  device arrays, environment blocks packed in the reference's
- *              block order (the values of lanczos<T>::renv / lenv);
- *   rmap/lmap  host arrays, the reference's task lists (7 ints per row);
+ *   renv/lenv  device arrays: each environment's blocks packed one after
+ *              another in block order, every block dense row-major;
+ *   rmap/lmap  host arrays: the task rows of stage 1 (renv applied to `in`)
+ *              and stage 2 (lenv applied to the intermediate), 7 ints per row:
+ *              [block, in offset, out offset, rows, cols, beta, sign];
  *   *_sizes    host arrays, element count of every environment block;
  *   in/out     device arrays of n elements; stream: a cudaStream_t (NULL = legacy
  *              default stream).  The work is queued on `stream`; the call returns
@@ -220,8 +222,10 @@ int dmrgx_av(dmrgx_ctx* ctx, const void* in, void* out, int mem);
  * descriptors), held by every GPU that loads the library until exit.  Larger
  * problems (d_store * element size > 32 MiB, more than 16384 task rows per
  * stage or 65536 blocks per environment) return DMRGX_E_ARG.  The first call on a
- * device looks the array up on that device (make it before any stream
- * capture).  All calls share the array: calls whose GPU work overlaps race. */
+ * device looks the array up on that device.  Every call uploads its descriptors
+ * from host buffers that the next call reuses, so a call made while `stream`
+ * is being captured into a CUDA graph returns DMRGX_E_STATE.  All calls share
+ * the array: calls whose GPU work overlaps race. */
 int dmrgx_av_noalloc(int dtype, int64_t n, int64_t d_store, const int* rmap, int n_rmap,
                      const void* renv, const int64_t* renv_sizes, int n_renv_blocks,
                      const int* lmap, int n_lmap, const void* lenv, const int64_t* lenv_sizes,
@@ -287,10 +291,27 @@ int dmrgx_set_solver(dmrgx_ctx* ctx, int nev, int ncv, int predict);
  * The final state of dmrgx_dmrg (MPS site tensors, environments and the one-site
  * centre of the last step) stays in the context for the two calls below. */
 
+/* The rest of the reference's singular-value rows (print_singular,
+ * src/useful.cpp:75-102) for every step of the last dmrgx_dmrg, in schedule
+ * order (the truncation error is dmrgx_dmrg's trunc):
+ *   entropy  cap values, S = -sum_i s_i^2 log(s_i^2 + 1e-10) over the whole
+ *            spectrum of the step's block SVD (the reference's TOL)
+ *   s20      cap * 20 values, the 20 largest singular values (the reference's
+ *            NSI), descending, 0 past the spectrum's length
+ *   nsv      cap values, the spectrum's length
+ * Each output may be NULL; nsteps gets the step count. */
+int dmrgx_singular(dmrgx_ctx* ctx, double* entropy, double* s20, int* nsv, int64_t cap,
+                   int64_t* nsteps);
+
 /* Wall seconds of every site step of the last dmrgx_dmrg (eigensolver, SVD,
  * environment update and fusion of the step), in schedule order; nsteps gets the
  * count, out (cap values, may be NULL) the times. */
 int dmrgx_step_seconds(dmrgx_ctx* ctx, double* out, int64_t cap, int64_t* nsteps);
+
+/* Per-step time split of the last dmrgx_dmrg (wall seconds), schedule order:
+ * out[5*i..5*i+5) = eigensolver, block SVD, environment update, env (x) MPO
+ * fusion, plan building of step i (cap steps at most; out may be NULL). */
+int dmrgx_step_split(dmrgx_ctx* ctx, double* out, int64_t cap, int64_t* nsteps);
 
 /* Time split of the last dmrgx_dmrg (wall seconds): out[0] all site steps,
  * [1] eigensolver, [2] block SVD, [3] environment update, [4] env (x) MPO fusion,

@@ -633,3 +633,99 @@ extern "C" int oref_run(int model, int L, int m, int n, int sector, const double
   }
   return -1;
 }
+
+/* ---- full-precision record of every step's singular values ----
+   The reference's print_singular (src/useful.cpp:75-102) writes the entropy,
+   the first NSI singular values and the truncation error with ACC decimals.
+   The oracle link wraps it (-Wl,--wrap=<its mangled name>): the wrapper keeps
+   the whole spectrum s the reference's svd returned and the cutoff, then calls
+   the reference's own print_singular, so the output files are unchanged. */
+#define OREF_PS _Z14print_singularRSt14basic_ofstreamIcSt11char_traitsIcEEiiRKSt6vectorIdSaIdEEi
+#define OREF_CAT2(a, b) a##b
+#define OREF_CAT(a, b) OREF_CAT2(a, b)
+
+struct oref_sv_rec {
+  int l, r, cutoff;
+  double entropy, error;  /* print_singular's two sums, same expressions and order */
+  vector<double> s;
+};
+static vector<oref_sv_rec> g_sv_rows;
+
+extern "C" void OREF_CAT(__real_, OREF_PS)(ofstream& data, int l, int r, const vector<double>& s,
+                                           int cutoff);
+extern "C" void OREF_CAT(__wrap_, OREF_PS)(ofstream& data, int l, int r, const vector<double>& s,
+                                           int cutoff)
+{
+  oref_sv_rec row;
+  row.l = l;
+  row.r = r;
+  row.cutoff = cutoff;
+  row.s = s;
+  row.entropy = 0;
+  for (size_t i = 0; i < s.size(); i++) row.entropy += -s[i] * s[i] * log(s[i] * s[i] + TOL);
+  row.error = 1;
+  int c = (int)s.size() < cutoff ? (int)s.size() : cutoff;
+  for (int i = 0; i < c; i++) row.error -= s[i] * s[i];
+  g_sv_rows.push_back(row);
+  OREF_CAT(__real_, OREF_PS)(data, l, r, s, cutoff);
+}
+
+/* The same for print_energy (src/useful.cpp:54-72): every energy row the
+   reference prints, with its values in full precision (val[0..n), n as passed). */
+#define OREF_PE _Z12print_energyRSt14basic_ofstreamIcSt11char_traitsIcEEiiPdi
+struct oref_en_rec {
+  int l, r;
+  vector<double> val;
+};
+static vector<oref_en_rec> g_en_rows;
+
+extern "C" void OREF_CAT(__real_, OREF_PE)(ofstream& data, int l, int r, double* val, int n);
+extern "C" void OREF_CAT(__wrap_, OREF_PE)(ofstream& data, int l, int r, double* val, int n)
+{
+  oref_en_rec row;
+  row.l = l;
+  row.r = r;
+  int k = n < NEV ? n : NEV;
+  row.val.assign(val, val + k);
+  g_en_rows.push_back(row);
+  OREF_CAT(__real_, OREF_PE)(data, l, r, val, n);
+}
+
+extern "C" long oref_en_count() { return (long)g_en_rows.size(); }
+
+/* Energy row i: lr[0..2) = l, r; val (NEV slots, zero past the row's count).
+   Returns the row's value count, or -1. */
+extern "C" long oref_en_row(long i, int* lr, double* val)
+{
+  if (i < 0 || i >= (long)g_en_rows.size()) return -1;
+  const oref_en_rec& row = g_en_rows[i];
+  lr[0] = row.l;
+  lr[1] = row.r;
+  for (int k = 0; k < NEV; k++) val[k] = k < (int)row.val.size() ? row.val[k] : 0.0;
+  return (long)row.val.size();
+}
+
+/* Rows recorded since the last clear. */
+extern "C" long oref_sv_count() { return (long)g_sv_rows.size(); }
+extern "C" void oref_sv_clear()
+{
+  g_sv_rows.clear();
+  g_en_rows.clear();
+}
+
+/* Row i: head[0..3) = l, r, cutoff; se[0..2) = entropy and truncation error in
+   full precision; s (cap values) = the spectrum in the order the reference's svd
+   returned it.  Returns the spectrum's length, or -1. */
+extern "C" long oref_sv_row(long i, int* head, double* se, double* s, long cap)
+{
+  if (i < 0 || i >= (long)g_sv_rows.size()) return -1;
+  const oref_sv_rec& row = g_sv_rows[i];
+  head[0] = row.l;
+  head[1] = row.r;
+  head[2] = row.cutoff;
+  se[0] = row.entropy;
+  se[1] = row.error;
+  long n = (long)row.s.size();
+  for (long k = 0; k < n && k < cap; k++) s[k] = row.s[k];
+  return n;
+}

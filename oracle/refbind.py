@@ -36,9 +36,14 @@ def available(variant: str = "xyz") -> bool:
     return os.path.exists(os.path.join(REFDIR, f"liboref_{variant}.so"))
 
 
-def build(ref: str = "/root/reference") -> None:
-    """Compile oracle/_ref from the reference sources (no-op without them)."""
-    if not os.path.isdir(ref):
+def build(ref: str | None = None) -> None:
+    """Compile oracle/_ref from the reference sources.
+
+    ref: the reference checkout (the directory holding include/ and src/), else
+    the DMRG_REFERENCE environment variable.  No-op when neither names an
+    existing directory (the prebuilt libraries are used as they are)."""
+    ref = ref or os.environ.get("DMRG_REFERENCE")
+    if not ref or not os.path.isdir(ref):
         return
     subprocess.run(["make", "-s", "-C", HERE, f"REF={ref}", "-j8"], check=True)
 
@@ -74,6 +79,7 @@ class Ref:
         _keep.append(self._cb)
         self.lib.oref_set_eig_callback(self._cb)
         self.energies_by_step = []
+        self.evals_by_step = []
 
     @staticmethod
     def _declare(lib):
@@ -110,6 +116,12 @@ class Ref:
         lib.oref_run.argtypes = [i, i, i, i, i, dp, C.c_char_p, i]
         lib.oref_tensor_read.argtypes = [i, C.c_char_p, ip, i, vp, l]
         lib.oref_tensor_read.restype = l
+        lib.oref_sv_count.restype = l
+        lib.oref_sv_row.argtypes = [l, ip, dp, dp, l]
+        lib.oref_sv_row.restype = l
+        lib.oref_en_count.restype = l
+        lib.oref_en_row.argtypes = [l, ip, dp]
+        lib.oref_en_row.restype = l
 
     # ------------------------------------------------------------------ eigensolver hook
     def _eig_cb(self, n, nev, is_complex, evals_p, evecs_p, pv):
@@ -135,6 +147,7 @@ class Ref:
                                         shape=(n * (2 if is_complex else 1),))
             dst[:] = v.view(np.float64) if is_complex else v
             self.energies_by_step.append(float(w[0]))
+            self.evals_by_step.append([float(x) for x in w[:nev]])
             if cap is not None and cap.want is not None:
                 info = self.pv_info(is_complex, pv)
                 if cap.want(cap.count - 1, info):
@@ -210,10 +223,16 @@ class Ref:
 
         Returns dict with 'energy' rows (l, r, E0..E5) and 'singular' rows
         (l, r, S, s0..s19, trunc_err) parsed from the reference's own output files
-        (src/useful.cpp:54-102)."""
+        (src/useful.cpp:54-102), and in full double precision: 'step_e0' /
+        'step_evals' (the eigensolver's values of every step, taken in the znaupd
+        hook), 'en' (every energy row at its print_energy call) and 'sv' (per step: l, r, cutoff, entropy, truncation error and the
+        whole spectrum the reference's svd returned, recorded at its
+        print_singular call)."""
         par = (C.c_double * 8)(*([float(p) for p in params] + [0.0] * (8 - len(params))))
         self.capture = capture
         self.energies_by_step = []
+        self.evals_by_step = []
+        self.lib.oref_sv_clear()
         cwd = os.getcwd()
         with tempfile.TemporaryDirectory() as td:
             os.chdir(td)
@@ -231,7 +250,32 @@ class Ref:
             en = np.loadtxt(os.path.join(td, "energy_oracle_.txt"), ndmin=2)
             sg = np.loadtxt(os.path.join(td, "singular_oracle_.txt"), ndmin=2)
         self.capture = None
-        return dict(energy=en, singular=sg, step_e0=list(self.energies_by_step))
+        return dict(energy=en, singular=sg, step_e0=list(self.energies_by_step),
+                    step_evals=list(self.evals_by_step), sv=self.sv_rows(),
+                    en=self.en_rows())
+
+    def en_rows(self):
+        """The energy rows recorded since the last run, full precision: (l, r, values)."""
+        rows = []
+        lr = (C.c_int * 2)()
+        val = (C.c_double * 6)()
+        for i in range(self.lib.oref_en_count()):
+            n = self.lib.oref_en_row(i, lr, val)
+            rows.append(dict(l=lr[0], r=lr[1], evals=[val[k] for k in range(max(n, 0))]))
+        return rows
+
+    def sv_rows(self):
+        """The full-precision singular-value rows recorded since the last run."""
+        rows = []
+        head = (C.c_int * 3)()
+        se = (C.c_double * 2)()
+        for i in range(self.lib.oref_sv_count()):
+            n = self.lib.oref_sv_row(i, head, se, None, 0)
+            s = np.zeros(max(n, 1))
+            self.lib.oref_sv_row(i, head, se, s.ctypes.data_as(C.POINTER(C.c_double)), n)
+            rows.append(dict(l=head[0], r=head[1], cutoff=head[2], entropy=se[0],
+                             trunc=se[1], s=s[:n]))
+        return rows
 
     def tensor_read(self, is_complex, path, icap=8, vcap=1 << 20):
         """The first dense tensor of a text file, read by the reference's

@@ -27,6 +27,14 @@ oracle/_ref by oracle/Makefile) and records:
                       global.h:14), each step with its edge pair: ledge/redge
                       and the task lists remap/lemap (src/core.cpp:241-247).
 
+  schedule_<name>.npz
+                      every step of a reference dmrg() run in full double
+                      precision (energies, truncation error, entropy, first 20
+                      singular values), recorded at the reference's own
+                      print_energy / print_singular calls: the small runs of
+                      RUNS (small_full) and BASELINE config 2, XYZ L=64 m=256
+                      n=8 (config2; about an hour on 8 host cores).
+
 ``python tests/golden/make_golden.py z2cubed`` regenerates only the named
 fixtures (steps, microbench, z2cubed, pbc); no argument regenerates all of them.
 
@@ -173,12 +181,57 @@ def make_z2cubed():
     np.savez_compressed(os.path.join(HERE, "z2cubed.npz"), **arrs)
 
 
+def record_schedule(name, variant, model, L, m, n, params, sector=0):
+    """Every step of one reference dmrg() run in full double precision.
+
+    Rows in schedule order, taken at the reference's own print_energy and
+    print_singular calls (the oracle link wraps both, oracle/ref_hooks.cpp):
+    (l, r), the six printed eigenvalues, the truncation error and entropy the
+    reference computes (src/useful.cpp:75-102) and its first 20 singular values."""
+    import time
+    R = refbind.Ref(variant)
+    t0 = time.time()
+    res = R.run(model, L, m, n, sector, params)
+    secs = time.time() - t0
+    en, sv = res["en"], res["sv"]
+    assert len(en) == len(sv), (len(en), len(sv))
+    lr = np.array([[e["l"], e["r"]] for e in en], np.int32)
+    assert np.array_equal(lr, np.array([[x["l"], x["r"]] for x in sv], np.int32))
+    evals = np.zeros((len(en), 6))
+    for i, e in enumerate(en):
+        evals[i, :len(e["evals"])] = e["evals"]
+    s20 = np.zeros((len(sv), 20))
+    for i, x in enumerate(sv):
+        k = min(20, len(x["s"]))
+        s20[i, :k] = x["s"][:k]
+    np.savez_compressed(
+        os.path.join(HERE, f"schedule_{name}.npz"), lr=lr, evals=evals,
+        trunc=np.array([x["trunc"] for x in sv]), entropy=np.array([x["entropy"] for x in sv]),
+        cutoff=np.array([x["cutoff"] for x in sv], np.int32), s20=s20,
+        nsv=np.array([len(x["s"]) for x in sv], np.int32),
+        args=np.array([L, m, n, sector], np.int32), params=np.array(params, np.float64),
+        ref_seconds=np.array(secs))
+    print(name, "rows", len(en), "E", evals[-1, 0], "seconds", round(secs, 1))
+
+
+def make_config2():
+    """XYZ L=64, m=256, 8 sweeps, the reference schedule (jx=1, jy=0.8, jz=0.5)."""
+    record_schedule("xyz_L64_m256", "xyz", "xyz", 64, 256, 8, [1.0, 0.8, 0.5])
+
+
+def make_small_full():
+    """Full-precision rows of the small golden runs (same arguments as RUNS)."""
+    for model, (variant, L, m, n, par, gn, ferm, exact_fn) in RUNS.items():
+        record_schedule(f"{model}_L{L}_m{m}", variant, model, L, m, n, par)
+
+
 PARTS = {"steps": make_steps, "microbench": make_microbench, "z2cubed": make_z2cubed,
-         "pbc": make_steps_pbc}
+         "pbc": make_steps_pbc, "small_full": make_small_full, "config2": make_config2}
 
 
 def main(parts):
-    for name in parts or PARTS:
+    # config2 takes about an hour of host time: only when named
+    for name in parts or [p for p in PARTS if p != "config2"]:
         PARTS[name]()
 
 

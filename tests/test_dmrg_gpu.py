@@ -40,6 +40,56 @@ def test_dmrg_small_chain_matches_reference_steps(gold, model, dtype):
     print(model, r["seconds"], r["energies"][-1, 0])
 
 
+def load_schedule(name):
+    """A reference dmrg() run recorded in full precision (make_golden.py record_schedule)."""
+    z = np.load(os.path.join(GOLDEN, f"schedule_{name}.npz"))
+    return {k: z[k] for k in z.files}
+
+
+# Tolerances of the full-precision comparison.  The bar is 1e-10 relative on
+# energies and truncation errors.  A truncation error 1 - sum s_i^2 is a
+# difference of O(1) numbers, so it carries an absolute rounding floor of a few
+# 1e-16 per kept value; 5e-14 covers the few hundred values kept here.  The
+# entropy and the singular values are compared to 1e-10 relative and 1e-13 of
+# s_0 (the largest singular value, 1 for a normalised state).
+E_REL = 1e-10
+TRUNC_REL, TRUNC_ABS = 1e-10, 5e-14
+S_REL, SV_ABS = 1e-10, 1e-13
+
+
+def check_schedule(r, g):
+    """Every step of a GPU run against the reference's full-precision rows."""
+    assert np.array_equal(r["lr"], g["lr"]), "step sequence differs from the reference"
+    e, e_ref = r["energies"][:, 0], g["evals"][:, 0]
+    de = np.abs(e - e_ref) / np.abs(e_ref)
+    assert de.max() <= E_REL, (de.max(), int(de.argmax()))
+    dt = np.abs(r["trunc"] - g["trunc"])
+    assert (dt <= TRUNC_REL * np.abs(g["trunc"]) + TRUNC_ABS).all(), (dt.max(), int(dt.argmax()))
+    ds = np.abs(r["entropy"] - g["entropy"])
+    assert (ds <= S_REL * np.abs(g["entropy"]) + 1e-13).all(), (ds.max(), int(ds.argmax()))
+    dv = np.abs(r["s20"] - g["s20"])
+    assert dv.max() <= SV_ABS, (dv.max(), np.unravel_index(dv.argmax(), dv.shape))
+    assert np.array_equal(r["nsv"], g["nsv"])
+    return de.max(), dt.max(), ds.max(), dv.max()
+
+
+SCHEDULE_CASES = [("kitaev_L8_m16", "kitaev", native.F64), ("xyz_L8_m16", "xyz", native.C128),
+                  ("xyz_L8_m16", "xyz_real", native.F64), ("potts_L6_m27", "potts", native.C128)]
+
+
+@pytest.mark.parametrize("name,model,dtype", SCHEDULE_CASES)
+def test_dmrg_schedule_full_precision(name, model, dtype):
+    """Per step: lowest energy, truncation error, entropy and the first 20
+    singular values (the reference's energy and singular-value rows,
+    src/useful.cpp:54-102) against the reference run recorded in full double
+    precision at its own print_energy / print_singular calls."""
+    g = load_schedule(name)
+    L, m, n, sector = (int(v) for v in g["args"])
+    ctx = native.Context(dtype)
+    r = ctx.dmrg(model, L, m, n, g["params"].tolist(), sector=sector)
+    print(name, model, "max dE/E %.1e dtrunc %.1e dS %.1e ds %.1e" % check_schedule(r, g))
+
+
 with open(os.path.join(GOLDEN, "energies_pbc.json")) as fh:
     GOLD_PBC = json.load(fh)
 

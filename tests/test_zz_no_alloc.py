@@ -32,7 +32,9 @@ def _problem(kind):
         p = load_microbench_m64()
         d_store = p["d_store"]
     else:
-        p = load_steps("xyz")[0]
+        # "xyz": complex, every sign +1; "kitaev": real, fermionic, with rows of
+        # sign -1 in rmap (the signs are applied as the operands are loaded)
+        p = load_steps(kind)[2 if kind == "kitaev" else 0]
         rs = _sizes(p["renv"][0])
         d_store = max(int(r[2] + rs[r[0]] // r[4] * r[3]) for r in p["rmap"])
     p = dict(p)
@@ -72,10 +74,12 @@ def _close(y, ref):
 
 
 def test_noalloc_matches_context_entry_on_consecutive_calls():
-    mb, xyz = _problem("microbench"), _problem("xyz")
+    mb, xyz, kit = _problem("microbench"), _problem("xyz"), _problem("kitaev")
+    assert (kit["rmap"][:, 6] < 0).any()            # the sign branch is exercised
     rng = np.random.default_rng(42)
     calls = []
-    for p in (mb, mb, xyz, mb):                     # repeated, then a different problem, then back
+    # repeated, then other problems (complex; fermionic signs), then back
+    for p in (mb, mb, xyz, kit, kit, mb):
         n = p["x"].size
         x = rng.standard_normal(n)
         if p["dtype"] == native.C128:
@@ -88,9 +92,10 @@ def test_noalloc_matches_context_entry_on_consecutive_calls():
 
 
 def test_noalloc_matches_reference_golden():
-    p = _problem("microbench")
-    for _ in range(2):
-        assert _close(_noalloc_result(p, p["x"]), p["ax"])
+    for kind in ("microbench", "kitaev"):
+        p = _problem(kind)
+        for _ in range(2):
+            assert _close(_noalloc_result(p, p["x"]), p["ax"])
 
 
 def test_noalloc_rejects_oversized_intermediate():
