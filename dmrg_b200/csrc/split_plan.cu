@@ -280,7 +280,8 @@ namespace {
 // (tc_cfg_*: four tile-width / ring-depth / CTAs-per-SM choices), halving of
 // one-tile blocks, K-split threshold x {1, 2, 4, none} -- is timed with CUDA events on the
 // context's stream (best of three launches after one warm-up, on the plan's own
-// buffers) and the fastest is kept for every later plan with the same histogram.
+// buffers) and the fastest is kept for every later plan with the same histogram,
+// and for plans of the same coarse class (stage_class).
 struct TuneVal {
   int cfg;
   bool halve;
@@ -308,6 +309,31 @@ uint64_t stage_key(const SplitStage& st, int eb, int which) {
   return h;
 }
 
+// Coarse class of a stage, for plans whose histograms differ but whose shape is
+// alike (the same chain position a sweep later, a neighbouring site): the
+// half-octave buckets of the number of 128-row output tiles, the total and the
+// longest output's K-tile counts, and the widest output's column count rounded
+// to 64.  A tuning measured for one plan of a class is reused for the others
+// without timing them: along a sweep the exact histograms rarely repeat, and
+// timing every candidate on every new one cost more than it saved.
+uint64_t stage_class(const SplitStage& st, int eb, int which) {
+  int64_t tiles = 0, totkt = 0, maxkt = 0, maxn = 0;
+  for (const auto& o : st.outs) {
+    int64_t kt = 0;
+    for (int q = 0; q < o.seg_count; q++) kt += st.segs[o.seg_begin + q].nkt;
+    tiles += (o.m + 127) / 128;
+    totkt += kt;
+    maxkt = std::max(maxkt, kt);
+    maxn = std::max<int64_t>(maxn, o.n);
+  }
+  auto hb = [](int64_t x) {
+    return (uint64_t)std::lround(2.0 * std::log2((double)std::max<int64_t>(x, 1)));
+  };
+  return (uint64_t)eb | ((uint64_t)which << 4) | (hb(tiles) << 8) | (hb(totkt) << 16) |
+         (hb(maxkt) << 24) | ((uint64_t)rup((int)maxn, 64) << 32);
+}
+std::map<uint64_t, TuneVal> g_tune_class;
+
 int launch_stage(dmrgx_ctx* c, int which) {
   SplitPlan& sp = c->sp;
   SplitStage& st = which == 1 ? sp.s1 : sp.s2;
@@ -334,9 +360,14 @@ int tune_stage(dmrgx_ctx* c, int which) {
     return configure_stage(c, st, 0, def_halve, 1.0);
   }
   const uint64_t key = stage_key(st, sp.eb, which);
+  const uint64_t cls = stage_class(st, sp.eb, which);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(key);
+    if (it == g_tune.end()) {
+      auto ic = g_tune_class.find(cls);
+      if (ic != g_tune_class.end()) it = g_tune.emplace(key, ic->second).first;
+    }
     if (it != g_tune.end()) {
       st.tuned = false;
       return configure_stage(c, st, it->second.cfg, it->second.halve, it->second.cap_scale);
@@ -401,6 +432,7 @@ int tune_stage(dmrgx_ctx* c, int which) {
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[key] = best;
+    g_tune_class[cls] = best;
   }
   rc = configure_stage(c, st, best.cfg, best.halve, best.cap_scale);
   st.tuned = true;

@@ -91,9 +91,11 @@ int dmrgx_matvec_launches(dmrgx_ctx* ctx, int* out);
  * SM), 2 up to 128 with a 3-deep ring and 3 up to 64 with a 4-deep ring (two
  * CTAs per SM); when a
  * plan's block-shape histogram (rows, columns and K-tiles of every output block,
- * rounded) is new, every candidate tiling is timed once on the device and the
- * fastest is cached for later plans (DMRGX_TUNE=0 in the environment turns the
- * tuner off).  out[0..3] stage 1, out[4..7] stage 2: configuration, halving of
+ * rounded) is new and no plan of its coarse class (half-octave buckets of its
+ * tile count, total and longest K, and its widest block) has been tuned, every
+ * candidate tiling is timed once on the device and the fastest is cached for
+ * later plans of that histogram and class (DMRGX_TUNE=0 in the environment
+ * turns the tuner off).  out[0..3] stage 1, out[4..7] stage 2: configuration, halving of
  * one-tile blocks, K-split threshold scale x100 (-100: no K-split), 1 if
  * measured for this plan (0: from the cache).  cap >= 8. */
 int dmrgx_split_tuning(dmrgx_ctx* ctx, int* out, int cap);
