@@ -127,6 +127,9 @@ struct dmrgx_ctx {
 
   bool per_block = false;                       // DMRGX_SCHED_PER_BLOCK: one GEMM per task row
   void* blas = nullptr;                         // cuBLAS handle of the per-block schedule
+  // results of the last dmrgx_svd: U and V (metadata, values) and the spectrum
+  std::vector<int> svd_um, svd_vm;
+  std::vector<double> svd_uv, svd_vv, svd_s;
   void* run = nullptr;                          // state of the last dmrgx_dmrg (MPS, centre)
   void (*run_free)(void*) = nullptr;
 

@@ -1279,6 +1279,70 @@ extern "C" int dmrgx_expect(dmrgx_ctx* c, const double* params, int nparams, dou
   return 0;
 }
 
+extern "C" int dmrgx_svd(dmrgx_ctx* c, const int* meta, const void* vals, int num, int cutoff,
+                         int group_n, int fermion, int64_t* sizes) {
+  if (!c || !meta || !vals || !sizes) {
+    set_error("svd: null argument");
+    return DMRGX_E_ARG;
+  }
+  Engine E;
+  E.stream = c->stream;
+  E.device = c->device;
+  E.num_sms = c->num_sms;
+  E.f = c->f();
+  if (!make_group(group_n, fermion, E.G)) {
+    set_error("svd: group_n must be >= 1 or DMRGX_GROUP_Z2CUBED");
+    return DMRGX_E_ARG;
+  }
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) {
+    set_error(std::string("svd: ") + cudaGetErrorString(e));
+    return DMRGX_E_CUDA;
+  }
+  std::string err;
+  QTPtr A = qt_from_host(E, meta, vals, err);
+  if (!A) {
+    set_error("svd: " + err);
+    return DMRGX_E_ARG;
+  }
+  QTPtr U, V;
+  std::vector<double> sv;
+  if (qt_svd(E, *A, num, cutoff, U, V, sv, err)) {
+    set_error("svd: " + err);
+    return err.rfind("svd: the number", 0) == 0 ? DMRGX_E_ARG : DMRGX_E_CUDA;
+  }
+  if (qt_to_host(*U, c->svd_um, c->svd_uv, c->stream) ||
+      qt_to_host(*V, c->svd_vm, c->svd_vv, c->stream)) {
+    set_error("svd: copy of the results failed");
+    return DMRGX_E_CUDA;
+  }
+  c->svd_s = sv;
+  sizes[0] = (int64_t)c->svd_um.size();
+  sizes[1] = (int64_t)c->svd_uv.size() / c->f();
+  sizes[2] = (int64_t)c->svd_vm.size();
+  sizes[3] = (int64_t)c->svd_vv.size() / c->f();
+  sizes[4] = (int64_t)c->svd_s.size();
+  return 0;
+}
+
+extern "C" int dmrgx_svd_result(dmrgx_ctx* c, int* u_meta, void* u_vals, int* v_meta,
+                                void* v_vals, double* s) {
+  if (!c) {
+    set_error("svd_result: null context");
+    return DMRGX_E_ARG;
+  }
+  if (c->svd_um.empty()) {
+    set_error("svd_result: no dmrgx_svd result on this context");
+    return DMRGX_E_STATE;
+  }
+  if (u_meta) std::memcpy(u_meta, c->svd_um.data(), sizeof(int) * c->svd_um.size());
+  if (u_vals) std::memcpy(u_vals, c->svd_uv.data(), sizeof(double) * c->svd_uv.size());
+  if (v_meta) std::memcpy(v_meta, c->svd_vm.data(), sizeof(int) * c->svd_vm.size());
+  if (v_vals) std::memcpy(v_vals, c->svd_vv.data(), sizeof(double) * c->svd_vv.size());
+  if (s) std::memcpy(s, c->svd_s.data(), sizeof(double) * c->svd_s.size());
+  return 0;
+}
+
 extern "C" int dmrgx_singular(dmrgx_ctx* c, double* entropy, double* s20, int* nsv, int64_t cap,
                               int64_t* nsteps) {
   if (!c || !c->run || !nsteps) {

@@ -101,102 +101,31 @@ __global__ void vdot_final(const double* __restrict__ part, int nblk, int k,
 }
 
 
-// ---------------------------------------------------------------- fused CGS2 step
-// One Lanczos step's reorthogonalisation in three launches instead of ten:
-//   lz_dots      c1 = V^H w                       (T[j][j] += Re c1[j])
-//   lz_sub_dots  w -= V c1, then c2 = V^H w       (T[j][j] += Re c2[j])
-//   lz_sub_norm  w -= V c2, then beta = |w|       (T[j][j+1] = T[j+1][j] = beta)
-// Every block reduces its rows for CH columns at a time in registers (one block
-// reduction per chunk, not per column) and writes partials part[j][block]; the
-// last block to finish (atomic ticket after a fence) sums the partials of every
-// column in block order -- a fixed order, so results do not depend on timing --
-// and resets the ticket.
-constexpr int CH = 8;  // columns per register chunk
+// ---------------------------------------------------------------- CGS2 step, row tiles
+// One Lanczos step's reorthogonalisation in three launches of lz_tile:
+//   MODE 0  c1 = V^H w                        (T[j][j] += Re c1[j])
+//   MODE 1  w -= V c1, then c2 = V^H w        (T[j][j] += Re c2[j])
+//   MODE 2  w -= V c2, then beta = |w|        (T[j][j+1] = T[j+1][j] = beta, inv = 1/beta)
+// The rows are cut into tiles of TR rows.  A block walks the tiles blockIdx.x,
+// +gridDim.x, ...; for each it stages the TR x k slice of the basis and the
+// TR values of w in shared memory (coalesced column reads), so a pass reads
+// the basis from memory exactly once although it uses every value twice
+// (subtract, then dots).  One thread per row subtracts; then warp q sums the
+// columns q, q + 8, ... over the tile into the block's running sums (one warp
+// per column: no atomics).  Block sums go to part[j][block]; the last block to
+// finish (atomic ticket after a fence) adds them up in block order -- a fixed
+// order, so results do not depend on timing -- and resets the ticket.
+constexpr int TR = 128;  // rows per tile (RB >= TR: one thread per row subtracts)
 
-// rows of block b: [b*per, min(n, (b+1)*per))
-__device__ __forceinline__ void lz_rows(int64_t n, int64_t& i0, int64_t& i1) {
-  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
-  i0 = (int64_t)blockIdx.x * per;
-  i1 = min(n, i0 + per);
+// 8-byte asynchronous copy global -> shared; zero-fills when !pred (nothing read)
+__device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc, bool pred) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(sdst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc),
+               "r"(pred ? 8 : 0)
+               : "memory");
 }
-
-// block-wide sums of v[0..2*CH) (pairs); thread 0 gets the results in v
-__device__ __forceinline__ void block_sum(double* v, double (*red)[2 * CH]) {
-  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-#pragma unroll
-  for (int q = 0; q < 2 * CH; q++)
-    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
-  if (lane == 0)
-#pragma unroll
-    for (int q = 0; q < 2 * CH; q++) red[wp][q] = v[q];
-  __syncthreads();
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int q = 0; q < 2 * CH; q++) {
-      double t = 0.0;
-      for (int u = 0; u < RB / 32; u++) t += red[u][q];
-      v[q] = t;
-    }
-  __syncthreads();
-}
-
-// partials of V[:, 0..k)^H w over this block's rows -> part[j][block]
-template <bool CPLX>
-__device__ __forceinline__ void lz_partial_dots(const double* __restrict__ V, int64_t ld, int k,
-                                                const double* w, int64_t i0, int64_t i1,
-                                                double* __restrict__ part,
-                                                double (*red)[2 * CH]) {
-  for (int j0 = 0; j0 < k; j0 += CH) {
-    double acc[2 * CH];
-#pragma unroll
-    for (int q = 0; q < 2 * CH; q++) acc[q] = 0.0;
-    for (int64_t i = i0 + threadIdx.x; i < i1; i += RB) {
-      if (CPLX) {
-        const double wr = w[2 * i], wi = w[2 * i + 1];
-#pragma unroll
-        for (int jj = 0; jj < CH; jj++)
-          if (j0 + jj < k) {
-            const double vr = V[2 * ((j0 + jj) * ld + i)], vi = V[2 * ((j0 + jj) * ld + i) + 1];
-            acc[2 * jj] += vr * wr + vi * wi;
-            acc[2 * jj + 1] += vr * wi - vi * wr;
-          }
-      } else {
-        const double wv = w[i];
-#pragma unroll
-        for (int jj = 0; jj < CH; jj++)
-          if (j0 + jj < k) acc[2 * jj] += V[(j0 + jj) * ld + i] * wv;
-      }
-    }
-    block_sum(acc, red);
-    if (threadIdx.x == 0)
-      for (int jj = 0; jj < CH && j0 + jj < k; jj++) {
-        part[2 * ((int64_t)(j0 + jj) * gridDim.x + blockIdx.x)] = acc[2 * jj];
-        part[2 * ((int64_t)(j0 + jj) * gridDim.x + blockIdx.x) + 1] = acc[2 * jj + 1];
-      }
-  }
-}
-
-// w[i] -= sum_j V[i, j] c[j] over this block's rows
-template <bool CPLX>
-__device__ __forceinline__ void lz_subtract(const double* __restrict__ V, int64_t ld, int k,
-                                            const double* __restrict__ c, double* w, int64_t i0,
-                                            int64_t i1) {
-  for (int64_t i = i0 + threadIdx.x; i < i1; i += RB) {
-    if (CPLX) {
-      double ar = 0.0, ai = 0.0;
-      for (int j = 0; j < k; j++) {
-        const double vr = V[2 * (j * ld + i)], vi = V[2 * (j * ld + i) + 1];
-        ar += vr * c[2 * j] - vi * c[2 * j + 1];
-        ai += vr * c[2 * j + 1] + vi * c[2 * j];
-      }
-      w[2 * i] -= ar;
-      w[2 * i + 1] -= ai;
-    } else {
-      double a = 0.0;
-      for (int j = 0; j < k; j++) a += V[j * ld + i] * c[2 * j];
-      w[i] -= a;
-    }
-  }
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
 // true in the block that finishes last (after all partials are visible)
@@ -231,70 +160,126 @@ __device__ __forceinline__ void lz_final_coef(const double* part, int k, double*
   }
 }
 
-template <bool CPLX>
-__global__ void __launch_bounds__(RB) lz_dots(const double* __restrict__ V, int64_t ld, int k,
-                                              const double* __restrict__ w, int64_t n,
+// dynamic shared memory of lz_tile for k basis columns (bytes)
+__host__ __device__ constexpr size_t lz_tile_smem(int k, bool cplx) {
+  return sizeof(double) * ((size_t)k * TR * (cplx ? 2 : 1) + TR * (cplx ? 2 : 1) + 4 * MAX_NCV +
+                           RB / 32);
+}
+
+template <bool CPLX, int MODE>
+__global__ void __launch_bounds__(RB) lz_tile(const double* __restrict__ V, int64_t ld, int k,
+                                              const double* __restrict__ cin,
+                                              double* __restrict__ w, int64_t n,
                                               double* __restrict__ part, unsigned* ticket,
-                                              double* __restrict__ coef, double* __restrict__ T,
-                                              int tdim, int jt) {
-  __shared__ double red[RB / 32][2 * CH];
-  int64_t i0, i1;
-  lz_rows(n, i0, i1);
-  lz_partial_dots<CPLX>(V, ld, k, w, i0, i1, part, red);
-  if (!lz_last(ticket)) return;
-  lz_final_coef(part, k, coef, T, tdim, jt);
-  if (threadIdx.x == 0) *ticket = 0u;
-}
-
-template <bool CPLX>
-__global__ void __launch_bounds__(RB) lz_sub_dots(const double* __restrict__ V, int64_t ld, int k,
-                                                  const double* __restrict__ cin,
-                                                  double* __restrict__ w, int64_t n,
-                                                  double* __restrict__ part, unsigned* ticket,
-                                                  double* __restrict__ cout,
-                                                  double* __restrict__ T, int tdim, int jt) {
-  __shared__ double red[RB / 32][2 * CH];
-  int64_t i0, i1;
-  lz_rows(n, i0, i1);
-  lz_subtract<CPLX>(V, ld, k, cin, w, i0, i1);
-  lz_partial_dots<CPLX>(V, ld, k, w, i0, i1, part, red);  // own rows: no cross-thread hazard
-  if (!lz_last(ticket)) return;
-  lz_final_coef(part, k, cout, T, tdim, jt);
-  if (threadIdx.x == 0) *ticket = 0u;
-}
-
-template <bool CPLX>
-__global__ void __launch_bounds__(RB) lz_sub_norm(const double* __restrict__ V, int64_t ld, int k,
-                                                  const double* __restrict__ cin,
-                                                  double* __restrict__ w, int64_t n,
-                                                  double* __restrict__ part, unsigned* ticket,
-                                                  double* __restrict__ T, int tdim, int j,
-                                                  double* __restrict__ inv) {
-  __shared__ double red[RB / 32][2 * CH];
-  int64_t i0, i1;
-  lz_rows(n, i0, i1);
-  lz_subtract<CPLX>(V, ld, k, cin, w, i0, i1);
-  double acc[2 * CH];
-#pragma unroll
-  for (int q = 0; q < 2 * CH; q++) acc[q] = 0.0;
-  for (int64_t i = i0 + threadIdx.x; i < i1; i += RB) {
-    if (CPLX) acc[0] += w[2 * i] * w[2 * i] + w[2 * i + 1] * w[2 * i + 1];
-    else acc[0] += w[i] * w[i];
-  }
-  block_sum(acc, red);
-  if (threadIdx.x == 0) part[2 * blockIdx.x] = acc[0];
-  if (!lz_last(ticket)) return;
-  if (threadIdx.x < 32) {
-    double sq = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) sq += __ldcg(part + 2 * b);
-    for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-    if (threadIdx.x == 0) {
-      const double beta = sqrt(fmax(sq, 0.0));
-      T[(int64_t)j * tdim + j + 1] = beta;
-      T[(int64_t)(j + 1) * tdim + j] = beta;
-      inv[0] = beta > 1e-300 ? 1.0 / beta : 0.0;
-      *ticket = 0u;
+                                              double* __restrict__ cout, double* __restrict__ T,
+                                              int tdim, int jt, double* __restrict__ inv) {
+  constexpr int F = CPLX ? 2 : 1;
+  extern __shared__ double smem[];
+  double* sV = smem;                        // column j, element e at sV[j * TR * F + e]
+  double* sw = sV + (size_t)k * TR * F;     // the tile of w
+  double* sc = sw + TR * F;                 // cin (pairs)
+  double* sacc = sc + 2 * MAX_NCV;          // running block sums (pairs)
+  double* sred = sacc + 2 * MAX_NCV;        // per-warp norm partials (MODE 2)
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  if (MODE != 0)
+    for (int t = tid; t < 2 * k; t += RB) sc[t] = cin[t];
+  for (int t = tid; t < 2 * MAX_NCV; t += RB) sacc[t] = 0.0;
+  double nrm = 0.0;  // MODE 2: this thread's sum of |w|^2
+  const int64_t ntiles = (n + TR - 1) / TR;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t i0 = tile * TR;
+    const int len = (int)(n - i0 < TR ? n - i0 : TR) * F;  // doubles of the tile per column
+    __syncthreads();  // the previous tile's readers are done (and sc / sacc are set)
+    // every thread queues all its copies before waiting (memory-level parallelism)
+    for (int t = tid; t < k * TR * F; t += RB) {
+      const int j = t / (TR * F), e = t - j * (TR * F);
+      cp_async8(sV + t, e < len ? V + (int64_t)j * ld * F + i0 * F + e : V, e < len);
     }
+    for (int t = tid; t < TR * F; t += RB) cp_async8(sw + t, t < len ? w + i0 * F + t : w, t < len);
+    cp_async_wait_all();
+    __syncthreads();
+    if (MODE != 0 && tid < TR) {
+      const int r = tid;
+      if (CPLX) {
+        double ar = 0.0, ai = 0.0;
+        for (int j = 0; j < k; j++) {
+          const double vr = sV[(size_t)j * TR * 2 + 2 * r], vi = sV[(size_t)j * TR * 2 + 2 * r + 1];
+          ar += vr * sc[2 * j] - vi * sc[2 * j + 1];
+          ai += vr * sc[2 * j + 1] + vi * sc[2 * j];
+        }
+        const double xr = sw[2 * r] - ar, xi = sw[2 * r + 1] - ai;
+        sw[2 * r] = xr;
+        sw[2 * r + 1] = xi;
+        if (2 * r < len) {
+          w[(i0 + r) * 2] = xr;
+          w[(i0 + r) * 2 + 1] = xi;
+          if (MODE == 2) nrm += xr * xr + xi * xi;
+        }
+      } else {
+        double a = 0.0;
+        for (int j = 0; j < k; j++) a += sV[(size_t)j * TR + r] * sc[2 * j];
+        const double x = sw[r] - a;
+        sw[r] = x;
+        if (r < len) {
+          w[i0 + r] = x;
+          if (MODE == 2) nrm += x * x;
+        }
+      }
+    }
+    __syncthreads();
+    for (int j = wp; MODE != 2 && j < k; j += RB / 32) {
+      double sr = 0.0, si = 0.0;
+      for (int r = lane; r < TR; r += 32) {
+        if (CPLX) {
+          const double vr = sV[(size_t)j * TR * 2 + 2 * r], vi = sV[(size_t)j * TR * 2 + 2 * r + 1];
+          const double xr = sw[2 * r], xi = sw[2 * r + 1];
+          sr += vr * xr + vi * xi;
+          si += vr * xi - vi * xr;
+        } else {
+          sr += sV[(size_t)j * TR + r] * sw[r];
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        si += __shfl_xor_sync(0xffffffffu, si, o);
+      }
+      if (lane == 0) {
+        sacc[2 * j] += sr;
+        sacc[2 * j + 1] += si;
+      }
+    }
+  }
+  __syncthreads();
+  if constexpr (MODE == 2) {
+    for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+    if (lane == 0) sred[wp] = nrm;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.0;
+      for (int q = 0; q < RB / 32; q++) t += sred[q];
+      part[2 * blockIdx.x] = t;
+    }
+    if (!lz_last(ticket)) return;
+    if (tid < 32) {
+      double sq = 0.0;
+      for (int b = tid; b < (int)gridDim.x; b += 32) sq += __ldcg(part + 2 * b);
+      for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+      if (tid == 0) {
+        const double beta = sqrt(fmax(sq, 0.0));
+        T[(int64_t)jt * tdim + jt + 1] = beta;
+        T[(int64_t)(jt + 1) * tdim + jt] = beta;
+        inv[0] = beta > 1e-300 ? 1.0 / beta : 0.0;
+        *ticket = 0u;
+      }
+    }
+  } else {
+    for (int j = tid; j < k; j += RB) {
+      part[2 * ((int64_t)j * gridDim.x + blockIdx.x)] = sacc[2 * j];
+      part[2 * ((int64_t)j * gridDim.x + blockIdx.x) + 1] = sacc[2 * j + 1];
+    }
+    if (!lz_last(ticket)) return;
+    lz_final_coef(part, k, cout, T, tdim, jt);
+    if (tid == 0) *ticket = 0u;
   }
 }
 
@@ -453,7 +438,22 @@ struct Lanczos {
     EIG_TRY(mem.alloc(T, (size_t)tdim * tdim));
     EIG_TRY(mem.alloc(inv, 2));
     EIG_TRY(mem.alloc(Y, (size_t)MAX_NCV * MAX_NCV));
+    for (int k = 1; k <= m; k++) tile_blocks(k);  // before any stream capture
     return 0;
+  }
+  // resident blocks per SM of the row-tile kernels at basis size k (occupancy
+  // calculator, registers and shared memory), cached: the persistent grid is
+  // that many per SM, so no block waits for a second wave
+  int occ[MAX_NCV + 2] = {0};
+  int tile_blocks(int k) {
+    if (!occ[k]) {
+      int b = 1;
+      const size_t sm = lz_tile_smem(k, cplx);
+      cudaError_t e = cplx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lz_tile<true, 1>, RB, sm)
+                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lz_tile<false, 1>, RB, sm);
+      occ[k] = (e == cudaSuccess && b > 0) ? std::min(b, 8) : 1;
+    }
+    return occ[k];
   }
   int matvec(const double* in, double* out, bool fp64) {
     matvecs++;
@@ -489,14 +489,17 @@ struct Lanczos {
   int step(int j) {
     if (matvec(col(V, j), w, force64)) return DMRGX_E_CUDA;
     const int k = j + 1;
+    const size_t sm = lz_tile_smem(k, cplx);
+    const int64_t ntiles = (n + TR - 1) / TR;
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)c->num_sms * tile_blocks(k)));
     if (cplx) {
-      lz_dots<true><<<nblk2, RB, 0, s>>>(V, n, k, w, n, part2, ticket, coef, T, tdim, j);
-      lz_sub_dots<true><<<nblk2, RB, 0, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j);
-      lz_sub_norm<true><<<nblk2, RB, 0, s>>>(V, n, k, coef2, w, n, part2, ticket, T, tdim, j, inv);
+      lz_tile<true, 0><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv);
+      lz_tile<true, 1><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv);
+      lz_tile<true, 2><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv);
     } else {
-      lz_dots<false><<<nblk2, RB, 0, s>>>(V, n, k, w, n, part2, ticket, coef, T, tdim, j);
-      lz_sub_dots<false><<<nblk2, RB, 0, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j);
-      lz_sub_norm<false><<<nblk2, RB, 0, s>>>(V, n, k, coef2, w, n, part2, ticket, T, tdim, j, inv);
+      lz_tile<false, 0><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv);
+      lz_tile<false, 1><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv);
+      lz_tile<false, 2><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv);
     }
     vscale<<<grid, RB, 0, s>>>(w, inv, 0.0, col(V, j + 1), len);
     EIG_TRY(cudaGetLastError());
@@ -519,6 +522,27 @@ int eigsolve_start_pattern(Lanczos& L) {
   return 0;
 }
 
+// opt the row-tile kernels in to the shared memory of the largest basis
+// (MAX_NCV columns, complex), once per process
+bool lz_tile_attrs(const char*& why) {
+  static int done = 0;  // 1 ok, -1 failed
+  static const char* msg = "";
+  if (!done) {
+    const int big = (int)lz_tile_smem(MAX_NCV, true);
+    const int bigr = (int)lz_tile_smem(MAX_NCV, false);
+    cudaError_t e = cudaFuncSetAttribute(lz_tile<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(lz_tile<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(lz_tile<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(lz_tile<false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bigr);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(lz_tile<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bigr);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(lz_tile<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bigr);
+    done = e == cudaSuccess ? 1 : -1;
+    if (e != cudaSuccess) msg = cudaGetErrorString(e);
+  }
+  why = msg;
+  return done == 1;
+}
+
 // v0 / evec: host arrays, or device arrays on the context's device when dev_vecs
 int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const void* v0,
                   double* evals, void* evec, int64_t* info, bool dev_vecs) {
@@ -538,6 +562,7 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
   if (maxiter <= 0) maxiter = (int)std::min<int64_t>(3 * n, 1000000);
   bool split = c->prec != DMRGX_PREC_FP64;
 
+  const char* err_attr = "";
   Lanczos L;
   L.c = c;
   L.cplx = cplx;
@@ -548,7 +573,11 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
   L.s = c->stream;
   L.grid = (int)std::max<int64_t>(1, std::min<int64_t>(c->num_sms * 8, (n + RB - 1) / RB));
   L.nblk = (int)std::max<int64_t>(1, std::min<int64_t>(c->num_sms * 4, (n + RB - 1) / RB));
-  L.nblk2 = (int)std::max<int64_t>(1, std::min<int64_t>(c->num_sms * 2, (n + 2 * RB - 1) / (2 * RB)));
+  L.nblk2 = c->num_sms * 8;  // largest grid of the row-tile kernels (partials per column)
+  if (!lz_tile_attrs(err_attr)) {
+    set_error(std::string("eigsolve: ") + err_attr);
+    return DMRGX_E_CUDA;
+  }
   int rc = L.init();
   if (rc) return rc;
   const int m = L.m, td = L.tdim;

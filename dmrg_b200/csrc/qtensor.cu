@@ -284,6 +284,155 @@ __global__ void rev_cols(const double* __restrict__ src, double* __restrict__ ds
     dst[e] = src[(n - 1 - col) * n * f + rem];
   }
 }
+// ---- batched one-sided Jacobi SVD (Hestenes) of small sector matrices
+// One CTA per sector.  With X the sector's C x R column-major matrix, Z = X^H
+// (C <= R) or Z = X (C > R) has p = min(C, R) columns of length q = max(C, R).
+// The stacked matrix [Z; I_p] ((q + p) x p) sits in shared memory and its
+// column pairs are rotated until every pair of Z columns is orthogonal to
+// working precision: Z W = Y with W unitary (the bottom p rows) and Y's
+// columns orthogonal, their norms the singular values.  Pairs follow a
+// round-robin tournament (p/2 disjoint pairs per round, one warp per pair, p-1
+// rounds per sweep); sweeps stop when none rotates.  One-sided Jacobi gives
+// every singular value to ~1e-16 s_0 or better (values far below sqrt(eps) s_0
+// included, which a Gram matrix loses).  Output, columns in descending order:
+// W into `full` (p x p, ld p: U of the rows when C <= R, V otherwise) and Y
+// into the first p columns of `other` (ld q), as the Gram path leaves them.
+struct JacJob {
+  int64_t x_off;   // element offset of X in the sector buffer
+  int C, R;
+  double* full;
+  double* other;
+  double* s;       // p singular values, descending
+  int* sweeps;     // sweeps used (a value past the limit: not converged)
+};
+constexpr int kJacMaxDoubles = 24576;  // shared-memory budget: (q + p) p f doubles
+constexpr int kJacSweeps = 40;
+
+template <bool CPLX>
+__global__ void __launch_bounds__(256) jacobi_svd(const double* __restrict__ M,
+                                                  const JacJob* __restrict__ jobs) {
+  constexpr int F = CPLX ? 2 : 1;
+  extern __shared__ double jsm[];
+  __shared__ int order[512];
+  __shared__ int rotated;
+  const JacJob jb = jobs[blockIdx.x];
+  const int C = jb.C, R = jb.R, p = min(C, R), q = max(C, R), h = q + p;
+  const double* X = M + jb.x_off * F;
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5, nw = blockDim.x >> 5;
+  // column j of the stacked matrix at jsm[j * h * F]
+  for (int t = tid; t < p * h; t += blockDim.x) {
+    const int j = t / h, r = t - j * h;
+    double re = 0.0, im = 0.0;
+    if (r < q) {
+      // C <= R: Z[r][j] = conj(X[j, r]);  C > R: Z[r][j] = X[r, j]
+      const int64_t e = C <= R ? (int64_t)r * C + j : (int64_t)j * C + r;
+      re = X[e * F];
+      if (CPLX) im = C <= R ? -X[e * F + 1] : X[e * F + 1];
+    } else {
+      re = (r - q == j) ? 1.0 : 0.0;
+    }
+    jsm[((size_t)j * h + r) * F] = re;
+    if (CPLX) jsm[((size_t)j * h + r) * F + 1] = im;
+  }
+  const int P = p + (p & 1);  // players of the tournament (one bye when p is odd)
+  for (int t = tid; t < P; t += blockDim.x) order[t] = t;
+  const double tol = 4e-16 * sqrt((double)q);
+  int sweep = 0;
+  for (; sweep < kJacSweeps; sweep++) {
+    if (tid == 0) rotated = 0;
+    __syncthreads();
+    for (int round = 0; round < P - 1; round++) {
+      for (int pr = wp; pr < P / 2; pr += nw) {
+        int a = order[pr], b = order[P - 1 - pr];
+        if (a >= p || b >= p) continue;
+        if (a > b) { const int x = a; a = b; b = x; }
+        double* ca = jsm + (size_t)a * h * F;
+        double* cb = jsm + (size_t)b * h * F;
+        double al = 0.0, be = 0.0, gr = 0.0, gi = 0.0;
+        for (int r = lane; r < q; r += 32) {
+          const double ar = ca[r * F], br = cb[r * F];
+          const double ai = CPLX ? ca[r * F + 1] : 0.0, bi = CPLX ? cb[r * F + 1] : 0.0;
+          al += ar * ar + ai * ai;
+          be += br * br + bi * bi;
+          gr += ar * br + ai * bi;   // conj(a) b
+          gi += ar * bi - ai * br;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          gr += __shfl_xor_sync(0xffffffffu, gr, o);
+          gi += __shfl_xor_sync(0xffffffffu, gi, o);
+        }
+        const double g = sqrt(gr * gr + gi * gi);
+        if (!(g > tol * sqrt(al * be)) || al == 0.0 || be == 0.0) continue;
+        // rotation zeroing the pair's off-diagonal: with b~ = conj(e) b (e = gamma/|gamma|)
+        //   a' = c a - s b~,  b~' = s a + c b~,  b' = e b~'
+        const double er = gr / g, ei = gi / g;
+        const double zeta = (be - al) / (2.0 * g);
+        const double tt = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double cs = 1.0 / sqrt(1.0 + tt * tt), sn = cs * tt;
+        for (int r = lane; r < h; r += 32) {
+          const double ar = ca[r * F], ai = CPLX ? ca[r * F + 1] : 0.0;
+          const double br = cb[r * F], bi = CPLX ? cb[r * F + 1] : 0.0;
+          // b~ = conj(e) b
+          const double tr = er * br + ei * bi, ti = er * bi - ei * br;
+          const double nar = cs * ar - sn * tr, nai = cs * ai - sn * ti;
+          const double nbr = sn * ar + cs * tr, nbi = sn * ai + cs * ti;
+          ca[r * F] = nar;
+          cb[r * F] = er * nbr - ei * nbi;   // e b~'
+          if (CPLX) {
+            ca[r * F + 1] = nai;
+            cb[r * F + 1] = er * nbi + ei * nbr;
+          }
+        }
+        if (lane == 0) rotated = 1;
+      }
+      __syncthreads();
+      if (tid == 0) {  // circle method: keep order[0], rotate the rest by one
+        const int last = order[P - 1];
+        for (int t = P - 1; t > 1; t--) order[t] = order[t - 1];
+        order[1] = last;
+      }
+      __syncthreads();
+    }
+    if (!rotated) break;
+    __syncthreads();
+  }
+  // singular values (norms of the Z parts), then the descending order
+  double* sv = jsm + (size_t)p * h * F;  // p values after the stacked matrix
+  for (int j = wp; j < p; j += nw) {
+    const double* cj = jsm + (size_t)j * h * F;
+    double a = 0.0;
+    for (int r = lane; r < q * F; r += 32) a += cj[r] * cj[r];
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) sv[j] = sqrt(a);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int j = 0; j < p; j++) order[j] = j;
+    for (int i = 1; i < p; i++) {  // stable insertion sort, descending
+      const int x = order[i];
+      int j = i - 1;
+      while (j >= 0 && sv[order[j]] < sv[x]) {
+        order[j + 1] = order[j];
+        j--;
+      }
+      order[j + 1] = x;
+    }
+    *jb.sweeps = sweep;
+  }
+  __syncthreads();
+  for (int t = tid; t < p; t += blockDim.x) jb.s[t] = sv[order[t]];
+  for (int t = tid; t < p * q * F; t += blockDim.x) {
+    const int jj = t / (q * F), e = t - jj * q * F;
+    jb.other[(size_t)jj * q * F + e] = jsm[(size_t)order[jj] * h * F + e];
+  }
+  for (int t = tid; t < p * p * F; t += blockDim.x) {
+    const int jj = t / (p * F), e = t - jj * p * F;
+    jb.full[(size_t)jj * p * F + e] = jsm[(size_t)order[jj] * h * F + q * F + e];
+  }
+}
+
 // nrm[j] = ||Y[:, j]||_2, j < k (rows x k, column-major, ld rows): one block
 // per column, fixed summation order
 __global__ void col_norms(const double* __restrict__ Y, int64_t rows, int k,
@@ -857,6 +1006,92 @@ std::vector<int> combine_layout(const Group& G, const std::vector<std::vector<in
 }
 }  // namespace
 
+// out[b] = max |element| of block b (off: element offsets, nb + 1 values)
+__global__ void block_maxabs(const double* __restrict__ d, const int64_t* __restrict__ off,
+                             int f, double* __restrict__ out) {
+  const int b = blockIdx.x;
+  double mx = 0.0;
+  for (int64_t e = off[b] + threadIdx.x; e < off[b + 1]; e += blockDim.x)
+    mx = fmax(mx, f == 2 ? hypot(d[2 * e], d[2 * e + 1]) : fabs(d[e]));
+  __shared__ double red[256];
+  red[threadIdx.x] = mx;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[b] = red[0];
+}
+
+// Drop the blocks of T whose entries are all <= 1e-10 in magnitude (the
+// reference's split rule); T is replaced only when a block goes.
+int drop_small_blocks(const Engine& E, QTPtr& T, std::string& err) {
+  const int nb = (int)T->m.syms.size();
+  if (nb == 0) return 0;
+  int64_t* doff = nullptr;
+  double* dmx = nullptr;
+  std::vector<double> mx(nb, 0.0);
+  cudaError_t e = dalloc(&doff, (size_t)nb + 1, E.stream);
+  if (e == cudaSuccess) e = dalloc(&dmx, (size_t)nb, E.stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(doff, T->off.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice,
+                        E.stream);
+  if (e == cudaSuccess) {
+    block_maxabs<<<nb, 256, 0, E.stream>>>(T->d, doff, T->f, dmx);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(mx.data(), dmx, sizeof(double) * nb, cudaMemcpyDeviceToHost, E.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+  dfree(doff, E.stream);
+  dfree(dmx, E.stream);
+  if (e != cudaSuccess) {
+    err = std::string("svd: ") + cudaGetErrorString(e);
+    return -1;
+  }
+  std::vector<int> keep;
+  for (int b = 0; b < nb; b++)
+    if (mx[b] > 1e-10) keep.push_back(b);
+  if ((int)keep.size() == nb) return 0;
+  auto N = std::make_shared<QTensor>();
+  N->f = T->f;
+  N->m.dims = T->m.dims;
+  N->m.dirs = T->m.dirs;
+  for (int b : keep) N->m.syms.push_back(T->m.syms[b]);
+  if (N->alloc(E.stream) != cudaSuccess) {
+    err = "svd: allocation failed";
+    return -1;
+  }
+  for (size_t q = 0; q < keep.size() && e == cudaSuccess; q++) {
+    const int b = keep[q];
+    if (T->bsize(b) > 0)
+      e = cudaMemcpyAsync(N->d + N->off[q] * N->f, T->d + T->off[b] * T->f,
+                          sizeof(double) * T->bsize(b) * T->f, cudaMemcpyDeviceToDevice, E.stream);
+  }
+  if (e != cudaSuccess) {
+    err = std::string("svd: ") + cudaGetErrorString(e);
+    return -1;
+  }
+  T = N;
+  return 0;
+}
+
+// the Jacobi kernel's shared memory: opted in once per process
+bool jacobi_attrs(std::string& err) {
+  static int done = 0;
+  if (!done) {
+    const int bytes = (int)(sizeof(double) * (kJacMaxDoubles + 256));
+    cudaError_t e = cudaFuncSetAttribute(jacobi_svd<true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(jacobi_svd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               bytes);
+    done = e == cudaSuccess ? 1 : -1;
+  }
+  if (done < 0) err = "svd: cannot set the Jacobi kernel's shared memory";
+  return done == 1;
+}
+
 int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTPtr& V,
            std::vector<double>& s, std::string& err) {
   const Group& G = E.G;
@@ -930,6 +1165,35 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
     dfree(dM, E.stream);
     return -1;
   }
+  // A sector whose entries are all <= TOL = 1e-10 in magnitude is taken as zero,
+  // as the reference's tensor::svd does (src/tensor.cpp:736-785): its singular
+  // values are 0 and its U and V the identity.
+  std::vector<char> zero(ns, 0);
+  {
+    std::vector<double> smax(ns, 0.0);
+    int64_t* doff = nullptr;
+    double* dmx = nullptr;
+    e = dalloc(&doff, (size_t)ns + 1, E.stream);
+    if (e == cudaSuccess) e = dalloc(&dmx, (size_t)ns, E.stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(doff, moff.data(), sizeof(int64_t) * (ns + 1), cudaMemcpyHostToDevice,
+                          E.stream);
+    if (e == cudaSuccess) {
+      block_maxabs<<<ns, 256, 0, E.stream>>>(dM, doff, f, dmx);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(smax.data(), dmx, sizeof(double) * ns, cudaMemcpyDeviceToHost, E.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+    dfree(doff, E.stream);
+    dfree(dmx, E.stream);
+    if (e != cudaSuccess) {
+      dfree(dM, E.stream);
+      err = std::string("svd: ") + cudaGetErrorString(e);
+      return -1;
+    }
+    for (int i = 0; i < ns; i++) zero[i] = !(smax[i] > 1e-10);
+  }
   // Per-sector SVD of X = A^T (column-major C x R view of the row-major block),
   // X = Ux S Vx^H with full Ux (C x C) and Vx (R x R), from the Hermitian
   // eigenproblem of the smaller Gram matrix (divide and conquer, syevd/heevd):
@@ -948,7 +1212,8 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
   std::vector<double*> Gm(ns, nullptr), Wd(ns, nullptr);
   int* dinfo = nullptr;
   double *work = nullptr, *aux = nullptr;
-  bool fail = dalloc(&dinfo, (size_t)std::max(1, 3 * ns), E.stream) != cudaSuccess;
+  bool fail = dalloc(&dinfo, (size_t)std::max(1, 3 * ns), E.stream) != cudaSuccess ||
+              cudaMemsetAsync(dinfo, 0, sizeof(int) * std::max(1, 3 * ns), E.stream) != cudaSuccess;
   g_sol.set_stream(t_sol.h, E.stream);
   g_sol.blas_set_stream(t_sol.blas, E.stream);
   const bool cx = f == 2;
@@ -964,12 +1229,60 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
     return g_sol.dgemm(t_sol.blas, ta, tb, m, n, k, &d1, A_, lda, B_, ldb, &d0, C_, ldc) ==
            CUBLAS_STATUS_SUCCESS;
   };
-  // ---- phase 1: Gram matrices and their eigendecompositions, all sectors queued
+  // ---- phase 1: sectors small enough for shared memory by the batched Jacobi
+  // kernel (one launch), the others by Gram matrices and their
+  // eigendecompositions, all queued
   int lmax = 1;
+  std::vector<char> jac(ns, 0);
+  std::vector<double*> sjac(ns, nullptr);
+  std::vector<JacJob> jobs;
+  int* djsw = nullptr;
+  JacJob* djobs = nullptr;
+  size_t jac_smem = 0;
+  for (int i = 0; i < ns && !fail; i++) {
+    const int C = (int)Cc[i], R = (int)Rr[i], p = std::min(C, R), q = std::max(C, R);
+    if (p == 0 || zero[i] || (int64_t)(q + p) * p * f > kJacMaxDoubles) continue;
+    jac[i] = 1;
+    double *full = nullptr, *other = nullptr;
+    if (dalloc(&full, (size_t)p * p * f, E.stream) != cudaSuccess ||
+        dalloc(&other, (size_t)q * q * f, E.stream) != cudaSuccess ||
+        dalloc(&sjac[i], (size_t)p, E.stream) != cudaSuccess) {
+      dfree(full, E.stream);
+      dfree(other, E.stream);
+      fail = true;
+      break;
+    }
+    if (C <= R) {
+      Ux[i] = full;
+      Vx[i] = other;
+    } else {
+      Vx[i] = full;
+      Ux[i] = other;
+    }
+    jobs.push_back(JacJob{moff[i], C, R, full, other, sjac[i], nullptr});
+    jac_smem = std::max(jac_smem, sizeof(double) * ((size_t)(q + p) * p * f + p));
+  }
+  if (!fail && !jobs.empty()) {
+    fail = dalloc(&djsw, jobs.size(), E.stream) != cudaSuccess ||
+           dalloc(&djobs, jobs.size(), E.stream) != cudaSuccess;
+    if (!fail) {
+      for (size_t t = 0; t < jobs.size(); t++) jobs[t].sweeps = djsw + t;
+      fail = cudaMemcpyAsync(djobs, jobs.data(), sizeof(JacJob) * jobs.size(),
+                             cudaMemcpyHostToDevice, E.stream) != cudaSuccess;
+    }
+    if (!fail) fail = !jacobi_attrs(err);
+    if (!fail) {
+      if (f == 2)
+        jacobi_svd<true><<<(int)jobs.size(), 256, jac_smem, E.stream>>>(dM, djobs);
+      else
+        jacobi_svd<false><<<(int)jobs.size(), 256, jac_smem, E.stream>>>(dM, djobs);
+      fail = cudaGetLastError() != cudaSuccess;
+    }
+  }
   for (int i = 0; i < ns && !fail; i++) {
     const int C = (int)Cc[i], R = (int)Rr[i], p = std::min(C, R);
     S[i].assign(p, 0.0);
-    if (p == 0) continue;
+    if (p == 0 || jac[i] || zero[i]) continue;
     const double* X = dM + moff[i] * f;
     if (dalloc(&Gm[i], (size_t)p * p * f, E.stream) != cudaSuccess ||
         dalloc(&Wd[i], (size_t)p, E.stream) != cudaSuccess) {
@@ -991,7 +1304,7 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
   if (!fail) fail = dalloc(&work, (size_t)lmax * f, E.stream) != cudaSuccess;
   for (int i = 0; i < ns && !fail; i++) {
     const int p = (int)std::min(Cc[i], Rr[i]);
-    if (p == 0) continue;
+    if (p == 0 || jac[i] || zero[i]) continue;
     const cusolverStatus_t st =
         cx ? g_sol.z_evd(t_sol.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, p,
                          (cuDoubleComplex*)Gm[i], p, Wd[i], (cuDoubleComplex*)work, lmax,
@@ -1002,14 +1315,23 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
   }
   std::vector<std::vector<double>> lam(ns);
   std::vector<int> hinfo((size_t)std::max(1, 3 * ns), 0);
+  std::vector<int> jsw(jobs.size(), 0);
   if (!fail) {
     for (int i = 0; i < ns; i++) {
       lam[i].assign(S[i].size(), 0.0);
-      if (!lam[i].empty())
-        cudaMemcpyAsync(lam[i].data(), Wd[i], sizeof(double) * lam[i].size(),
+      if (!lam[i].empty() && !zero[i])
+        cudaMemcpyAsync(lam[i].data(), jac[i] ? sjac[i] : Wd[i], sizeof(double) * lam[i].size(),
                         cudaMemcpyDeviceToHost, E.stream);
     }
+    if (!jobs.empty())
+      cudaMemcpyAsync(jsw.data(), djsw, sizeof(int) * jsw.size(), cudaMemcpyDeviceToHost,
+                      E.stream);
     if (cudaStreamSynchronize(E.stream) != cudaSuccess) fail = true;
+    for (int v : jsw)
+      if (!fail && v >= kJacSweeps) {
+        err = "svd: Jacobi sweeps did not converge";
+        fail = true;
+      }
   }
   // ---- phase 2: singular values, the derived side, QR completion
   std::vector<int> kk(ns, 0);
@@ -1020,26 +1342,47 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
     for (int i = 0; i < ns && !fail; i++) {
       const int p = (int)S[i].size();
       if (p == 0) continue;
-      for (int j = 0; j < p; j++) S[i][j] = std::sqrt(std::max(lam[i][p - 1 - j], 0.0));
+      // Jacobi sectors: the singular values, descending; Gram: eigenvalues,
+      // ascending; zero sectors: 0
+      for (int j = 0; j < p; j++)
+        S[i][j] = zero[i] ? 0.0 : jac[i] ? lam[i][j] : std::sqrt(std::max(lam[i][p - 1 - j], 0.0));
       int k = 0;
-      while (k < p && S[i][k] > 1e-13 * S[i][0]) k++;
+      while (!zero[i] && k < p && S[i][k] > 1e-13 * S[i][0]) k++;
       kk[i] = k;
       const int C = (int)Cc[i], R = (int)Rr[i], q = std::max(C, R);
-      double* full = nullptr;  // the Gram side, columns in descending order
-      double* other = nullptr; // the derived side, q x q
-      if (dalloc(&full, (size_t)p * p * f, E.stream) != cudaSuccess ||
-          dalloc(&other, (size_t)q * q * f, E.stream) != cudaSuccess) {
-        dfree(full, E.stream);
-        fail = true;
-        break;
-      }
-      rev_cols<<<gridfor((int64_t)p * p * f), 256, 0, E.stream>>>(Gm[i], full, p, f);
-      if (C <= R) {
-        Ux[i] = full;
-        Vx[i] = other;
-      } else {
-        Vx[i] = full;
-        Ux[i] = other;
+      double* other = C <= R ? Vx[i] : Ux[i];  // the derived side, q x q
+      if (zero[i]) {
+        double* full = nullptr;  // identity on both sides
+        if (dalloc(&full, (size_t)p * p * f, E.stream) != cudaSuccess ||
+            dalloc(&other, (size_t)q * q * f, E.stream) != cudaSuccess) {
+          dfree(full, E.stream);
+          fail = true;
+          break;
+        }
+        eye<<<gridfor((int64_t)p * p), 256, 0, E.stream>>>(full, p, f);
+        if (C <= R) {
+          Ux[i] = full;
+          Vx[i] = other;
+        } else {
+          Vx[i] = full;
+          Ux[i] = other;
+        }
+      } else if (!jac[i]) {
+        double* full = nullptr;  // the Gram side, columns in descending order
+        if (dalloc(&full, (size_t)p * p * f, E.stream) != cudaSuccess ||
+            dalloc(&other, (size_t)q * q * f, E.stream) != cudaSuccess) {
+          dfree(full, E.stream);
+          fail = true;
+          break;
+        }
+        rev_cols<<<gridfor((int64_t)p * p * f), 256, 0, E.stream>>>(Gm[i], full, p, f);
+        if (C <= R) {
+          Ux[i] = full;
+          Vx[i] = other;
+        } else {
+          Vx[i] = full;
+          Ux[i] = other;
+        }
       }
       int lq = 0, lo = 0;
       if (k > 0) {
@@ -1067,15 +1410,21 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
       double* other = C <= R ? Vx[i] : Ux[i];
       const double* full = C <= R ? Ux[i] : Vx[i];
       const double* X = dM + moff[i] * f;
+      if (zero[i]) {
+        eye<<<gridfor((int64_t)q * q), 256, 0, E.stream>>>(other, q, f);
+        continue;
+      }
       if (dalloc(&scs[i], (size_t)p, E.stream) != cudaSuccess) {
         fail = true;
         break;
       }
       // derived columns X^H u_j (C <= R) or X v_j (C > R) of all p Gram vectors
       // into the first p columns of `other` (q x q, ld q); their norms are the
-      // singular values
-      if (C <= R) fail = !gemm(OPH, CUBLAS_OP_N, R, p, C, X, C, full, C, other, R);
-      else fail = !gemm(CUBLAS_OP_N, CUBLAS_OP_N, C, p, R, X, C, full, R, other, C);
+      // singular values.  The Jacobi kernel left them there already.
+      if (!jac[i]) {
+        if (C <= R) fail = !gemm(OPH, CUBLAS_OP_N, R, p, C, X, C, full, C, other, R);
+        else fail = !gemm(CUBLAS_OP_N, CUBLAS_OP_N, C, p, R, X, C, full, R, other, C);
+      }
       if (fail) break;
       col_norms<<<p, 256, 0, E.stream>>>(other, q, p, scs[i], f);
       if (k == 0) {
@@ -1121,7 +1470,7 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
       // before it so each sector's list stays descending (the order of the
       // vectors), which moves a value only between near-equal neighbours
       for (int i = 0; i < ns && !fail; i++)
-        for (size_t j = 0; j < nrm_h[i].size(); j++)
+        for (size_t j = 0; j < nrm_h[i].size() && !zero[i]; j++)
           S[i][j] = j ? std::min(nrm_h[i][j], S[i][j - 1]) : nrm_h[i][j];
       for (int i = 0; i < 3 * ns && !fail; i++)
         if (hinfo[i] != 0) {
@@ -1131,7 +1480,10 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
     }
   }
   if (fail && err.empty()) err = "svd: cuSOLVER / cuBLAS call failed";
+  dfree(djsw, E.stream);
+  dfree(djobs, E.stream);
   for (int i = 0; i < ns; i++) {
+    dfree(sjac[i], E.stream);
     dfree(Gm[i], E.stream);
     dfree(Wd[i], E.stream);
     dfree(taus[i], E.stream);
@@ -1278,6 +1630,10 @@ int qt_svd(const Engine& E, const QTensor& A, int num, int cutoff, QTPtr& U, QTP
     err = std::string("svd: ") + cudaGetErrorString(e);
     return -1;
   }
+  // the reference's split keeps a sub-block only when one of its entries
+  // exceeds TOL = 1e-10 in magnitude (src/qtensor.cpp:589-652, U.split and
+  // V.split at :1254-1260): the others are dropped here too
+  if (drop_small_blocks(E, U, err) || drop_small_blocks(E, V, err)) return -1;
   return 0;
 }
 

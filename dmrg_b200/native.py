@@ -62,6 +62,8 @@ SIGNATURES = {
     "dmrgx_step_seconds": (_i, [_vp, _dp, _i64, _i64p]),
     "dmrgx_singular": (_i, [_vp, _dp, _dp, _ip, _i64, _i64p]),
     "dmrgx_step_split": (_i, [_vp, _dp, _i64, _i64p]),
+    "dmrgx_svd": (_i, [_vp, _ip, _vp, _i, _i, _i, _i, _i64p]),
+    "dmrgx_svd_result": (_i, [_vp, _ip, _vp, _ip, _vp, _dp]),
     "dmrgx_run_seconds": (_i, [_vp, _dp, _i]),
     "dmrgx_adjoint": (_i, [_vp, _i, _dp, _i, _dp, _i64, _i64p, _dp, _dp]),
     "dmrgx_expect": (_i, [_vp, _dp, _i, _dp]),
@@ -367,6 +369,24 @@ class Context:
         out = np.zeros(max(1, int(ns[0])))
         _check(lib().dmrgx_step_seconds(self.ptr, out.ctypes.data_as(_dp), out.size, _i64p(ns)))
         return out[:int(ns[0])]
+
+    def svd(self, meta, vals, num, cutoff, group_n, fermion):
+        """Block SVD with truncation (the reference's qtensor::svd): returns
+        ((U meta, U values), (V meta, V values), singular values)."""
+        m = np.ascontiguousarray(meta, np.int32)
+        dt = np.complex128 if self.dtype == C128 else np.float64
+        v = np.ascontiguousarray(vals, dt)
+        sz = np.zeros(5, np.int64)
+        _check(lib().dmrgx_svd(self.ptr, _ip(m), v.ctypes.data, num, cutoff, group_n, fermion,
+                               _i64p(sz)))
+        um = np.zeros(max(1, sz[0]), np.int32)
+        uv = np.zeros(max(1, sz[1]), dt)
+        vm = np.zeros(max(1, sz[2]), np.int32)
+        vv = np.zeros(max(1, sz[3]), dt)
+        sv = np.zeros(max(1, sz[4]))
+        _check(lib().dmrgx_svd_result(self.ptr, _ip(um), uv.ctypes.data, _ip(vm), vv.ctypes.data,
+                                      sv.ctypes.data_as(_dp)))
+        return (um[:sz[0]], uv[:sz[1]]), (vm[:sz[2]], vv[:sz[3]]), sv[:sz[4]]
 
     def step_split(self):
         """Per-step split of the last dmrg() run: rows (eig, svd, env, fuse, plan) seconds."""

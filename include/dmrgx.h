@@ -293,6 +293,23 @@ int dmrgx_set_solver(dmrgx_ctx* ctx, int nev, int ncv, int predict);
  * The final state of dmrgx_dmrg (MPS site tensors, environments and the one-site
  * centre of the last step) stays in the context for the two calls below. */
 
+/* The block SVD with truncation of the reference's qtensor<T>::svd(U, S, V,
+ * num, cutoff) (src/qtensor.cpp:1122-1262), on the device: the tensor (meta,
+ * host vals) is reshaped with its first num legs as rows and the rest as
+ * columns, every symmetry sector is decomposed, the singular values of all
+ * sectors are merged in descending order (ties to the lower sector), the
+ * cutoff largest are kept (0: all) and U / V are padded with complement
+ * columns to min(dim, cutoff) per sector, as the reference does.  group_n and
+ * fermion as for dmrgx_plan_build.  The results stay in the context;
+ * sizes[0..5) = U meta ints, U elements, V meta ints, V elements, number of
+ * singular values (the whole spectrum, descending).  dmrgx_svd_result copies
+ * them out (any pointer may be NULL): U as [legs 0..num), k], V as [k, legs
+ * num..), metadata in the layout of dmrgx_plan_psi_layout. */
+int dmrgx_svd(dmrgx_ctx* ctx, const int* meta, const void* vals, int num, int cutoff,
+              int group_n, int fermion, int64_t* sizes);
+int dmrgx_svd_result(dmrgx_ctx* ctx, int* u_meta, void* u_vals, int* v_meta, void* v_vals,
+                     double* s);
+
 /* The rest of the reference's singular-value rows (print_singular,
  * src/useful.cpp:75-102) for every step of the last dmrgx_dmrg, in schedule
  * order (the truncation error is dmrgx_dmrg's trunc):

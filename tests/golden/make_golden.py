@@ -35,6 +35,10 @@ oracle/_ref by oracle/Makefile) and records:
                       RUNS (small_full) and BASELINE config 2, XYZ L=64 m=256
                       n=8 (config2; about an hour on 8 host cores).
 
+  svd.npz             the reference's block SVD with truncation (qtensor::svd)
+                      on captured step states and a graded-spectrum tensor:
+                      inputs, U, V, the kept values per sector and the spectrum.
+
 ``python tests/golden/make_golden.py z2cubed`` regenerates only the named
 fixtures (steps, microbench, z2cubed, pbc); no argument regenerates all of them.
 
@@ -225,8 +229,95 @@ def make_small_full():
         record_schedule(f"{model}_L{L}_m{m}", variant, model, L, m, n, par)
 
 
+def psi_meta(R, cplx, lenv, lnum, renv, rnum, sector):
+    """The psi layout of a step (generate_dim_sym, src/useful.cpp:151-194) as qtensor
+    metadata; psi's legs carry direction 0 (the reference's qtensor(val, dim, sym)
+    constructor, src/qtensor.cpp:25-48)."""
+    le = R.py_to_qt(cplx, *lenv)
+    re_ = R.py_to_qt(cplx, *renv)
+    need = R.lib.oref_gen_dim_sym(cplx, le, lnum, re_, rnum, sector, None, 0)
+    out = np.zeros(need, np.int32)
+    R.lib.oref_gen_dim_sym(cplx, le, lnum, re_, rnum, sector,
+                           out.ctypes.data_as(refbind.C.POINTER(refbind.C.c_int)), need)
+    nleg = int(out[0])
+    head = 2 + nleg + int(out[2:2 + nleg].sum())
+    return np.concatenate([out[:head], np.zeros(nleg, np.int32), out[head:]])
+
+
+def reference_svd(R, cplx, meta, vals, num, cutoff):
+    """The reference's qtensor::svd (src/qtensor.cpp:1122-1262) on one tensor:
+    U, S (diagonal blocks: the kept values per sector) and V serialised, and the
+    whole spectrum it returns."""
+    C = refbind.C
+    a = R.py_to_qt(cplx, meta, vals)
+    U, S, V = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    cap = int(np.asarray(vals).size) + 16
+    sv = np.zeros(cap)
+    ns = R.lib.oref_svd(cplx, a, num, cutoff, C.byref(U), C.byref(S), C.byref(V),
+                        sv.ctypes.data_as(C.POINTER(C.c_double)), cap)
+    out = dict(u=R.qt_to_py(cplx, U.value), sdiag=R.qt_to_py(0, S.value),
+               v=R.qt_to_py(cplx, V.value), s=sv[:ns].copy())
+    R.lib.oref_qt_free(cplx, U.value)
+    R.lib.oref_qt_free(0, S.value)
+    R.lib.oref_qt_free(cplx, V.value)
+    return out
+
+
+def make_svd():
+    """Block SVD fixtures: the reference's qtensor::svd on the same inputs the
+    GPU test gives dmrgx_svd.  Inputs: the lowest Ritz vector of one captured
+    step of each model (their spectra fall to 1e-15 and exact zeros), and the
+    m=64 U(1) microbench psi with every block scaled by 10^-(2b mod 15) (a
+    graded spectrum with values far below 1e-8 s_0), each with a cutoff that
+    truncates."""
+    arrs = {}
+    cases = []
+    for model, variant, gn, ferm in (("kitaev", "kitaev", 2, 1), ("xyz", "xyz", 2, 0),
+                                     ("potts", "potts", 3, 0)):
+        z = np.load(os.path.join(HERE, f"steps_{model}.npz"))
+        k = int(z["nsteps"]) - 1
+        p = f"s{k}_"
+        cplx = int(np.iscomplexobj(z[p + "lenv_vals"]))
+        R = refbind.Ref(variant)
+        ln, rn = (int(v) for v in z[p + "nums"])
+        meta = psi_meta(R, cplx, (z[p + "lenv_meta"], z[p + "lenv_vals"]), ln - 1,
+                        (z[p + "renv_meta"], z[p + "renv_vals"]), rn, 0)
+        num = 2 if meta[0] == 4 else 1
+        cases.append((model, R, cplx, meta, z[p + "evec"], num, 6, gn, ferm))
+    w = workloads.microbench(64)
+    R = refbind.Ref("u1")
+    meta = psi_meta(R, 0, w["lenv"], 2, w["renv"], 2, w["sector"])
+    nblk = int(meta[1])
+    nleg = int(meta[0])
+    nsec = meta[2:2 + nleg]
+    dims = []
+    o = 2 + nleg
+    for l in range(nleg):
+        dims.append(meta[o:o + nsec[l]])
+        o += nsec[l]
+    sym = meta[o + nleg:].reshape(nblk, nleg)
+    rng = np.random.default_rng(5)
+    parts = []
+    for b in range(nblk):
+        size = int(np.prod([dims[l][sym[b, l]] for l in range(nleg)]))
+        parts.append(rng.standard_normal(size) * 10.0 ** (-((2 * b) % 15)))
+    cases.append(("graded_u1", R, 0, meta, np.concatenate(parts), 2, 40, w["group_n"], 0))
+    for name, R, cplx, meta, vals, num, cutoff, gn, ferm in cases:
+        ref = reference_svd(R, cplx, meta, vals, num, cutoff)
+        p = name + "_"
+        arrs[p + "meta"], arrs[p + "vals"] = meta, vals
+        arrs[p + "args"] = np.array([num, cutoff, gn, ferm, cplx], np.int32)
+        arrs[p + "u_meta"], arrs[p + "u_vals"] = ref["u"]
+        arrs[p + "v_meta"], arrs[p + "v_vals"] = ref["v"]
+        arrs[p + "sd_meta"], arrs[p + "sd_vals"] = ref["sdiag"]
+        arrs[p + "s"] = ref["s"]
+        print("svd", name, "values", ref["s"].size, "s0", ref["s"][0], "min", ref["s"][-1])
+    arrs["cases"] = np.array([c[0] for c in cases])
+    np.savez_compressed(os.path.join(HERE, "svd.npz"), **arrs)
+
+
 PARTS = {"steps": make_steps, "microbench": make_microbench, "z2cubed": make_z2cubed,
-         "pbc": make_steps_pbc, "small_full": make_small_full, "config2": make_config2}
+         "pbc": make_steps_pbc, "small_full": make_small_full, "svd": make_svd, "config2": make_config2}
 
 
 def main(parts):

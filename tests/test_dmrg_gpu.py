@@ -50,11 +50,15 @@ def load_schedule(name):
 # energies and truncation errors.  A truncation error 1 - sum s_i^2 is a
 # difference of O(1) numbers, so it carries an absolute rounding floor of a few
 # 1e-16 per kept value; 5e-14 covers the few hundred values kept here.  The
-# entropy and the singular values are compared to 1e-10 relative and 1e-13 of
-# s_0 (the largest singular value, 1 for a normalised state).
+# entropy is compared to 1e-10 relative.  The singular values are those of
+# the step's eigenvector, which both eigensolvers converge only to a residual
+# |H psi - E psi| <= 1e-10 |E|: the vectors may differ by |d psi| ~ 1e-10 |E| /
+# gap (~1e-9 for these chains), and a singular value moves by at most |d psi|,
+# so they are compared to 1e-8 absolute (s_0 ~ 1).  The SVD itself is held to
+# 1e-13 of s_0 on identical inputs in test_svd_gpu.py.
 E_REL = 1e-10
 TRUNC_REL, TRUNC_ABS = 1e-10, 5e-14
-S_REL, SV_ABS = 1e-10, 1e-13
+S_REL, SV_ABS = 1e-10, 1e-8
 
 
 def check_schedule(r, g):
