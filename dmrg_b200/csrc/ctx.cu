@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <string>
@@ -16,6 +17,10 @@
 using namespace dmrgx;
 
 namespace dmrgx {
+
+double wall_now() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 int build_split_plan(dmrgx_ctx* c, int eb);
 int run_matvec_split(dmrgx_ctx* c, const double* in, double* out);
@@ -80,6 +85,7 @@ void DevBuf::release() {
   } while (0)
 
 namespace {
+using dmrgx::wall_now;
 
 // Environment image on the host with the task signs folded into the blocks:
 // a block used only with alpha=-1 is stored negated, a block used with both
@@ -284,6 +290,7 @@ struct PairSrc {
 // which is the reference's accumulation of the edge pair into out (lemap built
 // with beta = 1, src/core.cpp:247).
 int finalize_plan(dmrgx_ctx* c, const std::vector<PairSrc>& pairs) {
+  const double t0 = wall_now();
   const int f = c->f();
   c->has_plan = false;
   c->flops = 0;
@@ -371,6 +378,8 @@ int finalize_plan(dmrgx_ctx* c, const std::vector<PairSrc>& pairs) {
   if (rc) return rc;
   // RI/LI are host temporaries: wait for the uploads before they go away
   CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const double t1 = wall_now();
+  c->t_plan_part[1] += t1 - t0;
   c->sp.free_device();
   c->sp = SplitPlan();
   if (c->prec != DMRGX_PREC_FP64) {
@@ -473,6 +482,7 @@ int plan_build_device(dmrgx_ctx* c, const QTensor& L, const QTensor& R, int l_nu
     set_error("plan: tensor element type differs from the context's");
     return DMRGX_E_ARG;
   }
+  const double t0 = wall_now();
   const bool pbc = Le && Re;
   std::vector<PairSrc> pairs(pbc ? 2 : 1);
   std::vector<std::vector<int>> dim, sym;
@@ -505,6 +515,7 @@ int plan_build_device(dmrgx_ctx* c, const QTensor& L, const QTensor& R, int l_nu
   };
   dev(pairs[0], R, L);
   if (pbc) dev(pairs[1], *Re, *Le);
+  c->t_plan_part[0] += wall_now() - t0;
   return finalize_plan(c, pairs);
 }
 

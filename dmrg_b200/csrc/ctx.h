@@ -127,6 +127,11 @@ struct dmrgx_ctx {
 
   bool per_block = false;                       // DMRGX_SCHED_PER_BLOCK: one GEMM per task row
   void* blas = nullptr;                         // cuBLAS handle of the per-block schedule
+  // wall seconds of the plan-building parts, summed since the last dmrgx_dmrg
+  // began: [0] sector bookkeeping and task lists, [1] FP64 images and
+  // descriptors (uploads included), [2] split-precision images and
+  // descriptors, [3] autotuning
+  double t_plan_part[4] = {0, 0, 0, 0};
   // results of the last dmrgx_svd: U and V (metadata, values) and the spectrum
   std::vector<int> svd_um, svd_vm;
   std::vector<double> svd_uv, svd_vv, svd_s;

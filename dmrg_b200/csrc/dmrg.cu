@@ -1152,6 +1152,7 @@ extern "C" int dmrgx_dmrg(dmrgx_ctx* c, int model, int L, int m, int sweeps, int
     R->edge[0] = el;
     R->edge[L - 1] = er;
   }
+  for (double& x : c->t_plan_part) x = 0.0;
   const double t0 = Run::now();
   int rc = R->dmrg(m, sweeps);
   const double t1 = Run::now();
@@ -1399,6 +1400,7 @@ extern "C" int dmrgx_run_seconds(dmrgx_ctx* c, double* out, int cap) {
   out[3] = R->t_env;
   out[4] = R->t_fuse;
   out[5] = R->t_plan;
+  for (int q = 0; q < 4 && 6 + q < cap; q++) out[6 + q] = c->t_plan_part[q];
   return 0;
 }
 

@@ -124,8 +124,13 @@ __device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc, bool
                "r"(pred ? 8 : 0)
                : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+
+// 16-byte asynchronous copy global -> shared of `bytes` (0, 8 or 16) valid
+// bytes, the rest zero-filled; both addresses 16-byte aligned
+__device__ __forceinline__ void cp_async16(double* sdst, const double* gsrc, int bytes) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(sdst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes)
+               : "memory");
 }
 
 // true in the block that finishes last (after all partials are visible)
@@ -160,52 +165,95 @@ __device__ __forceinline__ void lz_final_coef(const double* part, int k, double*
   }
 }
 
-// dynamic shared memory of lz_tile for k basis columns (bytes)
-__host__ __device__ constexpr size_t lz_tile_smem(int k, bool cplx) {
-  return sizeof(double) * ((size_t)k * TR * (cplx ? 2 : 1) + TR * (cplx ? 2 : 1) + 4 * MAX_NCV +
-                           RB / 32);
+// dynamic shared memory of lz_tile for k basis columns (bytes): two tile
+// buffers (basis slice and w), the coefficients, per-warp norm partials
+__host__ __device__ constexpr size_t lz_tile_smem(int k, bool cplx, int tr) {
+  return sizeof(double) * (2 * ((size_t)k * tr * (cplx ? 2 : 1) + tr * (cplx ? 2 : 1)) +
+                           2 * MAX_NCV + RB / 32);
+}
+// rows per tile: TR, or TR / 2 where two TR-row buffers would not fit
+__host__ __device__ constexpr int lz_tile_rows(int k, bool cplx) {
+  return lz_tile_smem(k, cplx, TR) <= (200u << 10) ? TR : TR / 2;
 }
 
-template <bool CPLX, int MODE>
+constexpr int LZ_COLS = (MAX_NCV + RB / 32 - 1) / (RB / 32);  // columns per warp, at most
+
+template <bool CPLX, int MODE, int TRT>
 __global__ void __launch_bounds__(RB) lz_tile(const double* __restrict__ V, int64_t ld, int k,
                                               const double* __restrict__ cin,
                                               double* __restrict__ w, int64_t n,
                                               double* __restrict__ part, unsigned* ticket,
                                               double* __restrict__ cout, double* __restrict__ T,
-                                              int tdim, int jt, double* __restrict__ inv) {
+                                              int tdim, int jt, double* __restrict__ inv,
+                                              int vec) {
   constexpr int F = CPLX ? 2 : 1;
+  constexpr int tr = TRT;
+  constexpr int EPC = tr * F;          // doubles of one column in a tile
+  constexpr int CPC = EPC / 2;         // 16-byte chunks of one column
   extern __shared__ double smem[];
-  double* sV = smem;                        // column j, element e at sV[j * TR * F + e]
-  double* sw = sV + (size_t)k * TR * F;     // the tile of w
-  double* sc = sw + TR * F;                 // cin (pairs)
-  double* sacc = sc + 2 * MAX_NCV;          // running block sums (pairs)
-  double* sred = sacc + 2 * MAX_NCV;        // per-warp norm partials (MODE 2)
+  const size_t tsz = (size_t)k * tr * F + tr * F;  // one buffer: slice then w
+  double* sc = smem + 2 * tsz;                     // cin (pairs)
+  double* sred = sc + 2 * MAX_NCV;                 // per-warp norm partials (MODE 2)
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   if (MODE != 0)
     for (int t = tid; t < 2 * k; t += RB) sc[t] = cin[t];
-  for (int t = tid; t < 2 * MAX_NCV; t += RB) sacc[t] = 0.0;
+  // warp wp owns columns wp, wp + 8, ...: per-lane running sums over all tiles,
+  // reduced across the warp once at the end
+  double accr[LZ_COLS], acci[LZ_COLS];
+#pragma unroll
+  for (int q = 0; q < LZ_COLS; q++) accr[q] = acci[q] = 0.0;
   double nrm = 0.0;  // MODE 2: this thread's sum of |w|^2
-  const int64_t ntiles = (n + TR - 1) / TR;
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int64_t i0 = tile * TR;
-    const int len = (int)(n - i0 < TR ? n - i0 : TR) * F;  // doubles of the tile per column
-    __syncthreads();  // the previous tile's readers are done (and sc / sacc are set)
-    // every thread queues all its copies before waiting (memory-level parallelism)
-    for (int t = tid; t < k * TR * F; t += RB) {
-      const int j = t / (TR * F), e = t - j * (TR * F);
-      cp_async8(sV + t, e < len ? V + (int64_t)j * ld * F + i0 * F + e : V, e < len);
+  const int64_t ntiles = (n + tr - 1) / tr;
+  // queue the copies of one tile into buffer b (one commit group per thread)
+  auto stage = [&](int64_t tile, int b) {
+    double* sV = smem + b * tsz;
+    double* sw = sV + (size_t)k * tr * F;
+    const int64_t i0 = tile * tr;
+    const int len = (int)(n - i0 < tr ? n - i0 : tr) * F;
+    if (vec) {
+      // columns start 16-byte aligned (ld * F even): 16-byte chunks, thread
+      // tid copies chunk tid % CPC of columns tid / CPC, + RB / CPC, ...
+      const int c = tid % CPC, e = 2 * c;
+      const int bytes = e + 2 <= len ? 16 : (e < len ? 8 : 0);
+      const double* src = V + i0 * F + e;
+      for (int j = tid / CPC; j < k; j += RB / CPC)
+        cp_async16(sV + j * EPC + e, bytes ? src + (int64_t)j * ld * F : V, bytes);
+    } else {
+      const int e = tid % EPC;
+      const double* src = V + i0 * F + e;
+      for (int j = tid / EPC; j < k; j += RB / EPC)
+        cp_async8(sV + j * EPC + e, e < len ? src + (int64_t)j * ld * F : V, e < len);
     }
-    for (int t = tid; t < TR * F; t += RB) cp_async8(sw + t, t < len ? w + i0 * F + t : w, t < len);
-    cp_async_wait_all();
-    __syncthreads();
-    if (MODE != 0 && tid < TR) {
+    if (tid < CPC) {
+      const int e = 2 * tid;
+      const int bytes = e + 2 <= len ? 16 : (e < len ? 8 : 0);
+      cp_async16(sw + e, bytes ? w + i0 * F + e : w, bytes);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  int b = 0;
+  if ((int64_t)blockIdx.x < ntiles) stage(blockIdx.x, 0);
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t next = tile + gridDim.x;
+    if (next < ntiles) {
+      stage(next, b ^ 1);  // overlaps this tile's work
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncthreads();  // this tile's copies (all threads') have landed; sc is set
+    double* sV = smem + b * tsz;
+    double* sw = sV + (size_t)k * tr * F;
+    const int64_t i0 = tile * tr;
+    const int len = (int)(n - i0 < tr ? n - i0 : tr) * F;  // doubles of the tile per column
+    if (MODE != 0 && tid < tr) {
       const int r = tid;
       if (CPLX) {
         double ar = 0.0, ai = 0.0;
         for (int j = 0; j < k; j++) {
-          const double vr = sV[(size_t)j * TR * 2 + 2 * r], vi = sV[(size_t)j * TR * 2 + 2 * r + 1];
-          ar += vr * sc[2 * j] - vi * sc[2 * j + 1];
-          ai += vr * sc[2 * j + 1] + vi * sc[2 * j];
+          const double2 v = *reinterpret_cast<const double2*>(sV + (size_t)j * tr * 2 + 2 * r);
+          ar += v.x * sc[2 * j] - v.y * sc[2 * j + 1];
+          ai += v.x * sc[2 * j + 1] + v.y * sc[2 * j];
         }
         const double xr = sw[2 * r] - ar, xi = sw[2 * r + 1] - ai;
         sw[2 * r] = xr;
@@ -217,7 +265,7 @@ __global__ void __launch_bounds__(RB) lz_tile(const double* __restrict__ V, int6
         }
       } else {
         double a = 0.0;
-        for (int j = 0; j < k; j++) a += sV[(size_t)j * TR + r] * sc[2 * j];
+        for (int j = 0; j < k; j++) a += sV[(size_t)j * tr + r] * sc[2 * j];
         const double x = sw[r] - a;
         sw[r] = x;
         if (r < len) {
@@ -226,30 +274,27 @@ __global__ void __launch_bounds__(RB) lz_tile(const double* __restrict__ V, int6
         }
       }
     }
-    __syncthreads();
-    for (int j = wp; MODE != 2 && j < k; j += RB / 32) {
-      double sr = 0.0, si = 0.0;
-      for (int r = lane; r < TR; r += 32) {
-        if (CPLX) {
-          const double vr = sV[(size_t)j * TR * 2 + 2 * r], vi = sV[(size_t)j * TR * 2 + 2 * r + 1];
-          const double xr = sw[2 * r], xi = sw[2 * r + 1];
-          sr += vr * xr + vi * xi;
-          si += vr * xi - vi * xr;
-        } else {
-          sr += sV[(size_t)j * TR + r] * sw[r];
+    if (MODE != 2) {
+      __syncthreads();  // the subtracted w of the tile is in shared memory
+#pragma unroll
+      for (int q = 0; q < LZ_COLS; q++) {
+        const int j = wp + q * (RB / 32);
+        if (j >= k) break;
+        for (int r = lane; r < tr; r += 32) {
+          if (CPLX) {
+            const double2 v = *reinterpret_cast<const double2*>(sV + (size_t)j * tr * 2 + 2 * r);
+            const double xr = sw[2 * r], xi = sw[2 * r + 1];
+            accr[q] += v.x * xr + v.y * xi;
+            acci[q] += v.x * xi - v.y * xr;
+          } else {
+            accr[q] += sV[(size_t)j * tr + r] * sw[r];
+          }
         }
       }
-      for (int o = 16; o > 0; o >>= 1) {
-        sr += __shfl_xor_sync(0xffffffffu, sr, o);
-        si += __shfl_xor_sync(0xffffffffu, si, o);
-      }
-      if (lane == 0) {
-        sacc[2 * j] += sr;
-        sacc[2 * j + 1] += si;
-      }
     }
+    __syncthreads();  // the buffer is free for the copies two tiles ahead
+    b ^= 1;
   }
-  __syncthreads();
   if constexpr (MODE == 2) {
     for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
     if (lane == 0) sred[wp] = nrm;
@@ -262,7 +307,7 @@ __global__ void __launch_bounds__(RB) lz_tile(const double* __restrict__ V, int6
     if (!lz_last(ticket)) return;
     if (tid < 32) {
       double sq = 0.0;
-      for (int b = tid; b < (int)gridDim.x; b += 32) sq += __ldcg(part + 2 * b);
+      for (int bb = tid; bb < (int)gridDim.x; bb += 32) sq += __ldcg(part + 2 * bb);
       for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
       if (tid == 0) {
         const double beta = sqrt(fmax(sq, 0.0));
@@ -273,9 +318,19 @@ __global__ void __launch_bounds__(RB) lz_tile(const double* __restrict__ V, int6
       }
     }
   } else {
-    for (int j = tid; j < k; j += RB) {
-      part[2 * ((int64_t)j * gridDim.x + blockIdx.x)] = sacc[2 * j];
-      part[2 * ((int64_t)j * gridDim.x + blockIdx.x) + 1] = sacc[2 * j + 1];
+#pragma unroll
+    for (int q = 0; q < LZ_COLS; q++) {
+      const int j = wp + q * (RB / 32);
+      if (j >= k) break;
+      double sr = accr[q], si = acci[q];
+      for (int o = 16; o > 0; o >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        si += __shfl_xor_sync(0xffffffffu, si, o);
+      }
+      if (lane == 0) {
+        part[2 * ((int64_t)j * gridDim.x + blockIdx.x)] = sr;
+        part[2 * ((int64_t)j * gridDim.x + blockIdx.x) + 1] = si;
+      }
     }
     if (!lz_last(ticket)) return;
     lz_final_coef(part, k, cout, T, tdim, jt);
@@ -448,9 +503,12 @@ struct Lanczos {
   int tile_blocks(int k) {
     if (!occ[k]) {
       int b = 1;
-      const size_t sm = lz_tile_smem(k, cplx);
-      cudaError_t e = cplx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lz_tile<true, 1>, RB, sm)
-                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lz_tile<false, 1>, RB, sm);
+      const size_t sm = lz_tile_smem(k, cplx, lz_tile_rows(k, cplx));
+      cudaError_t e =
+          !cplx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lz_tile<false, 1, TR>, RB, sm)
+          : lz_tile_rows(k, cplx) == TR
+              ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lz_tile<true, 1, TR>, RB, sm)
+              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lz_tile<true, 1, TR / 2>, RB, sm);
       occ[k] = (e == cudaSuccess && b > 0) ? std::min(b, 8) : 1;
     }
     return occ[k];
@@ -489,17 +547,25 @@ struct Lanczos {
   int step(int j) {
     if (matvec(col(V, j), w, force64)) return DMRGX_E_CUDA;
     const int k = j + 1;
-    const size_t sm = lz_tile_smem(k, cplx);
-    const int64_t ntiles = (n + TR - 1) / TR;
+    const int tr = lz_tile_rows(k, cplx);
+    const size_t sm = lz_tile_smem(k, cplx, tr);
+    const int64_t ntiles = (n + tr - 1) / tr;
     const int g = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)c->num_sms * tile_blocks(k)));
+    const int vec = (n * (cplx ? 2 : 1)) % 2 == 0;  // columns 16-byte aligned
     if (cplx) {
-      lz_tile<true, 0><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv);
-      lz_tile<true, 1><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv);
-      lz_tile<true, 2><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv);
+      if (tr == TR) {
+        lz_tile<true, 0, TR><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv, vec);
+        lz_tile<true, 1, TR><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv, vec);
+        lz_tile<true, 2, TR><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv, vec);
+      } else {
+        lz_tile<true, 0, TR / 2><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv, vec);
+        lz_tile<true, 1, TR / 2><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv, vec);
+        lz_tile<true, 2, TR / 2><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv, vec);
+      }
     } else {
-      lz_tile<false, 0><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv);
-      lz_tile<false, 1><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv);
-      lz_tile<false, 2><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv);
+      lz_tile<false, 0, TR><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv, vec);
+      lz_tile<false, 1, TR><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv, vec);
+      lz_tile<false, 2, TR><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv, vec);
     }
     vscale<<<grid, RB, 0, s>>>(w, inv, 0.0, col(V, j + 1), len);
     EIG_TRY(cudaGetLastError());
@@ -528,14 +594,25 @@ bool lz_tile_attrs(const char*& why) {
   static int done = 0;  // 1 ok, -1 failed
   static const char* msg = "";
   if (!done) {
-    const int big = (int)lz_tile_smem(MAX_NCV, true);
-    const int bigr = (int)lz_tile_smem(MAX_NCV, false);
-    cudaError_t e = cudaFuncSetAttribute(lz_tile<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(lz_tile<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(lz_tile<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(lz_tile<false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bigr);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(lz_tile<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bigr);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(lz_tile<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bigr);
+    int big = 0, bigr = 0;  // the largest over every basis size
+    for (int k = 1; k <= MAX_NCV; k++) {
+      big = std::max(big, (int)lz_tile_smem(k, true, lz_tile_rows(k, true)));
+      bigr = std::max(bigr, (int)lz_tile_smem(k, false, lz_tile_rows(k, false)));
+    }
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* fn, int bytes) {
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    };
+    set((const void*)lz_tile<true, 0, TR>, big);
+    set((const void*)lz_tile<true, 1, TR>, big);
+    set((const void*)lz_tile<true, 2, TR>, big);
+    set((const void*)lz_tile<true, 0, TR / 2>, big);
+    set((const void*)lz_tile<true, 1, TR / 2>, big);
+    set((const void*)lz_tile<true, 2, TR / 2>, big);
+    set((const void*)lz_tile<false, 0, TR>, bigr);
+    set((const void*)lz_tile<false, 1, TR>, bigr);
+    set((const void*)lz_tile<false, 2, TR>, bigr);
     done = e == cudaSuccess ? 1 : -1;
     if (e != cudaSuccess) msg = cudaGetErrorString(e);
   }

@@ -33,6 +33,8 @@
 
 namespace dmrgx {
 
+double wall_now();  // steady-clock seconds (ctx.cu)
+
 void SplitStage::free_device() {
   for (void* p : {(void*)d_outs, (void*)d_segs, (void*)d_units, (void*)d_cta_begin, (void*)d_reds,
                   (void*)d_redblk, (void*)d_maps})
@@ -440,6 +442,7 @@ int tune_stage(dmrgx_ctx* c, int which) {
 }
 
 int build_split_plan(dmrgx_ctx* c, int eb) {
+  const double t0 = wall_now();
   SplitPlan& sp = c->sp;
   sp.free_device();
   sp = SplitPlan();
@@ -625,10 +628,14 @@ int build_split_plan(dmrgx_ctx* c, int eb) {
   sp.eb = eb;
   rc = upload_vec(sp.psi_jobs, sp.d_psi_jobs, s);
   if (!rc) rc = upload_vec(sp.psi_rows, sp.d_psi_rows, s);
+  SP_TRY(cudaStreamSynchronize(s));
+  const double t1 = wall_now();
   if (!rc) rc = tune_stage(c, 1);
   if (!rc) rc = tune_stage(c, 2);
   if (rc) return rc;
   SP_TRY(cudaStreamSynchronize(s));
+  c->t_plan_part[2] += t1 - t0;
+  c->t_plan_part[3] += wall_now() - t1;
   return 0;
 }
 

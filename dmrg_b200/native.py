@@ -358,9 +358,10 @@ class Context:
 
     def run_seconds(self):
         """Time split of the last dmrg() run: steps, eig, svd, env, fuse, plan (seconds)."""
-        out = np.zeros(6)
-        _check(lib().dmrgx_run_seconds(self.ptr, out.ctypes.data_as(_dp), 6))
-        return dict(zip(("steps", "eig", "svd", "env", "fuse", "plan"), out.tolist()))
+        out = np.zeros(10)
+        _check(lib().dmrgx_run_seconds(self.ptr, out.ctypes.data_as(_dp), 10))
+        return dict(zip(("steps", "eig", "svd", "env", "fuse", "plan", "plan_maps",
+                         "plan_images", "plan_split", "plan_tune"), out.tolist()))
 
     def step_seconds(self):
         """Wall seconds of every site step of the last dmrg() run."""

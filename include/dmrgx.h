@@ -335,7 +335,9 @@ int dmrgx_step_split(dmrgx_ctx* ctx, double* out, int64_t cap, int64_t* nsteps);
 /* Time split of the last dmrgx_dmrg (wall seconds): out[0] all site steps,
  * [1] eigensolver, [2] block SVD, [3] environment update, [4] env (x) MPO fusion,
  * [5] plan building (sector bookkeeping, task lists, device images, split-precision
- * images and tuning).  cap >= 6. */
+ * images and tuning).  cap >= 6.  With cap >= 10 the plan building is also
+ * split: [6] sector bookkeeping and task lists, [7] FP64 images and
+ * descriptors, [8] split-precision images and descriptors, [9] autotuning. */
 int dmrgx_run_seconds(dmrgx_ctx* ctx, double* out, int cap);
 
 /* Gradient of the ground-state energy of the last dmrgx_dmrg with respect to the
