@@ -32,8 +32,10 @@ oracle/_ref by oracle/Makefile) and records:
                       precision (energies, truncation error, entropy, first 20
                       singular values), recorded at the reference's own
                       print_energy / print_singular calls: the small runs of
-                      RUNS (small_full) and BASELINE config 2, XYZ L=64 m=256
-                      n=8 (config2; about an hour on 8 host cores).
+                      RUNS (small_full), BASELINE config 2, XYZ L=64 m=256
+                      n=8 (config2; about an hour on 8 host cores), and
+                      BASELINE config 4's chain, Potts3 L=48 at m=512, on the
+                      reference's growth schedule sweep = -1 (config4).
 
   svd.npz             the reference's block SVD with truncation (qtensor::svd)
                       on captured step states and a graded-spectrum tensor:
@@ -223,6 +225,15 @@ def make_config2():
     record_schedule("xyz_L64_m256", "xyz", "xyz", 64, 256, 8, [1.0, 0.8, 0.5])
 
 
+def make_config4():
+    """Potts3 L=48 at m=512 (f=1, j=1, p=t=0): the reference's dmrg() with
+    sweep = -1, its growth schedule (two_sites, then update_two to the middle
+    with cutoff 512 at every step, src/functions.cpp:169-182).  Bond dimensions
+    reach 512 from the sixth step on.  About half an hour on 8 host cores."""
+    record_schedule("potts_L48_m512_growth", "potts", "potts", 48, 512, -1,
+                    [1.0, 1.0, 0.0, 0.0])
+
+
 def make_small_full():
     """Full-precision rows of the small golden runs (same arguments as RUNS)."""
     for model, (variant, L, m, n, par, gn, ferm, exact_fn) in RUNS.items():
@@ -317,12 +328,13 @@ def make_svd():
 
 
 PARTS = {"steps": make_steps, "microbench": make_microbench, "z2cubed": make_z2cubed,
-         "pbc": make_steps_pbc, "small_full": make_small_full, "svd": make_svd, "config2": make_config2}
+         "pbc": make_steps_pbc, "small_full": make_small_full, "svd": make_svd, "config2": make_config2,
+         "config4": make_config4}
 
 
 def main(parts):
-    # config2 takes about an hour of host time: only when named
-    for name in parts or [p for p in PARTS if p != "config2"]:
+    # config2 and config4 take up to an hour of host time each: only when named
+    for name in parts or [p for p in PARTS if p not in ("config2", "config4")]:
         PARTS[name]()
 
 
