@@ -78,7 +78,10 @@ extern "C" void oref_quiet(int on)
   }
 }
 
-/* ---- ARPACK replacement: same signatures as include/basic.h:12,28-29 ---- */
+/* ---- ARPACK replacement: same signatures as include/basic.h:12,28-29 ----
+   Left out of the drop-in variants (OREF_DROPIN), where the maintainer's file
+   dmrg_b200/dropin/dmrgx_znaupd.cpp provides znaupd on top of libdmrgx.so. */
+#ifndef OREF_DROPIN
 void znaupd(int n, int nev, double* Evals, double* Evecs, lanczos<double>& pass_val)
 {
   if (!g_eig_cb) { cerr << "oracle: no eigensolver callback registered\n"; return; }
@@ -91,6 +94,7 @@ void znaupd(int n, int nev, double* Evals, complex<double>* Evecs,
   if (!g_eig_cb) { cerr << "oracle: no eigensolver callback registered\n"; return; }
   g_eig_cb(n, nev, 1, Evals, (void*)Evecs, (void*)&pass_val);
 }
+#endif
 
 /* ---- the reference matvec on a captured or built context ---- */
 extern "C" void oref_av(int is_complex, void* pv, const void* in, void* out)

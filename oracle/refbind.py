@@ -23,7 +23,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REFDIR = os.path.join(HERE, "_ref")
-VARIANTS = ("kitaev", "xyz", "potts", "u1", "s4e", "kitaev_pbc", "xyz_pbc", "potts_pbc")
+VARIANTS = ("kitaev", "xyz", "potts", "u1", "s4e", "kitaev_pbc", "xyz_pbc", "potts_pbc",
+            "kitaev_dropin", "xyz_dropin", "potts_dropin")
 MODEL = {"kitaev": 0, "xyz": 1, "potts": 2}
 
 _EIG_CB = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double),
