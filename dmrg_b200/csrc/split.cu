@@ -76,20 +76,42 @@ __global__ void __launch_bounds__(64 * RPB) pad_split_kernel(const double* __res
     return;
   }
   uint8_t* row = dst + (jb.dst + (int64_t)pr.row * 2 * jb.kq) * EB;
-  for (int e0 = 0; e0 < gc; e0 += 4 * 64) {
-    double x[4];
+  // VE consecutive padded positions per thread: one 16-byte store of their hi
+  // parts and one of their lo parts (positions past a group's columns are
+  // padding and get zeros)
+  constexpr int VE = 16 / EB;
+  constexpr int CH = 64 / EB;
+  const int span = jb.groups * jb.colsp;
+  for (int k0 = tx * VE; k0 < span; k0 += 64 * VE) {
+    double x[VE];
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int e = e0 + u * 64 + tx;
-      x[u] = e < gc ? __ldg(s + e) : 0.0;
+    for (int u = 0; u < VE; u++) {
+      const int k = k0 + u, grp = k / jb.colsp, j = k - grp * jb.colsp;
+      x[u] = (k < span && j < jb.cols) ? __ldg(s + (int64_t)grp * jb.cols + j) : 0.0;
     }
+    uint32_t hw[4], lw[4];
+    if (EB == 2) {
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int e = e0 + u * 64 + tx;
-      if (e >= gc) break;
-      const int grp = e / jb.cols, j = e - grp * jb.cols;
-      put_pair<EB>(row, (int64_t)grp * jb.colsp + j, x[u]);
+      for (int p = 0; p < 4; p++) {
+        const __nv_bfloat16 h0 = __float2bfloat16_rn((float)x[2 * p]);
+        const __nv_bfloat16 h1 = __float2bfloat16_rn((float)x[2 * p + 1]);
+        const __nv_bfloat16 l0 =
+            __float2bfloat16_rn((float)(x[2 * p] - (double)__bfloat162float(h0)));
+        const __nv_bfloat16 l1 =
+            __float2bfloat16_rn((float)(x[2 * p + 1] - (double)__bfloat162float(h1)));
+        hw[p] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+        lw[p] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+      }
+    } else {
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        hw[p] = tf32_rna((float)x[p]);
+        lw[p] = tf32_rna((float)(x[p] - (double)__uint_as_float(hw[p])));
+      }
     }
+    const int64_t h = pair_off(k0, CH) * EB;  // bytes; 16-aligned (k0 % VE == 0)
+    *reinterpret_cast<uint4*>(row + h) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    *reinterpret_cast<uint4*>(row + h + 64) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
   }
 }
 

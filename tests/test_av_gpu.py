@@ -134,6 +134,37 @@ def test_av_microbench_full_size_against_restatement():
     assert close(y3, 2.0 * y - 0.5 * y2, 1e-12)
 
 
+@pytest.mark.parametrize("cplx", [False, True])
+def test_av_large_blocks_against_restatement(cplx):
+    """Blocks of ~340 rows and columns (three U(1) sectors at m=1024, the shape of
+    a sweep's middle steps), many tiles per block and K up to ~1000 per segment.
+    Real and complex (environment values given complex phases), against the
+    numpy restatement and the per-block library schedule, 1e-12 relative."""
+    w = workloads.microbench(1024, qmax=1, width=1e9)
+    lm, lv = w["lenv"]
+    rm, rv = w["renv"]
+    if cplx:
+        rng = np.random.default_rng(5)
+        lv = lv * np.exp(1j * rng.uniform(0, 2 * np.pi, lv.size))
+        rv = rv * np.exp(1j * rng.uniform(0, 2 * np.pi, rv.size))
+    ctx = native.Context(native.C128 if cplx else native.F64)
+    ctx.plan_build((lm, lv), (rm, rv), 3, 2, w["sector"], 32, 0)
+    le = restate.QT.from_ibuf(lm, lv)
+    re_ = restate.QT.from_ibuf(rm, rv)
+    rmap, lmap = ctx.maps()
+    assert max(le.blocks[r[0]].size // r[4] for r in lmap) >= 256
+    x = workloads.random_psi(ctx.n, seed=2, complex_=cplx)
+    store = np.zeros(ctx.d_store, x.dtype)
+    restate.contract_map(re_, store, x, rmap, 2)
+    ref = np.zeros(ctx.n, x.dtype)
+    restate.contract_map(le, ref, store, lmap, 3)
+    y = ctx.av(x)
+    assert close(y, ref, 1e-12)
+    ctx.set_schedule(native.SCHED_PER_BLOCK)
+    assert close(ctx.av(x), y, 1e-12)
+    ctx.close()
+
+
 @pytest.mark.parametrize("model", MODELS)
 def test_av_is_hermitian_on_physical_steps(model):
     """<u|H v> = <H u|v>: the reference's check_hermitian (src/core.cpp:40-83) as a
