@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(RB) lz_tile(const double* __restrict__ V, int6
                                               double* __restrict__ part, unsigned* ticket,
                                               double* __restrict__ cout, double* __restrict__ T,
                                               int tdim, int jt, double* __restrict__ inv,
-                                              int vec) {
+                                              int vec, int rev) {
   constexpr int F = CPLX ? 2 : 1;
   constexpr int tr = TRT;
   constexpr int EPC = tr * F;          // doubles of one column in a tile
@@ -231,12 +231,16 @@ __global__ void __launch_bounds__(RB) lz_tile(const double* __restrict__ V, int6
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
+  // rev: the tiles are walked from the end, so that a pass starts on the rows the
+  // previous pass (the other direction) read last and L2 still holds
+  auto at = [&](int64_t q) { return rev ? ntiles - 1 - q : q; };
   int b = 0;
-  if ((int64_t)blockIdx.x < ntiles) stage(blockIdx.x, 0);
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int64_t next = tile + gridDim.x;
+  if ((int64_t)blockIdx.x < ntiles) stage(at(blockIdx.x), 0);
+  for (int64_t q = blockIdx.x; q < ntiles; q += gridDim.x) {
+    const int64_t tile = at(q);
+    const int64_t next = q + gridDim.x;
     if (next < ntiles) {
-      stage(next, b ^ 1);  // overlaps this tile's work
+      stage(at(next), b ^ 1);  // overlaps this tile's work
       asm volatile("cp.async.wait_group 1;\n" ::: "memory");
     } else {
       asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -554,18 +558,18 @@ struct Lanczos {
     const int vec = (n * (cplx ? 2 : 1)) % 2 == 0;  // columns 16-byte aligned
     if (cplx) {
       if (tr == TR) {
-        lz_tile<true, 0, TR><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv, vec);
-        lz_tile<true, 1, TR><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv, vec);
-        lz_tile<true, 2, TR><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv, vec);
+        lz_tile<true, 0, TR><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv, vec, (3 * j + 0) & 1);
+        lz_tile<true, 1, TR><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv, vec, (3 * j + 1) & 1);
+        lz_tile<true, 2, TR><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv, vec, (3 * j + 2) & 1);
       } else {
-        lz_tile<true, 0, TR / 2><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv, vec);
-        lz_tile<true, 1, TR / 2><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv, vec);
-        lz_tile<true, 2, TR / 2><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv, vec);
+        lz_tile<true, 0, TR / 2><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv, vec, (3 * j + 0) & 1);
+        lz_tile<true, 1, TR / 2><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv, vec, (3 * j + 1) & 1);
+        lz_tile<true, 2, TR / 2><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv, vec, (3 * j + 2) & 1);
       }
     } else {
-      lz_tile<false, 0, TR><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv, vec);
-      lz_tile<false, 1, TR><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv, vec);
-      lz_tile<false, 2, TR><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv, vec);
+      lz_tile<false, 0, TR><<<g, RB, sm, s>>>(V, n, k, nullptr, w, n, part2, ticket, coef, T, tdim, j, inv, vec, (3 * j + 0) & 1);
+      lz_tile<false, 1, TR><<<g, RB, sm, s>>>(V, n, k, coef, w, n, part2, ticket, coef2, T, tdim, j, inv, vec, (3 * j + 1) & 1);
+      lz_tile<false, 2, TR><<<g, RB, sm, s>>>(V, n, k, coef2, w, n, part2, ticket, nullptr, T, tdim, j, inv, vec, (3 * j + 2) & 1);
     }
     vscale<<<grid, RB, 0, s>>>(w, inv, 0.0, col(V, j + 1), len);
     EIG_TRY(cudaGetLastError());
