@@ -142,6 +142,29 @@ def test_config2_xyz_L64_m256_full_precision(solver):
           "GPU s", r["seconds"]["total"], "reference s", float(g["ref_seconds"]))
 
 
+@pytest.mark.parametrize("prec", ["fp64", "bf16x3"])
+def test_config4_potts_L48_m512_growth_full_precision(prec):
+    """BASELINE config 4's chain at its bond dimension: the 3-state Potts chain
+    L=48 (f=1, j=1, complex128, Z3 sectors) on the reference's dmrg() growth
+    schedule sweep = -1 (src/functions.cpp:169-182: two_sites, then update_two
+    to the middle with cutoff 512 at every step; the full schedule runs for
+    hours on the host).  Bond dimensions reach 512 from the sixth step on.
+    Every one of the 24 steps against the reference run recorded in full
+    precision: energies to 1e-10 relative, truncation errors, entropies and
+    singular values to the bars above.  "bf16x3": the split-precision matvec
+    with FP64 defect correction, to the same bars."""
+    g = load_schedule("potts_L48_m512_growth")
+    L, m, n, sector = (int(v) for v in g["args"])
+    ctx = native.Context(native.C128)
+    if prec == "bf16x3":
+        ctx.set_precision(native.PREC_BF16X3)
+    r = ctx.dmrg("potts", L, m, n, g["params"].tolist(), sector=sector)
+    assert r["nsv"].max() >= 512
+    print("config 4", prec, "max dE/E %.1e dtrunc %.1e dS %.1e ds %.1e" % check_schedule(r, g),
+          "E", r["energies"][-1, 0], "GPU s", r["seconds"]["total"],
+          "reference s", float(g["ref_seconds"]))
+
+
 with open(os.path.join(GOLDEN, "energies_pbc.json")) as fh:
     GOLD_PBC = json.load(fh)
 
