@@ -50,7 +50,47 @@ def parse():
     p.add_argument("--sweep-L", type=int, default=32)
     p.add_argument("--sweep-m", type=int, default=1024)
     p.add_argument("--sweep-n", type=int, default=1)
+    p.add_argument("--probe", default="", choices=["", "eig", "mv"],
+                   help="profiling workload instead of the benchmark: the state at the middle "
+                        "of an XYZ chain (L=--sweep-L, m=--sweep-m, fast solver schedule), then "
+                        "one eigensolve with the reference's settings (eig) or one matvec (mv) "
+                        "in the headline precision, inside the NVTX range 'probe'")
     return p.parse_args()
+
+
+def run_probe(args):
+    """A sweep step's matvec / eigensolve at full size, for ncu captures
+    (ncu --nvtx --nvtx-include "probe/" ...).  Prints one JSON line."""
+    import time
+    import torch
+    from dmrg_b200 import native
+    prec = {"fp64": native.PREC_FP64, "bf16x3": native.PREC_BF16X3,
+            "tf32x3": native.PREC_TF32X3}[args.prec]
+    c = native.Context(native.F64)
+    c.set_solver(1, 12, True)
+    c.dmrg("xyz_real", args.sweep_L, args.sweep_m, 0, [1.0, 0.8, 0.5])
+    c._refresh()
+    c.set_precision(prec)
+    x = torch.randn(c.n, dtype=torch.float64, device="cuda:0")
+    y = torch.empty_like(x)
+    for _ in range(3):                       # split images, tuning, warm caches
+        c.av_device(x.data_ptr(), y.data_ptr())
+    if args.probe == "eig":
+        c.eigsolve(nev=6)
+    c.sync()
+    torch.cuda.nvtx.range_push("probe")
+    t0 = time.time()
+    if args.probe == "eig":
+        _, _, info = c.eigsolve(nev=6)
+    else:
+        c.av_device(x.data_ptr(), y.data_ptr())
+        info = {"matvecs": 1}
+    c.sync()
+    dt = time.time() - t0
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"probe": args.probe, "n": c.n, "gflop_per_matvec": c.flops / 1e9,
+                      "precision": args.prec, "seconds": dt, "matvecs": info["matvecs"],
+                      "us_per_step": dt / info["matvecs"] * 1e6}))
 
 
 def dist_init(args):
@@ -338,6 +378,9 @@ def main():
     from dmrg_b200 import native, workloads
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
+    if args.probe:
+        run_probe(args)
+        return
     prec = {"fp64": native.PREC_FP64, "bf16x3": native.PREC_BF16X3,
             "tf32x3": native.PREC_TF32X3}[args.prec]
 

@@ -167,8 +167,9 @@ __device__ __forceinline__ void lz_final_coef(const double* part, int k, double*
 
 // dynamic shared memory of lz_tile for k basis columns (bytes): two tile
 // buffers (basis slice and w), the coefficients, per-warp norm partials
+constexpr int LZ_BUF = 3;  // tile buffers: copies run two tiles ahead of the work
 __host__ __device__ constexpr size_t lz_tile_smem(int k, bool cplx, int tr) {
-  return sizeof(double) * (2 * ((size_t)k * tr * (cplx ? 2 : 1) + tr * (cplx ? 2 : 1)) +
+  return sizeof(double) * (LZ_BUF * ((size_t)k * tr * (cplx ? 2 : 1) + tr * (cplx ? 2 : 1)) +
                            2 * MAX_NCV + RB / 32);
 }
 // rows per tile: TR, or TR / 2 where two TR-row buffers would not fit
@@ -192,7 +193,7 @@ __global__ void __launch_bounds__(RB) lz_tile(const double* __restrict__ V, int6
   constexpr int CPC = EPC / 2;         // 16-byte chunks of one column
   extern __shared__ double smem[];
   const size_t tsz = (size_t)k * tr * F + tr * F;  // one buffer: slice then w
-  double* sc = smem + 2 * tsz;                     // cin (pairs)
+  double* sc = smem + LZ_BUF * tsz;                // cin (pairs)
   double* sred = sc + 2 * MAX_NCV;                 // per-warp norm partials (MODE 2)
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   if (MODE != 0)
@@ -234,17 +235,23 @@ __global__ void __launch_bounds__(RB) lz_tile(const double* __restrict__ V, int6
   // rev: the tiles are walked from the end, so that a pass starts on the rows the
   // previous pass (the other direction) read last and L2 still holds
   auto at = [&](int64_t q) { return rev ? ntiles - 1 - q : q; };
+  // tile i of this block sits in buffer i % LZ_BUF; the copies of tiles i + 1
+  // and i + 2 are in flight while tile i is worked on (one commit group per
+  // tile, empty past the end, so wait_group LZ_BUF - 1 always means "tile i")
   int b = 0;
-  if ((int64_t)blockIdx.x < ntiles) stage(at(blockIdx.x), 0);
+#pragma unroll
+  for (int u = 0; u < LZ_BUF - 1; u++) {
+    const int64_t q0 = blockIdx.x + (int64_t)u * gridDim.x;
+    if (q0 < ntiles) stage(at(q0), u);
+    else asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
   for (int64_t q = blockIdx.x; q < ntiles; q += gridDim.x) {
     const int64_t tile = at(q);
-    const int64_t next = q + gridDim.x;
-    if (next < ntiles) {
-      stage(at(next), b ^ 1);  // overlaps this tile's work
-      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-    } else {
-      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    }
+    const int64_t ahead = q + (int64_t)(LZ_BUF - 1) * gridDim.x;
+    const int ba = (b + LZ_BUF - 1) % LZ_BUF;  // the buffer of tile i - 1: free
+    if (ahead < ntiles) stage(at(ahead), ba);
+    else asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(LZ_BUF - 1) : "memory");
     __syncthreads();  // this tile's copies (all threads') have landed; sc is set
     double* sV = smem + b * tsz;
     double* sw = sV + (size_t)k * tr * F;
@@ -296,8 +303,8 @@ __global__ void __launch_bounds__(RB) lz_tile(const double* __restrict__ V, int6
         }
       }
     }
-    __syncthreads();  // the buffer is free for the copies two tiles ahead
-    b ^= 1;
+    __syncthreads();  // the buffer is free for the copies LZ_BUF - 1 tiles ahead
+    b = (b + 1) % LZ_BUF;
   }
   if constexpr (MODE == 2) {
     for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
