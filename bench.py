@@ -88,9 +88,18 @@ def run_probe(args):
     c.sync()
     dt = time.time() - t0
     torch.cuda.nvtx.range_pop()
+    # per-launch device time of 20 more matvecs (outside the NVTX range)
+    c.profile(True)
+    for _ in range(20):
+        c.av_device(x.data_ptr(), y.data_ptr())
+    cnt, slots = c.profile_read()
+    c.profile(False)
+    info["stage_us"] = (slots / max(cnt, 1) * 1e3).round(1).tolist()
+    info["tuning"] = [list(t) for t in c.split_tuning()] if prec != native.PREC_FP64 else None
     print(json.dumps({"probe": args.probe, "n": c.n, "gflop_per_matvec": c.flops / 1e9,
                       "precision": args.prec, "seconds": dt, "matvecs": info["matvecs"],
-                      "us_per_step": dt / info["matvecs"] * 1e6}))
+                      "us_per_step": dt / info["matvecs"] * 1e6,
+                      "matvec_stage_us": info["stage_us"], "tuning": info["tuning"]}, default=float))
 
 
 def dist_init(args):
