@@ -366,33 +366,61 @@ __global__ void vresid(const double* __restrict__ x, const double* __restrict__ 
     y[i] = x[i] - theta * v[i];
 }
 
-// Vout[:, q] = sum_j V[:, j] Y[j, q], q < k (Y real, column-major m x k)
-template <bool CPLX>
+// Vout[:, q] = sum_j V[:, j] Y[j, q], q < k (Y real, column-major m x k): the
+// thick restart's rotation.  Row tiles of RB rows x m columns are staged in
+// shared memory by cp.async (16-byte copies when the columns are 16-byte
+// aligned), then each thread forms its row's k outputs from shared memory and
+// writes them (coalesced across the block).
+template <bool CPLX, int TRR>
 __global__ void __launch_bounds__(RB) vrotate(const double* __restrict__ V, int64_t ld, int m,
                                               const double* __restrict__ Y, int k,
-                                              double* __restrict__ Vout, int64_t n) {
-  extern __shared__ double sY[];
-  for (int t = threadIdx.x; t < m * k; t += blockDim.x) sY[t] = Y[t];
-  __syncthreads();
+                                              double* __restrict__ Vout, int64_t n, int vec) {
   constexpr int F = CPLX ? 2 : 1;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    double x[F * MAX_NCV];
-    for (int j = 0; j < m; j++) {
-      x[F * j] = V[F * (j * ld + i)];
-      if (CPLX) x[F * j + 1] = V[F * (j * ld + i) + 1];
+  constexpr int EPC = TRR * F;  // doubles of one column in a tile (TRR <= RB rows)
+  extern __shared__ double rsm[];
+  double* sY = rsm;                            // m * k
+  double* sV = rsm + ((m * k + 1) & ~1);       // column j at sV[j * EPC], 16-byte aligned
+  for (int t = threadIdx.x; t < m * k; t += RB) sY[t] = Y[t];
+  const int64_t ntiles = (n + TRR - 1) / TRR;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t i0 = tile * TRR;
+    const int len = (int)(n - i0 < TRR ? n - i0 : TRR) * F;
+    __syncthreads();  // the previous tile is consumed (and sY is set)
+    if (vec) {
+      constexpr int CPC = EPC / 2;
+      const int c = threadIdx.x % CPC, e = 2 * c;
+      const int bytes = e + 2 <= len ? 16 : (e < len ? 8 : 0);
+      for (int j = threadIdx.x / CPC; j < m; j += RB / CPC)
+        cp_async16(sV + j * EPC + e, bytes ? V + (int64_t)j * ld * F + i0 * F + e : V, bytes);
+    } else {
+      const int e = threadIdx.x % EPC;
+      for (int j = threadIdx.x / EPC; j < m; j += RB / EPC)
+        cp_async8(sV + j * EPC + e, e < len ? V + (int64_t)j * ld * F + i0 * F + e : V, e < len);
     }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    const int r = threadIdx.x;
+    if (r >= TRR || r * F >= len) continue;
     for (int q = 0; q < k; q++) {
       double ar = 0.0, ai = 0.0;
       for (int j = 0; j < m; j++) {
         const double y = sY[q * m + j];
-        ar += x[F * j] * y;
-        if (CPLX) ai += x[F * j + 1] * y;
+        ar += sV[j * EPC + r * F] * y;
+        if (CPLX) ai += sV[j * EPC + r * F + 1] * y;
       }
-      Vout[F * (q * ld + i)] = ar;
-      if (CPLX) Vout[F * (q * ld + i) + 1] = ai;
+      Vout[(int64_t)q * ld * F + (i0 + r) * F] = ar;
+      if (CPLX) Vout[(int64_t)q * ld * F + (i0 + r) * F + 1] = ai;
     }
   }
+}
+
+// dynamic shared memory of vrotate (bytes) with tiles of `rows` rows
+size_t vrotate_smem(int m, int k, bool cplx, int rows) {
+  return sizeof(double) * (((size_t)m * k + 1) / 2 * 2 + (size_t)m * rows * (cplx ? 2 : 1));
+}
+// tile rows of vrotate: RB, or RB / 2 for a wide complex basis (shared memory)
+int vrotate_rows(int m, bool cplx) {
+  return vrotate_smem(m, MAX_NCV, cplx, RB) <= (200u << 10) ? RB : RB / 2;
 }
 
 // Cyclic Jacobi eigen-decomposition of a small real symmetric matrix (FP64).
@@ -539,10 +567,18 @@ struct Lanczos {
   }
 
   void rotate(const double* Vin, int mm, int k, double* Vout) {
-    if (cplx)
-      vrotate<true><<<grid, RB, sizeof(double) * mm * k, s>>>(Vin, n, mm, Y, k, Vout, n);
+    const int rows = vrotate_rows(mm, cplx);
+    const size_t sm = vrotate_smem(mm, k, cplx, rows);
+    const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, (200u << 10) / sm));
+    const int64_t ntiles = (n + rows - 1) / rows;
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)c->num_sms * per_sm));
+    const int vec = (n * (cplx ? 2 : 1)) % 2 == 0;
+    if (cplx && rows == RB)
+      vrotate<true, RB><<<g, RB, sm, s>>>(Vin, n, mm, Y, k, Vout, n, vec);
+    else if (cplx)
+      vrotate<true, RB / 2><<<g, RB, sm, s>>>(Vin, n, mm, Y, k, Vout, n, vec);
     else
-      vrotate<false><<<grid, RB, sizeof(double) * mm * k, s>>>(Vin, n, mm, Y, k, Vout, n);
+      vrotate<false, RB><<<g, RB, sm, s>>>(Vin, n, mm, Y, k, Vout, n, vec);
   }
   // host value of <x, x>
   int norm2(const double* x, double& out) {
@@ -624,6 +660,9 @@ bool lz_tile_attrs(const char*& why) {
     set((const void*)lz_tile<false, 0, TR>, bigr);
     set((const void*)lz_tile<false, 1, TR>, bigr);
     set((const void*)lz_tile<false, 2, TR>, bigr);
+    set((const void*)vrotate<true, RB>, 200 << 10);
+    set((const void*)vrotate<true, RB / 2>, 200 << 10);
+    set((const void*)vrotate<false, RB>, 200 << 10);
     done = e == cudaSuccess ? 1 : -1;
     if (e != cudaSuccess) msg = cudaGetErrorString(e);
   }

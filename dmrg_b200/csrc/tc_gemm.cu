@@ -102,6 +102,10 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
       : "memory");
 }
+// bring a tensor map (global memory) into the TMA descriptor cache
+__device__ __forceinline__ void prefetch_map(const CUtensorMap* m) {
+  asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(m)) : "memory");
+}
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
   // K-major, 128-byte swizzle: LBO unused (1), SBO = 1 KB, version 1, layout 2
   return (uint64_t)((addr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(SBO >> 4) << 32) |
@@ -292,6 +296,20 @@ tc_grouped_gemm(const CUtensorMap* __restrict__ maps, const SUnit* __restrict__ 
   tc_fence_after();
   // programmatic dependent launch: the set-up above may overlap the previous
   // kernel's tail; operands and outputs are touched only after it completed
+  // the tensor maps of this CTA's units go to the descriptor cache while the
+  // previous kernel finishes: maps, units and segments are plan data, written
+  // before any kernel of the matvec (operands are read only after pdl_wait)
+  if (warp == 0) {
+    const int ub = cta_begin[blockIdx.x], ue = cta_begin[blockIdx.x + 1];
+    for (int u = ub; u < ue; u++) {
+      const SOut o = outs[units[u].out];
+      for (int q = lane; q < o.seg_count; q += 32) {
+        const SSeg2 sg = segs[o.seg_begin + q];
+        prefetch_map(maps + sg.amap);
+        prefetch_map(maps + sg.bmap);
+      }
+    }
+  }
   pdl_wait();
   pdl_launch_dependents();
   const uint32_t tmem = *tmem_slot;
