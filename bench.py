@@ -44,6 +44,9 @@ def parse():
     p.add_argument("--prec", default="bf16x3", choices=["fp64", "bf16x3", "tf32x3"])
     p.add_argument("--impl", default="dmrgx", choices=["dmrgx", "reference"])
     p.add_argument("--cpu-sample-s", type=float, default=12.0)
+    p.add_argument("--config1", type=int, default=1,
+                   help="1: BASELINE config 1 (Kitaev L=32, m=64, 6 sweeps) on the GPU beside the "
+                        "reference's own run on the host cores")
     p.add_argument("--sweep", type=int, default=1,
                    help="also time the DMRG schedule (XYZ real chain) in three forms: plain "
                         "per-block FP64, grouped FP64, grouped headline precision")
@@ -305,6 +308,60 @@ def sweep_compare(native, args):
     return out
 
 
+def config1_compare(native):
+    """BASELINE config 1 end to end, GPU beside the reference on the host: the Kitaev
+    chain L=32 (t=1, Delta=1, mu=0.5 -> u=0.25), the reference's dmrg() schedule to
+    m=64 with 6 sweeps.  The reference run is its own code (oracle/_ref, ARPACK
+    settings, OpenBLAS on all host threads), timed in this process; the GPU runs
+    the same schedule in FP64 and BF16x3 with the reference's solver settings,
+    and in FP64 with the fast settings.  Reports wall seconds, the final energies
+    against the exact BdG value, and the largest per-step energy differences
+    between the GPU FP64 runs and the reference."""
+    from oracle import exact, refbind
+    L, m, n, par = 32, 64, 6, [1.0, 1.0, 0.25]
+    out = {"workload": "Kitaev chain L=32, t=1, Delta=1, mu=0.5, m=64, 6 sweeps, "
+                       "reference dmrg() schedule, FP64 real"}
+    runs = {}
+    # the reference's solver settings in both precisions, then the fast settings
+    # (lowest value only, 12-vector basis, White's prediction) in FP64
+    for name, prec, fast in (("fp64", native.PREC_FP64, False),
+                             ("bf16x3", native.PREC_BF16X3, False),
+                             ("fp64_fast", native.PREC_FP64, True)):
+        c = native.Context(native.F64)
+        c.set_precision(prec)
+        if fast:
+            c.set_solver(1, 12, True)
+        t0 = time.perf_counter()
+        r = c.dmrg("kitaev", L, m, n, par)
+        runs[name] = (time.perf_counter() - t0, r)
+        runs[name][1]["split_s"] = c.run_seconds()
+        c.close()
+    e_bdg = exact.kitaev_bdg(L, *par)
+    out["bdg_energy"] = e_bdg
+    for name, (secs, r) in runs.items():
+        e = float(r["energies"][-1, 0])
+        out["gpu_" + name] = {"seconds": secs, "energy": e, "dE_rel_vs_bdg": abs(e - e_bdg) / abs(e_bdg),
+                              "matvecs": int(r["matvecs"].sum()),
+                              "split_s": {k: round(v, 4) for k, v in r["split_s"].items()}}
+    if refbind.available("kitaev"):
+        R = refbind.Ref("kitaev")
+        t0 = time.perf_counter()
+        res = R.run("kitaev", L, m, n, 0, par)
+        secs = time.perf_counter() - t0
+        e_ref = np.array([row["evals"][0] for row in res["en"]])
+        out["reference"] = {"seconds": secs, "threads": os.cpu_count(), "energy": float(e_ref[-1]),
+                            "kind": "reference (its own code built from its sources, ARPACK "
+                                    "settings, OpenBLAS on all host threads)"}
+        for name in ("fp64", "fp64_fast"):
+            e_gpu = runs[name][1]["energies"][:, 0]
+            if e_ref.shape == e_gpu.shape:
+                out["max_step_dE_rel_%s_vs_reference" % name] = float(
+                    np.max(np.abs(e_gpu - e_ref) / np.abs(e_ref)))
+        for name in runs:
+            out["speedup_" + name + "_vs_reference"] = secs / runs[name][0]
+    return out
+
+
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
@@ -448,6 +505,13 @@ def main():
         fp64 = {"value": args.steps / f_s, "ms_per_step": 1e3 * f_s / args.steps,
                 "stage_ms": [float(x / fc) for x in fslots[1:]],
                 "tflops": flops / (float(fslots[1] + fslots[2]) / fc / 1e3) / 1e12}
+        # the FP64 path's own roofline: the FP64 tensor-core (DMMA) ceiling, measured
+        # in-run by a cuBLAS DGEMM burst (the peak file has no FP64 figure)
+        pk64 = fp64_gemm_peak(torch, dev)
+        fp64["roofline"] = {"bound": "tensor", "achieved": fp64["tflops"], "peak": pk64,
+                            "unit": "TFLOP/s", "frac": fp64["tflops"] / pk64,
+                            "kernel": "grouped_gemm_nt_f64 (stage 1 + stage 2 launches)",
+                            "peak_source": "in-run cuBLAS DGEMM 8192^3 burst"}
 
     ysp = torch.empty_like(xs)
     p_s, _ = time_matvecs(torch, plain, plain_stream, xs, ysp, flush, args.steps, args.warmup)
@@ -488,6 +552,7 @@ def main():
             kernel = "grouped_split_tc<tf32> (stage 1 + stage 2 launches)"
         cpu = cpu_reference_rate(args.cpu_sample_s, w)
         sweep = sweep_compare(native, args) if args.sweep else None
+        cfg1 = config1_compare(native) if args.config1 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
@@ -517,6 +582,8 @@ def main():
         }
         if sweep is not None:
             line["sweep"] = sweep
+        if cfg1 is not None:
+            line["config1"] = cfg1
         line["plain_fp64_path"] = plain_path
         line["vs_plain_fp64"] = value / plain_path["value"]
         if fp64 is not None:
