@@ -573,6 +573,7 @@ void dmrgx_ctx_destroy(dmrgx_ctx* c) {
   c->st1.free_device();
   c->st2.free_device();
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+  for (auto& g : c->cycle_graphs) cudaGraphExecDestroy(g.second);
   c->sp.free_device();
   for (DevBuf* b : {&c->sa1, &c->sa2, &c->spsi, &c->sstore, &c->sws, &c->err})
     b->release();

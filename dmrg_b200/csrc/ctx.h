@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <map>
 #include <vector>
 
 #include "grouped.h"
@@ -132,6 +133,8 @@ struct dmrgx_ctx {
   // descriptors (uploads included), [2] split-precision images and
   // descriptors, [3] autotuning
   double t_plan_part[4] = {0, 0, 0, 0};
+  // instantiated Lanczos cycle graphs kept between solves (eig.cu)
+  std::map<int64_t, cudaGraphExec_t> cycle_graphs;
   // results of the last dmrgx_svd: U and V (metadata, values) and the spectrum
   std::vector<int> svd_um, svd_vm;
   std::vector<double> svd_uv, svd_vv, svd_s;

@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <string>
 #include <vector>
 
@@ -476,6 +477,108 @@ void jacobi_eig(std::vector<double> A, int m, std::vector<double>& w, std::vecto
   }
 }
 
+// Symmetric eigen-decomposition of a small real matrix (FP64) in O(m^3) with a
+// small constant: Householder reduction to tridiagonal form, then implicit
+// symmetric QR steps with Wilkinson shifts (Golub & Van Loan, Matrix
+// Computations, sections 8.3.1 and 8.3.2), rotations accumulated into the
+// eigenvectors.  Same outputs as jacobi_eig: w ascending, Z[j*m+q] = component
+// j of eigenvector q.  Returns false if an eigenvalue did not converge in
+// 30 m steps (the caller then uses jacobi_eig).
+bool tridiag_qr_eig(std::vector<double> A, int m, std::vector<double>& w, std::vector<double>& Z) {
+  std::vector<double> Q((size_t)m * m, 0.0);  // Q[i*m+j]: row i, column j
+  for (int i = 0; i < m; i++) Q[(size_t)i * m + i] = 1.0;
+  std::vector<double> v(m), pv(m);
+  // ---- A = Q T Q^T: for column k, a reflector H = I - 2 v v^T (v unit, zero
+  // in rows <= k) maps A[k+1:, k] onto a multiple of e_{k+1}
+  for (int k = 0; k + 2 < m; k++) {
+    double nx = 0.0;
+    for (int i = k + 1; i < m; i++) nx += A[(size_t)i * m + k] * A[(size_t)i * m + k];
+    nx = std::sqrt(nx);
+    if (nx == 0.0) continue;
+    const double x0 = A[(size_t)(k + 1) * m + k];
+    const double alpha = x0 >= 0 ? -nx : nx;
+    for (int i = 0; i < m; i++) v[i] = 0.0;
+    v[k + 1] = x0 - alpha;
+    for (int i = k + 2; i < m; i++) v[i] = A[(size_t)i * m + k];
+    double nv = 0.0;
+    for (int i = k + 1; i < m; i++) nv += v[i] * v[i];
+    nv = std::sqrt(nv);
+    if (nv == 0.0) continue;
+    for (int i = k + 1; i < m; i++) v[i] /= nv;
+    // trailing block: A22 <- H A22 H = A22 - 2 v q^T - 2 q v^T, q = p - (v^T p) v, p = A22 v
+    double vp = 0.0;
+    for (int i = k + 1; i < m; i++) {
+      double t = 0.0;
+      for (int j = k + 1; j < m; j++) t += A[(size_t)i * m + j] * v[j];
+      pv[i] = t;
+      vp += v[i] * t;
+    }
+    for (int i = k + 1; i < m; i++) pv[i] -= vp * v[i];
+    for (int i = k + 1; i < m; i++)
+      for (int j = k + 1; j < m; j++)
+        A[(size_t)i * m + j] -= 2.0 * (v[i] * pv[j] + pv[i] * v[j]);
+    A[(size_t)(k + 1) * m + k] = A[(size_t)k * m + k + 1] = alpha;
+    for (int i = k + 2; i < m; i++) A[(size_t)i * m + k] = A[(size_t)k * m + i] = 0.0;
+    // Q <- Q H
+    for (int i = 0; i < m; i++) {
+      double t = 0.0;
+      for (int j = k + 1; j < m; j++) t += Q[(size_t)i * m + j] * v[j];
+      for (int j = k + 1; j < m; j++) Q[(size_t)i * m + j] -= 2.0 * t * v[j];
+    }
+  }
+  std::vector<double> a(m), b(std::max(m - 1, 1), 0.0);
+  for (int i = 0; i < m; i++) a[i] = A[(size_t)i * m + i];
+  for (int i = 0; i + 1 < m; i++) b[i] = A[(size_t)(i + 1) * m + i];
+  // ---- implicit symmetric QR on (a, b): chase the bulge of a Wilkinson-shifted
+  // rotation down the unreduced block [l, h]; deflate negligible b from the bottom
+  const double eps = std::numeric_limits<double>::epsilon();
+  int h = m - 1, steps = 0;
+  while (h > 0) {
+    if (std::fabs(b[h - 1]) <= eps * (std::fabs(a[h - 1]) + std::fabs(a[h]))) {
+      b[h - 1] = 0.0;
+      h--;
+      continue;
+    }
+    if (++steps > 30 * m) return false;
+    int l = h - 1;
+    while (l > 0 && std::fabs(b[l - 1]) > eps * (std::fabs(a[l - 1]) + std::fabs(a[l]))) l--;
+    const double d = 0.5 * (a[h - 1] - a[h]);
+    const double r0 = std::hypot(d, b[h - 1]);
+    const double mu = a[h] - b[h - 1] * b[h - 1] / (d + (d >= 0 ? r0 : -r0));
+    double x = a[l] - mu, z = b[l];
+    for (int k = l; k < h; k++) {
+      // rotation of rows / columns k, k+1 taking (x, z) to (r, 0)
+      const double r = std::hypot(x, z);
+      const double c = r > 0 ? x / r : 1.0, s = r > 0 ? z / r : 0.0;
+      if (k > l) b[k - 1] = r;
+      const double ak = a[k], ak1 = a[k + 1], bk = b[k];
+      a[k] = c * c * ak + 2.0 * c * s * bk + s * s * ak1;
+      a[k + 1] = s * s * ak - 2.0 * c * s * bk + c * c * ak1;
+      b[k] = c * s * (ak1 - ak) + (c * c - s * s) * bk;
+      if (k + 1 < h) {  // the rotation carries b[k+1] into the bulge at (k+2, k)
+        z = s * b[k + 1];
+        b[k + 1] *= c;
+        x = b[k];
+      }
+      for (int i = 0; i < m; i++) {
+        const double qk = Q[(size_t)i * m + k], qk1 = Q[(size_t)i * m + k + 1];
+        Q[(size_t)i * m + k] = c * qk + s * qk1;
+        Q[(size_t)i * m + k + 1] = -s * qk + c * qk1;
+      }
+    }
+  }
+  std::vector<int> idx(m);
+  for (int i = 0; i < m; i++) idx[i] = i;
+  std::sort(idx.begin(), idx.end(), [&](int x1, int x2) { return a[x1] < a[x2]; });
+  w.resize(m);
+  Z.assign((size_t)m * m, 0.0);
+  for (int q = 0; q < m; q++) {
+    w[q] = a[idx[q]];
+    for (int j = 0; j < m; j++) Z[(size_t)j * m + q] = Q[(size_t)j * m + idx[q]];
+  }
+  return true;
+}
+
 struct DevMem {
   std::vector<void*> ptrs;
   cudaStream_t s = nullptr;
@@ -774,13 +877,13 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
     const double* V;
     cudaGraphExec_t exec;
   };
+  // The instantiated graphs stay in the context (c->cycle_graphs) for the next
+  // solves, keyed by (first step, basis buffer slot, basis size): a new capture
+  // with the same topology -- the usual case from one site step to the next --
+  // updates the old executable in place (cudaGraphExecUpdate) instead of
+  // instantiating a new one.
   std::vector<CycleGraph> graphs;
-  struct GraphFree {
-    std::vector<CycleGraph>& g;
-    ~GraphFree() {
-      for (auto& x : g) cudaGraphExecDestroy(x.exec);
-    }
-  } graph_free{graphs};
+  const double* v_first = L.V;  // the basis buffer V starts in (restarts swap V and V2)
   const bool use_graph = !c->per_block && !c->prof && !getenv("DMRGX_NO_GRAPH");
   auto run_cycle = [&](int first) -> int {
     if (use_graph) {
@@ -796,7 +899,24 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
         for (int j = first; j < m && !r; j++) r = L.step(j);
         const cudaError_t e = cudaStreamEndCapture(L.s, &gr);
         cudaGraphExec_t ex = nullptr;
-        if (!r && e == cudaSuccess && gr && cudaGraphInstantiate(&ex, gr, 0) == cudaSuccess) {
+        if (!r && e == cudaSuccess && gr) {
+          const int64_t key = ((int64_t)first << 20) | ((int64_t)(L.V == v_first ? 0 : 1) << 16) |
+                              (int64_t)m;
+          auto it = c->cycle_graphs.find(key);
+          if (it != c->cycle_graphs.end()) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(it->second, gr, &info) == cudaSuccess) {
+              ex = it->second;
+            } else {
+              cudaGetLastError();
+              cudaGraphExecDestroy(it->second);
+              c->cycle_graphs.erase(it);
+            }
+          }
+          if (!ex && cudaGraphInstantiate(&ex, gr, 0) == cudaSuccess) c->cycle_graphs[key] = ex;
+          else if (!ex) ex = nullptr;
+        }
+        if (ex) {
           cudaGraphDestroy(gr);
           graphs.push_back({first, L.V, ex});
           EIG_TRY(cudaGraphLaunch(ex, L.s));
@@ -839,7 +959,7 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
     std::vector<double> A((size_t)mm * mm);
     for (int a = 0; a < mm; a++)
       for (int b = 0; b < mm; b++) A[(size_t)a * mm + b] = Th[(size_t)a * td + b];
-    jacobi_eig(A, mm, th, Z);
+    if (!tridiag_qr_eig(A, mm, th, Z)) jacobi_eig(A, mm, th, Z);
     const double beta_m = mm < m ? 0.0 : Th[(size_t)(m - 1) * td + m];
     const int kev = std::min(nev_cur, mm);
     nconv = 0;
