@@ -133,6 +133,8 @@ struct dmrgx_ctx {
   // descriptors (uploads included), [2] split-precision images and
   // descriptors, [3] autotuning
   double t_plan_part[4] = {0, 0, 0, 0};
+  // solve group of this context's site steps (dmrgx_set_group), or null
+  struct dmrgx_group* group = nullptr;
   // instantiated Lanczos cycle graphs kept between solves (eig.cu)
   std::map<int64_t, cudaGraphExec_t> cycle_graphs;
   // results of the last dmrgx_svd: U and V (metadata, values) and the spectrum

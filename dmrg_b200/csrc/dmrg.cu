@@ -29,6 +29,8 @@ namespace dmrgx {
 int plan_build_device(dmrgx_ctx* c, const QTensor& L, const QTensor& R, int l_num, int r_num,
                       int sector, const Group& G, const QTensor* Le = nullptr,
                       const QTensor* Re = nullptr);
+int group_solve(dmrgx_ctx* c, int nev, int ncv, double tol, const double* v0, double* evals,
+                double* evec, int64_t* info);
 int eigsolve_device(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const double* v0,
                     double* evals, double* evec, int64_t* info);
 
@@ -336,7 +338,18 @@ struct Run {
       }
       guess.reset();
     }
-    int rc = eigsolve_device(c, eig_nev, eig_ncv, 1e-10, 0, v0, ev.data(), psi->d, info);
+    int rc;
+    if (c->group) {
+      // one lock-step solve with the group's other contexts (FP64 grouped matvec)
+      if (c->prec != DMRGX_PREC_FP64 || c->per_block) {
+        err = "a solve group needs FP64 contexts on the grouped schedule";
+        if (v0) dfree(v0, E.stream);
+        return DMRGX_E_STATE;
+      }
+      rc = group_solve(c, eig_nev, eig_ncv, 1e-10, v0, ev.data(), psi->d, info);
+    } else {
+      rc = eigsolve_device(c, eig_nev, eig_ncv, 1e-10, 0, v0, ev.data(), psi->d, info);
+    }
     if (v0) dfree(v0, E.stream);
     if (rc) {
       err = std::string("eigsolve: ") + dmrgx_last_error();

@@ -23,6 +23,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <mutex>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -33,6 +36,7 @@
 #include "../../include/dmrgx.h"
 #include "ctx.h"
 #include "devmem.h"
+#include "kernels.h"
 
 namespace dmrgx {
 
@@ -696,6 +700,10 @@ struct Lanczos {
   // (classical Gram-Schmidt against the whole basis, twice)
   int step(int j) {
     if (matvec(col(V, j), w, force64)) return DMRGX_E_CUDA;
+    return ortho(j);
+  }
+  // the rest of step j once w = H v_j: CGS2 against v_0..v_j, T entries, v_{j+1}
+  int ortho(int j) {
     const int k = j + 1;
     const int tr = lz_tile_rows(k, cplx);
     const size_t sm = lz_tile_smem(k, cplx, tr);
@@ -719,6 +727,119 @@ struct Lanczos {
     }
     vscale<<<grid, RB, 0, s>>>(w, inv, 0.0, col(V, j + 1), len);
     EIG_TRY(cudaGetLastError());
+    return 0;
+  }
+};
+
+// One FP64 matvec of several contexts in two launches (config 5's chains in one
+// batched launch per stage): the members' stage-1 descriptors, then their
+// stage-2 descriptors, merged into one grouped launch each, every offset rebased
+// from the member's own buffers to one common base address.  A member reads its
+// input from its din buffer and writes its output to its dout buffer; run()
+// copies the Krylov vectors in and out around the launches.
+struct GroupMatvec {
+  cudaStream_t s = nullptr;
+  std::vector<dmrgx_ctx*> cs;
+  double* base = nullptr;
+  DOut* d_outs[2] = {nullptr, nullptr};
+  DSeg* d_segs[2] = {nullptr, nullptr};
+  DTile* d_tiles[2] = {nullptr, nullptr};
+  int ntiles[2] = {0, 0};
+  bool cplx = false;
+  ~GroupMatvec() { release(); }
+  void release() {
+    for (int q = 0; q < 2; q++) {
+      dfree(d_outs[q], s);
+      dfree(d_segs[q], s);
+      dfree(d_tiles[q], s);
+      d_outs[q] = nullptr;
+      d_segs[q] = nullptr;
+      d_tiles[q] = nullptr;
+      ntiles[q] = 0;
+    }
+  }
+  int build(const std::vector<dmrgx_ctx*>& members) {
+    release();
+    cs = members;
+    if (cs.empty()) return 0;
+    cplx = cs[0]->dtype == DMRGX_C128;
+    uintptr_t lo = UINTPTR_MAX;
+    for (dmrgx_ctx* c : cs)
+      for (void* p : {c->renv.p, c->lenv.p, c->store.p, c->din.p, c->dout.p})
+        if (p) lo = std::min<uintptr_t>(lo, reinterpret_cast<uintptr_t>(p));
+    base = reinterpret_cast<double*>(lo);
+    auto off = [lo](const void* p) {
+      return (int64_t)((reinterpret_cast<uintptr_t>(p) - lo) / sizeof(double));
+    };
+    const int BK = f64_tile_k();
+    for (int q = 0; q < 2; q++) {
+      std::vector<DOut> outs;
+      std::vector<DSeg> segs;
+      std::vector<std::pair<int64_t, DTile>> tl;
+      for (dmrgx_ctx* c : cs) {
+        const Stage& st = q == 0 ? c->st1 : c->st2;
+        const int64_t a = off(q == 0 ? c->renv.p : c->lenv.p);
+        const int64_t b = off(q == 0 ? c->din.p : c->store.p);
+        const int64_t cc = off(q == 0 ? c->store.p : c->dout.p);
+        const int o0 = (int)outs.size(), s0 = (int)segs.size();
+        for (DOut o : st.outs) {
+          o.c_off += cc;
+          o.seg_begin += s0;
+          outs.push_back(o);
+        }
+        for (DSeg g : st.segs) {
+          g.a_off += a;
+          g.b_off += b;
+          segs.push_back(g);
+        }
+        for (DTile t : st.tiles) {
+          const DOut& o = st.outs[t.out];
+          int64_t kt = 0;
+          for (int x = 0; x < o.seg_count; x++) kt += (st.segs[o.seg_begin + x].k + BK - 1) / BK;
+          t.out += o0;
+          tl.push_back({kt, t});
+        }
+      }
+      std::stable_sort(tl.begin(), tl.end(), [](const std::pair<int64_t, DTile>& x,
+                                                const std::pair<int64_t, DTile>& y) {
+        return x.first > y.first;
+      });
+      std::vector<DTile> tiles;
+      for (auto& x : tl) tiles.push_back(x.second);
+      ntiles[q] = (int)tiles.size();
+      EIG_TRY(dalloc(&d_outs[q], std::max<size_t>(1, outs.size()), s));
+      EIG_TRY(dalloc(&d_segs[q], std::max<size_t>(1, segs.size()), s));
+      EIG_TRY(dalloc(&d_tiles[q], std::max<size_t>(1, tiles.size()), s));
+      if (!outs.empty())
+        EIG_TRY(cudaMemcpyAsync(d_outs[q], outs.data(), sizeof(DOut) * outs.size(),
+                                cudaMemcpyHostToDevice, s));
+      if (!segs.empty())
+        EIG_TRY(cudaMemcpyAsync(d_segs[q], segs.data(), sizeof(DSeg) * segs.size(),
+                                cudaMemcpyHostToDevice, s));
+      if (!tiles.empty())
+        EIG_TRY(cudaMemcpyAsync(d_tiles[q], tiles.data(), sizeof(DTile) * tiles.size(),
+                                cudaMemcpyHostToDevice, s));
+    }
+    EIG_TRY(cudaStreamSynchronize(s));  // the host vectors go away
+    return 0;
+  }
+  // out_b = H_b in_b for every member b (device vectors of n_b elements)
+  int run(const std::vector<const double*>& in, const std::vector<double*>& out, int grid) {
+    for (size_t b = 0; b < cs.size(); b++) {
+      dmrgx_ctx* c = cs[b];
+      const size_t bytes = sizeof(double) * (size_t)c->n * c->f();
+      EIG_TRY(cudaMemcpyAsync(c->din.p, in[b], bytes, cudaMemcpyDeviceToDevice, s));
+      if (!c->st1.full_cover)
+        EIG_TRY(cudaMemsetAsync(c->store.p, 0, sizeof(double) * c->d_store * c->f(), s));
+      if (!c->st2.full_cover) EIG_TRY(cudaMemsetAsync(c->dout.p, 0, bytes, s));
+    }
+    EIG_TRY(launch_grouped_f64(base, base, base, d_tiles[0], ntiles[0], d_outs[0], d_segs[0],
+                               cplx, grid, s));
+    EIG_TRY(launch_grouped_f64(base, base, base, d_tiles[1], ntiles[1], d_outs[1], d_segs[1],
+                               cplx, grid, s));
+    for (size_t b = 0; b < cs.size(); b++)
+      EIG_TRY(cudaMemcpyAsync(out[b], cs[b]->dout.p, sizeof(double) * (size_t)cs[b]->n * cs[b]->f(),
+                              cudaMemcpyDeviceToDevice, s));
     return 0;
   }
 };
@@ -1059,6 +1180,282 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
 
 }  // namespace
 
+// One member's solve in a lock-step group (device start / result vectors).
+struct GroupArgs {
+  dmrgx_ctx* c;
+  int nev, ncv;
+  double tol;
+  const double* v0;  // device start vector or null
+  double* evals;     // host, nev values
+  double* evec;      // device, n elements
+  int64_t* info;     // host, 6 slots, or null
+  int rc;
+};
+
+// Thick-restart Lanczos (the FP64 form of eigsolve_impl) for several contexts
+// at once, in lock step: every round applies H to one Krylov vector of each
+// member with a single merged launch per stage (GroupMatvec), then each member
+// reorthogonalises; after a cycle the host handles each member's projected
+// matrix as eigsolve_impl does.  A member that has converged leaves the
+// launches.  All work runs on stream s.
+int eigsolve_group(std::vector<GroupArgs>& args, cudaStream_t s, int64_t* stats) {
+  const char* err_attr = "";
+  if (!lz_tile_attrs(err_attr)) {
+    set_error(std::string("eigsolve: ") + err_attr);
+    return DMRGX_E_CUDA;
+  }
+  struct M {
+    GroupArgs* a;
+    Lanczos L;
+    int m = 0, td = 0, nev = 0, maxiter = 0, kkeep = 0, cycles = 0, nconv = 0;
+    double tol = 1e-10, resid = 0.0;
+    std::vector<double> Th, th, Z, ritz;
+    bool done = false, have_vec = false;
+  };
+  std::vector<M> ms(args.size());
+  for (size_t b = 0; b < args.size(); b++) {
+    M& x = ms[b];
+    GroupArgs& a = args[b];
+    dmrgx_ctx* c = a.c;
+    x.a = &a;
+    const int64_t n = c->n;
+    const bool cplx = c->dtype == DMRGX_C128;
+    int nev = a.nev, ncv = a.ncv;
+    if (ncv <= 0) ncv = cplx ? 6 * nev : 4 * nev;
+    ncv = std::min(ncv, MAX_NCV);
+    if (ncv >= n) {
+      ncv = (int)n;
+      nev = (int)std::min<int64_t>(nev, n);
+    } else if (nev >= ncv) {
+      nev = std::max(1, ncv - 1);
+    }
+    x.nev = nev;
+    x.tol = a.tol > 0 ? a.tol : 1e-10;
+    x.maxiter = (int)std::min<int64_t>(3 * n, 1000000);
+    Lanczos& L = x.L;
+    L.c = c;
+    L.cplx = cplx;
+    L.n = n;
+    L.len = n * (cplx ? 2 : 1);
+    L.m = ncv;
+    L.tdim = ncv + 1;
+    L.s = s;
+    L.grid = (int)std::max<int64_t>(1, std::min<int64_t>(c->num_sms * 8, (n + RB - 1) / RB));
+    L.nblk = (int)std::max<int64_t>(1, std::min<int64_t>(c->num_sms * 4, (n + RB - 1) / RB));
+    L.nblk2 = c->num_sms * 8;
+    int rc = L.init();
+    if (rc) return rc;
+    x.m = L.m;
+    x.td = L.tdim;
+    if (a.v0) EIG_TRY(cudaMemcpyAsync(L.V, a.v0, sizeof(double) * L.len, cudaMemcpyDeviceToDevice, s));
+    else if ((rc = eigsolve_start_pattern(L))) return rc;
+    double nn;
+    if ((rc = L.norm2(L.V, nn))) return rc;
+    if (!(nn > 0) && a.v0) {
+      if ((rc = eigsolve_start_pattern(L))) return rc;
+      if ((rc = L.norm2(L.V, nn))) return rc;
+    }
+    if (!(nn > 0)) {
+      set_error("eigsolve: zero start vector");
+      return DMRGX_E_ARG;
+    }
+    vscale<<<L.grid, RB, 0, s>>>(L.V, nullptr, 1.0 / std::sqrt(nn), L.V, L.len);
+    x.Th.assign((size_t)x.td * x.td, 0.0);
+    EIG_TRY(cudaMemsetAsync(L.T, 0, sizeof(double) * x.td * x.td, s));
+  }
+  GroupMatvec gm;
+  gm.s = s;
+  const int grid = args.empty() ? 1 : args[0].c->num_sms * 3;
+  for (;;) {
+    std::vector<int> act;
+    for (size_t b = 0; b < ms.size(); b++)
+      if (!ms[b].done) act.push_back((int)b);
+    if (act.empty()) break;
+    // one cycle: rounds t = 0, 1, ...; member b takes its step kkeep_b + t
+    int rounds = 0;
+    for (int b : act) rounds = std::max(rounds, ms[b].m - ms[b].kkeep);
+    for (int t = 0; t < rounds; t++) {
+      std::vector<dmrgx_ctx*> part;
+      std::vector<const double*> in;
+      std::vector<double*> out;
+      std::vector<int> who;
+      for (int b : act)
+        if (ms[b].kkeep + t < ms[b].m) {
+          part.push_back(ms[b].L.c);
+          in.push_back(ms[b].L.col(ms[b].L.V, ms[b].kkeep + t));
+          out.push_back(ms[b].L.w);
+          who.push_back(b);
+        }
+      if (part != gm.cs) {
+        const int rc = gm.build(part);
+        if (rc) return rc;
+      }
+      int rc = gm.run(in, out, grid);
+      if (rc) return rc;
+      if (stats) {
+        stats[0] += 1;                     // Krylov rounds
+        stats[1] += 2;                     // grouped launches (one per stage)
+        stats[2] += (int64_t)part.size();  // member matvecs served
+      }
+      for (int b : who) {
+        ms[b].L.matvecs++;
+        if ((rc = ms[b].L.ortho(ms[b].kkeep + t))) return rc;
+      }
+    }
+    for (int b : act)
+      EIG_TRY(cudaMemcpyAsync(ms[b].Th.data(), ms[b].L.T, sizeof(double) * ms[b].td * ms[b].td,
+                              cudaMemcpyDeviceToHost, s));
+    EIG_TRY(cudaStreamSynchronize(s));
+    for (int b : act) {
+      M& x = ms[b];
+      Lanczos& L = x.L;
+      const int m = x.m, td = x.td;
+      std::vector<double>& Th = x.Th;
+      int mm = m;
+      x.cycles++;
+      for (int j = x.kkeep; j < m; j++) {
+        const double av = std::fabs(Th[(size_t)j * td + j]);
+        if (Th[(size_t)j * td + j + 1] <= 1e-14 * std::max(1.0, av)) {
+          mm = j + 1;
+          break;
+        }
+      }
+      std::vector<double> A((size_t)mm * mm);
+      for (int r = 0; r < mm; r++)
+        for (int q = 0; q < mm; q++) A[(size_t)r * mm + q] = Th[(size_t)r * td + q];
+      if (!tridiag_qr_eig(A, mm, x.th, x.Z)) jacobi_eig(A, mm, x.th, x.Z);
+      const std::vector<double>& th = x.th;
+      const std::vector<double>& Z = x.Z;
+      const double beta_m = mm < m ? 0.0 : Th[(size_t)(m - 1) * td + m];
+      const int kev = std::min(x.nev, mm);
+      x.nconv = 0;
+      for (int q = 0; q < kev; q++) {
+        const double r = std::fabs(beta_m * Z[(size_t)(mm - 1) * mm + q]);
+        if (r <= x.tol * std::max(std::fabs(th[q]), 1e-30)) x.nconv++;
+        else break;
+      }
+      if (x.nconv >= kev || x.cycles >= x.maxiter || mm < m) {
+        x.ritz.assign(th.begin(), th.begin() + kev);
+        std::vector<double> Yh(mm);
+        for (int q = 0; q < mm; q++) Yh[q] = Z[(size_t)q * mm + 0];
+        EIG_TRY(cudaMemcpyAsync(L.Y, Yh.data(), sizeof(double) * mm, cudaMemcpyHostToDevice, s));
+        EIG_TRY(cudaStreamSynchronize(s));  // Yh is a host temporary
+        L.rotate(L.V, mm, 1, L.V2);
+        x.have_vec = true;
+        x.resid = std::fabs(beta_m * Z[(size_t)(mm - 1) * mm + 0]);
+        x.done = true;
+        continue;
+      }
+      // thick restart: the k lowest Ritz vectors, then the residual direction
+      const int k = std::min(m - 2, std::max(x.nev + 1, x.nev + (m - x.nev) / 2));
+      std::vector<double> Yh((size_t)m * k);
+      for (int q = 0; q < k; q++)
+        for (int r = 0; r < m; r++) Yh[(size_t)q * m + r] = Z[(size_t)r * m + q];
+      EIG_TRY(cudaMemcpyAsync(L.Y, Yh.data(), sizeof(double) * Yh.size(), cudaMemcpyHostToDevice, s));
+      L.rotate(L.V, m, k, L.V2);
+      EIG_TRY(cudaMemcpyAsync(L.col(L.V2, k), L.col(L.V, m), sizeof(double) * L.len,
+                              cudaMemcpyDeviceToDevice, s));
+      std::swap(L.V, L.V2);
+      std::fill(Th.begin(), Th.end(), 0.0);
+      for (int q = 0; q < k; q++) {
+        Th[(size_t)q * td + q] = th[q];
+        const double cpl = beta_m * Z[(size_t)(m - 1) * m + q];
+        Th[(size_t)q * td + k] = cpl;
+        Th[(size_t)k * td + q] = cpl;
+      }
+      EIG_TRY(cudaMemcpyAsync(L.T, Th.data(), sizeof(double) * td * td, cudaMemcpyHostToDevice, s));
+      EIG_TRY(cudaStreamSynchronize(s));  // Yh and Th are host arrays reused below
+      x.kkeep = k;
+    }
+  }
+  for (M& x : ms) {
+    Lanczos& L = x.L;
+    GroupArgs& a = *x.a;
+    for (int q = 0; q < a.nev; q++) a.evals[q] = q < (int)x.ritz.size() ? x.ritz[q] : 0.0;
+    double nn;
+    int rc = L.norm2(L.V2, nn);
+    if (rc) return rc;
+    vscale<<<L.grid, RB, 0, s>>>(L.V2, nullptr, 1.0 / std::sqrt(std::max(nn, 1e-300)), L.V2, L.len);
+    EIG_TRY(cudaMemcpyAsync(a.evec, L.V2, sizeof(double) * L.len, cudaMemcpyDeviceToDevice, s));
+    if (a.info) {
+      a.info[0] = L.matvecs;
+      a.info[1] = L.matvecs;
+      a.info[2] = x.cycles;
+      a.info[3] = 0;
+      a.info[4] = x.nconv;
+      std::memcpy(&a.info[5], &x.resid, sizeof(double));
+    }
+    a.rc = (x.nconv < 1 && x.cycles >= x.maxiter) ? DMRGX_E_NOCONV : 0;
+  }
+  EIG_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+}  // namespace dmrgx
+
+// A set of contexts whose site-step solves meet and run as one lock-step solve
+// (dmrgx_set_group).  The members arrive from their own host threads; the last
+// to arrive runs eigsolve_group for all of them on its stream while the others
+// wait; a member that waits longer than kWaitSeconds gives up with
+// DMRGX_E_TIMEOUT (a chain that failed before arriving).
+struct dmrgx_group {
+  int size = 0;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<dmrgx::GroupArgs> pending, results;
+  int64_t generation = 0;
+  int64_t stats[3] = {0, 0, 0};  // Krylov rounds, grouped launches, member matvecs
+  int last_rc = 0;
+  std::string last_err;
+};
+
+namespace dmrgx {
+
+constexpr int kWaitSeconds = 300;
+
+int group_solve(dmrgx_ctx* c, int nev, int ncv, double tol, const double* v0, double* evals,
+                double* evec, int64_t* info) {
+  dmrgx_group* g = c->group;
+  // this member's device data (plan, start vector, result buffer) is complete
+  // before another stream touches it
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    set_error(std::string("eigsolve: ") + cudaGetErrorString(e));
+    return DMRGX_E_CUDA;
+  }
+  std::unique_lock<std::mutex> lk(g->mu);
+  const int64_t gen = g->generation;
+  const size_t me = g->pending.size();
+  g->pending.push_back(GroupArgs{c, nev, ncv, tol, v0, evals, evec, info, 0});
+  if ((int)g->pending.size() == g->size) {
+    std::vector<GroupArgs> work;
+    work.swap(g->pending);
+    lk.unlock();
+    if (cudaSetDevice(c->device) != cudaSuccess) return DMRGX_E_CUDA;
+    const int rc = eigsolve_group(work, c->stream, g->stats);
+    const std::string msg = rc ? std::string(dmrgx_last_error()) : std::string();
+    lk.lock();
+    g->results = work;
+    g->last_rc = rc;
+    g->last_err = msg;
+    g->generation++;
+    g->cv.notify_all();
+    if (rc) return rc;
+    return work[me].rc;
+  }
+  if (!g->cv.wait_for(lk, std::chrono::seconds(kWaitSeconds),
+                      [&] { return g->generation != gen; })) {
+    set_error("eigsolve: the solve group did not assemble (a member failed or never arrived)");
+    return DMRGX_E_TIMEOUT;
+  }
+  if (g->last_rc) {
+    set_error(g->last_err);
+    return g->last_rc;
+  }
+  if (g->results[me].rc) set_error("eigsolve: maximum number of restarts reached");
+  return g->results[me].rc;
+}
+
 // the eigensolver with device start and result vectors (the site steps)
 int eigsolve_device(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const double* v0,
                     double* evals, double* evec, int64_t* info) {
@@ -1090,4 +1487,35 @@ extern "C" int dmrgx_eigsolve(dmrgx_ctx* c, int nev, int ncv, double tol, int ma
     return DMRGX_E_CUDA;
   }
   return dmrgx::eigsolve_impl(c, nev, ncv, tol, maxiter, v0, evals, evec, info, false);
+}
+
+extern "C" int dmrgx_group_create(dmrgx_group** g, int members) {
+  if (!g || members < 1) {
+    dmrgx::set_error("group_create: need an output pointer and members >= 1");
+    return DMRGX_E_ARG;
+  }
+  *g = new dmrgx_group();
+  (*g)->size = members;
+  return 0;
+}
+
+extern "C" void dmrgx_group_destroy(dmrgx_group* g) { delete g; }
+
+extern "C" int dmrgx_group_stats(dmrgx_group* g, int64_t* out) {
+  if (!g || !out) {
+    dmrgx::set_error("group_stats: null argument");
+    return DMRGX_E_ARG;
+  }
+  std::lock_guard<std::mutex> lk(g->mu);
+  for (int q = 0; q < 3; q++) out[q] = g->stats[q];
+  return 0;
+}
+
+extern "C" int dmrgx_set_group(dmrgx_ctx* c, dmrgx_group* g) {
+  if (!c) {
+    dmrgx::set_error("set_group: null context");
+    return DMRGX_E_ARG;
+  }
+  c->group = g;
+  return 0;
 }

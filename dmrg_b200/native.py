@@ -63,6 +63,10 @@ SIGNATURES = {
     "dmrgx_singular": (_i, [_vp, _dp, _dp, _ip, _i64, _i64p]),
     "dmrgx_step_split": (_i, [_vp, _dp, _i64, _i64p]),
     "dmrgx_svd": (_i, [_vp, _ip, _vp, _i, _i, _i, _i, _i64p]),
+    "dmrgx_group_create": (_i, [C.POINTER(_vp), _i]),
+    "dmrgx_group_destroy": (None, [_vp]),
+    "dmrgx_set_group": (_i, [_vp, _vp]),
+    "dmrgx_group_stats": (_i, [_vp, _i64p]),
     "dmrgx_svd_result": (_i, [_vp, _ip, _vp, _ip, _vp, _dp]),
     "dmrgx_run_seconds": (_i, [_vp, _dp, _i]),
     "dmrgx_adjoint": (_i, [_vp, _i, _dp, _i, _dp, _i64, _i64p, _dp, _dp]),
@@ -153,6 +157,34 @@ def av_noalloc(dtype, n, d_store, rmap, renv_dev, renv_sizes, lmap, lenv_dev, le
                                   C.c_void_p(renv_dev), _i64p(rs), rs.size, _ip(lmap),
                                   lmap.shape[0], C.c_void_p(lenv_dev), _i64p(ls), ls.size,
                                   C.c_void_p(in_dev), C.c_void_p(out_dev), C.c_void_p(stream)))
+
+
+class Group:
+    """A solve group (dmrgx_group_create): contexts that join it and run dmrg()
+    from their own threads meet at every site step's eigensolve, which runs as
+    one lock-step Lanczos with one grouped matvec launch per stage for all."""
+
+    def __init__(self, members):
+        p = C.c_void_p()
+        _check(lib().dmrgx_group_create(C.byref(p), int(members)))
+        self.ptr = p
+
+    def stats(self):
+        """(Krylov rounds, grouped launches, member matvecs served)."""
+        out = np.zeros(3, np.int64)
+        _check(lib().dmrgx_group_stats(self.ptr, _i64p(out)))
+        return tuple(int(v) for v in out)
+
+    def close(self):
+        if self.ptr:
+            lib().dmrgx_group_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Context:
@@ -264,6 +296,10 @@ class Context:
         """Site-step eigensolver of the next dmrg(): eigenvalues per step, Krylov basis
         (0: the reference's), White's wavefunction prediction."""
         _check(lib().dmrgx_set_solver(self.ptr, nev, ncv, int(bool(predict))))
+
+    def set_group(self, group):
+        """Join a solve group (None: leave it)."""
+        _check(lib().dmrgx_set_group(self.ptr, group.ptr if group is not None else None))
 
     def set_boundary(self, boundary):
         """BOUNDARY_OPEN (default) or BOUNDARY_PERIODIC for the next dmrg()."""

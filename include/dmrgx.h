@@ -322,6 +322,27 @@ int dmrgx_svd_result(dmrgx_ctx* ctx, int* u_meta, void* u_vals, int* v_meta, voi
 int dmrgx_singular(dmrgx_ctx* ctx, double* entropy, double* s20, int* nsv, int64_t cap,
                    int64_t* nsteps);
 
+/* Solve groups: one batched launch for several chains.  New work (BASELINE
+ * config 5): the reference solves chains one after another, each site step's
+ * matvec as one serial BLAS call per task row (src/core.cpp:22-31).
+ *
+ * Contexts that join one group (dmrgx_set_group) and run dmrgx_dmrg from their
+ * own host threads meet at every site step's eigensolve: the last to arrive
+ * runs one lock-step Lanczos over all members, in which each Krylov round
+ * applies every member's H_eff in one grouped FP64 launch per stage (the task
+ * lists of all members merged).  The members must run the same schedule (same
+ * L, m, sweeps and solver settings, so that their site steps pair up), in FP64
+ * on the grouped schedule.  A member that waits 5 minutes for the others gives
+ * up with DMRGX_E_TIMEOUT.  members: the number of contexts that will join.
+ * dmrgx_set_group(ctx, NULL) leaves the group. */
+typedef struct dmrgx_group dmrgx_group;
+int dmrgx_group_create(dmrgx_group** group, int members);
+void dmrgx_group_destroy(dmrgx_group* group);
+int dmrgx_set_group(dmrgx_ctx* ctx, dmrgx_group* group);
+/* Work of the group so far: out[0] Krylov rounds, out[1] grouped matvec
+ * launches (one per stage per round), out[2] member matvecs they served. */
+int dmrgx_group_stats(dmrgx_group* group, int64_t* out);
+
 /* Wall seconds of every site step of the last dmrgx_dmrg (eigensolver, SVD,
  * environment update and fusion of the step), in schedule order; nsteps gets the
  * count, out (cap values, may be NULL) the times. */
