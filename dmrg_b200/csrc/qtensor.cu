@@ -337,6 +337,31 @@ __global__ void __launch_bounds__(256) jacobi_svd(const double* __restrict__ M,
   const int P = p + (p & 1);  // players of the tournament (one bye when p is odd)
   for (int t = tid; t < P; t += blockDim.x) order[t] = t;
   const double tol = 4e-16 * sqrt((double)q);
+  // |Z|_F^2: a column whose norm is below 1e-15 |Z|_F is rounding noise (a
+  // rank-deficient sector); rotating it against a large column only turns the
+  // noise, so such pairs are skipped and the column's norm, the singular value,
+  // stays at that level
+  __shared__ double fro_w[32];
+  __shared__ double fro2;
+  __syncthreads();  // the stacked matrix is complete
+  {
+    double a = 0.0;
+    for (int t = tid; t < p * q; t += blockDim.x) {
+      const int j = t / q, r = t - j * q;
+      const double re = jsm[((size_t)j * h + r) * F], im = CPLX ? jsm[((size_t)j * h + r) * F + 1] : 0.0;
+      a += re * re + im * im;
+    }
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) fro_w[wp] = a;
+    __syncthreads();
+    if (tid == 0) {
+      double t2 = 0.0;
+      for (int w = 0; w < nw; w++) t2 += fro_w[w];
+      fro2 = t2;
+    }
+    __syncthreads();
+  }
+  const double tiny = 1e-30 * fro2;
   int sweep = 0;
   for (; sweep < kJacSweeps; sweep++) {
     if (tid == 0) rotated = 0;
@@ -364,7 +389,7 @@ __global__ void __launch_bounds__(256) jacobi_svd(const double* __restrict__ M,
           gi += __shfl_xor_sync(0xffffffffu, gi, o);
         }
         const double g = sqrt(gr * gr + gi * gi);
-        if (!(g > tol * sqrt(al * be)) || al == 0.0 || be == 0.0) continue;
+        if (al <= tiny || be <= tiny || !(g > tol * sqrt(al) * sqrt(be))) continue;
         // rotation zeroing the pair's off-diagonal: with b~ = conj(e) b (e = gamma/|gamma|)
         //   a' = c a - s b~,  b~' = s a + c b~,  b' = e b~'
         const double er = gr / g, ei = gi / g;

@@ -67,3 +67,17 @@ def test_solve_group_one_launch_per_stage_matches_serial_runs():
     for c in ctxs:
         c.close()
     g.close()
+
+
+def test_grouped_batch_matches_serial():
+    """The config-5 runner with solve groups (chains of one m in lock step):
+    energies and adjoint gradients equal the one-by-one runs."""
+    specs = [dict(chain=i, L=12, m=m, params=[1.0, 0.8, jz, 0.0])
+             for i, (m, jz) in enumerate([(16, 0.3), (16, 0.5), (24, 0.7), (24, 0.9)])]
+    par, wall = batch.run_batch(specs, grouped=True, sweeps=2, fd=False)
+    ser = [batch.run_chain(s, sweeps=2, fd=False) for s in specs]
+    for a, b in zip(par, ser):
+        assert abs(a["E0"] - b["E0"]) < 1e-12 * abs(b["E0"])
+        assert abs(a["dE_dJz"] - b["dE_dJz"]) < 1e-10 * abs(b["dE_dJz"])
+        st = a["group_stats"]
+        assert st["launches"] == 2 * st["rounds"] and st["member_matvecs"] > st["rounds"]
