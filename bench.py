@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--config1", type=int, default=1,
                    help="1: BASELINE config 1 (Kitaev L=32, m=64, 6 sweeps) on the GPU beside the "
                         "reference's own run on the host cores")
+    p.add_argument("--config5", type=int, default=1,
+                   help="1: BASELINE config 5 reduced (8 chains, m in {64, 128}) in solve groups")
     p.add_argument("--sweep", type=int, default=1,
                    help="also time the DMRG schedule (XYZ real chain) in three forms: plain "
                         "per-block FP64, grouped FP64, grouped headline precision")
@@ -362,6 +364,25 @@ def config1_compare(native):
     return out
 
 
+def config5_compare():
+    """BASELINE config 5 in solve groups, reduced to fit the benchmark's time: the
+    eight chains of bond dimensions 64 and 128 (XYZ L=64, Jz from seed 20261203),
+    one sweep, two solve groups of four whose matvecs are one grouped launch per
+    stage, then each chain's adjoint dE/dJz, dE/dh against Hellmann-Feynman.
+    The full sixteen-chain run is `python -m dmrg_b200.batch --grouped`."""
+    from dmrg_b200 import batch
+    specs = batch.config5_chains(L=64, ms=(64, 128), per_m=4)
+    res, wall = batch.run_batch(specs, grouped=True, sweeps=1, fd=False)
+    return {"workload": "config 5 reduced: 8 XYZ chains L=64, m in {64, 128} x 4, 1 sweep, "
+                        "FP64, two solve groups (one grouped matvec launch per stage)",
+            "wall_s": wall,
+            "max_rel_hf_dE_dJz": max(r["rel_hf_Jz"] for r in res),
+            "max_abs_hf_dE_dh": max(r["abs_hf_h"] for r in res),
+            "groups": {str(r["m"]): r["group_stats"] for r in res},
+            "chains": [{"m": r["m"], "jz": r["jz"], "E0": r["E0"], "dE_dJz": r["dE_dJz"],
+                        "hf_Jz": r["hf_Jz"]} for r in res]}
+
+
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
@@ -553,6 +574,7 @@ def main():
         cpu = cpu_reference_rate(args.cpu_sample_s, w)
         sweep = sweep_compare(native, args) if args.sweep else None
         cfg1 = config1_compare(native) if args.config1 else None
+        cfg5 = config5_compare() if args.config5 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
@@ -584,6 +606,8 @@ def main():
             line["sweep"] = sweep
         if cfg1 is not None:
             line["config1"] = cfg1
+        if cfg5 is not None:
+            line["config5"] = cfg5
         line["plain_fp64_path"] = plain_path
         line["vs_plain_fp64"] = value / plain_path["value"]
         if fp64 is not None:
