@@ -33,10 +33,14 @@ void set_error(const std::string& msg) { g_err = msg; }
 void Stage::free_device() {
   dfree(d_outs, st);
   dfree(d_segs, st);
-  dfree(d_tiles, st);
+  dfree(d_units, st);
+  dfree(d_ws, st);
+  dfree(d_tickets, st);
   d_outs = nullptr;
   d_segs = nullptr;
-  d_tiles = nullptr;
+  d_units = nullptr;
+  d_ws = nullptr;
+  d_tickets = nullptr;
 }
 
 cudaError_t DevBuf::ensure(size_t b) {
@@ -135,10 +139,10 @@ EnvImage make_image(const double* src, const std::vector<int64_t>& off,
 
 std::string build_stage(const std::vector<MapRow>& rows, const std::vector<int64_t>& blk_size,
                         const EnvImage& im, int f, int64_t in_len, int64_t out_len, Stage& st,
-                        int64_t& flops) {
+                        int64_t& flops, int grid) {
   st.outs.clear();
   st.segs.clear();
-  st.tiles.clear();
+  st.units.clear();
   st.rows.clear();
   std::map<int64_t, int> by_off;  // output offset -> out index
   std::vector<std::vector<DSeg>> per_out;
@@ -192,28 +196,11 @@ std::string build_stage(const std::vector<MapRow>& rows, const std::vector<int64
     covered += (int64_t)st.outs[o].m * st.outs[o].n / f;
   }
   st.full_cover = covered == out_len;
-  // tiles, heaviest first
-  const int BM = f64_tile_m(), BN = f64_tile_n(), BK = f64_tile_k();
-  std::vector<std::pair<int64_t, DTile>> tl;
-  for (size_t o = 0; o < st.outs.size(); o++) {
-    int64_t kt = 0;
-    for (int s = 0; s < st.outs[o].seg_count; s++) kt += (st.segs[st.outs[o].seg_begin + s].k + BK - 1) / BK;
-    const int tm = (st.outs[o].m + BM - 1) / BM, tn = (st.outs[o].n + BN - 1) / BN;
-    if (tm > 32767 || tn > 32767) return "output block too large for the tile grid";
-    for (int a = 0; a < tm; a++)
-      for (int b = 0; b < tn; b++) {
-        DTile t;
-        t.out = (int32_t)o;
-        t.tm = (int16_t)a;
-        t.tn = (int16_t)b;
-        tl.push_back({kt, t});
-      }
-  }
-  std::stable_sort(tl.begin(), tl.end(),
-                   [](const std::pair<int64_t, DTile>& x, const std::pair<int64_t, DTile>& y) {
-                     return x.first > y.first;
-                   });
-  for (auto& p : tl) st.tiles.push_back(p.second);
+  const int BM = f64_tile_m(), BN = f64_tile_n();
+  for (const DOut& o : st.outs)
+    if ((o.m + BM - 1) / BM > 32767 || (o.n + BN - 1) / BN > 32767)
+      return "output block too large for the tile grid";
+  st.nslots = make_f64_units(st.outs, st.segs, grid, f64_split_mode(), st.units);
   return "";
 }
 
@@ -222,15 +209,20 @@ int upload_stage(Stage& st, cudaStream_t s) {
   st.st = s;
   CUDA_TRY(dalloc(&st.d_outs, st.outs.size(), s));
   CUDA_TRY(dalloc(&st.d_segs, st.segs.size(), s));
-  CUDA_TRY(dalloc(&st.d_tiles, st.tiles.size(), s));
+  CUDA_TRY(dalloc(&st.d_units, st.units.size(), s));
+  if (st.nslots > 0) {
+    CUDA_TRY(dalloc(&st.d_ws, (size_t)st.nslots * f64_tile_m() * f64_tile_n(), s));
+    CUDA_TRY(dalloc(&st.d_tickets, (size_t)st.nslots, s));
+    CUDA_TRY(cudaMemsetAsync(st.d_tickets, 0, sizeof(int) * st.nslots, s));
+  }
   if (!st.outs.empty())
     CUDA_TRY(cudaMemcpyAsync(st.d_outs, st.outs.data(), sizeof(DOut) * st.outs.size(),
                              cudaMemcpyHostToDevice, s));
   if (!st.segs.empty())
     CUDA_TRY(cudaMemcpyAsync(st.d_segs, st.segs.data(), sizeof(DSeg) * st.segs.size(),
                              cudaMemcpyHostToDevice, s));
-  if (!st.tiles.empty())
-    CUDA_TRY(cudaMemcpyAsync(st.d_tiles, st.tiles.data(), sizeof(DTile) * st.tiles.size(),
+  if (!st.units.empty())
+    CUDA_TRY(cudaMemcpyAsync(st.d_units, st.units.data(), sizeof(DUnit) * st.units.size(),
                              cudaMemcpyHostToDevice, s));
   return 0;
 }
@@ -339,8 +331,9 @@ int finalize_plan(dmrgx_ctx* c, const std::vector<PairSrc>& pairs) {
   c->r_blocks_main = pairs.empty() ? 0 : (int)pairs[0].rsize.size();
   c->l_blocks_main = pairs.empty() ? 0 : (int)pairs[0].lsize.size();
   c->d_store = soff;
-  std::string e = build_stage(c->rmap, rsz, RI, f, c->n, c->d_store, c->st1, c->flops);
-  if (e.empty()) e = build_stage(c->lmap, lsz, LI, f, c->d_store, c->n, c->st2, c->flops);
+  const int grid = c->num_sms * 3;
+  std::string e = build_stage(c->rmap, rsz, RI, f, c->n, c->d_store, c->st1, c->flops, grid);
+  if (e.empty()) e = build_stage(c->lmap, lsz, LI, f, c->d_store, c->n, c->st2, c->flops, grid);
   if (!e.empty()) {
     set_error(e);
     return DMRGX_E_ARG;
@@ -420,15 +413,15 @@ int run_matvec_fp64(dmrgx_ctx* c, const double* in, double* out) {
   double* store = (double*)c->store.p;
   if (!c->st1.full_cover)
     CUDA_TRY(cudaMemsetAsync(store, 0, sizeof(double) * c->d_store * c->f(), c->stream));
-  CUDA_TRY(launch_grouped_f64((const double*)c->renv.p, in, store, c->st1.d_tiles,
-                              (int)c->st1.tiles.size(), c->st1.d_outs, c->st1.d_segs, cplx, grid,
-                              c->stream));
+  CUDA_TRY(launch_grouped_f64((const double*)c->renv.p, in, store, c->st1.d_units,
+                              (int)c->st1.units.size(), c->st1.d_outs, c->st1.d_segs, cplx, grid,
+                              c->stream, c->st1.d_ws, c->st1.d_tickets));
   c->prof_mark();
   if (!c->st2.full_cover)
     CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double) * c->n * c->f(), c->stream));
-  CUDA_TRY(launch_grouped_f64((const double*)c->lenv.p, store, out, c->st2.d_tiles,
-                              (int)c->st2.tiles.size(), c->st2.d_outs, c->st2.d_segs, cplx, grid,
-                              c->stream));
+  CUDA_TRY(launch_grouped_f64((const double*)c->lenv.p, store, out, c->st2.d_units,
+                              (int)c->st2.units.size(), c->st2.d_outs, c->st2.d_segs, cplx, grid,
+                              c->stream, c->st2.d_ws, c->st2.d_tickets));
   c->prof_mark();
   return 0;
 }
@@ -615,7 +608,7 @@ int dmrgx_matvec_launches(dmrgx_ctx* c, int* out) {
   else if (c->per_block)
     *out = (int)(c->st1.rows.size() + c->st2.rows.size());
   else
-    *out = (c->st1.tiles.empty() ? 0 : 1) + (c->st2.tiles.empty() ? 0 : 1);
+    *out = (c->st1.units.empty() ? 0 : 1) + (c->st2.units.empty() ? 0 : 1);
   return 0;
 }
 

@@ -28,10 +28,13 @@ struct Stage {
   std::vector<PlainRow> rows;  // the same work as one GEMM per task row
   std::vector<DOut> outs;
   std::vector<DSeg> segs;
-  std::vector<DTile> tiles;
+  std::vector<DUnit> units;   // CTA assignment of the FP64 grouped kernel
+  int64_t nslots = 0;          // K-split workspace slots the units use
   DOut* d_outs = nullptr;
   DSeg* d_segs = nullptr;
-  DTile* d_tiles = nullptr;
+  DUnit* d_units = nullptr;
+  double* d_ws = nullptr;      // nslots x 4096 doubles
+  int* d_tickets = nullptr;    // nslots, zero between launches
   bool full_cover = true;   // every element of the output is written by some tile
   int64_t a_len = 0;        // real length of operand-A image
   cudaStream_t st = nullptr; // stream of the device arrays

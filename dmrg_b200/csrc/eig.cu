@@ -743,24 +743,32 @@ struct GroupMatvec {
   double* base = nullptr;
   DOut* d_outs[2] = {nullptr, nullptr};
   DSeg* d_segs[2] = {nullptr, nullptr};
-  DTile* d_tiles[2] = {nullptr, nullptr};
-  int ntiles[2] = {0, 0};
+  DUnit* d_units[2] = {nullptr, nullptr};
+  double* d_ws[2] = {nullptr, nullptr};
+  int* d_tickets[2] = {nullptr, nullptr};
+  int nunits[2] = {0, 0};
+  int grid = 0;
   bool cplx = false;
   ~GroupMatvec() { release(); }
   void release() {
     for (int q = 0; q < 2; q++) {
       dfree(d_outs[q], s);
       dfree(d_segs[q], s);
-      dfree(d_tiles[q], s);
+      dfree(d_units[q], s);
+      dfree(d_ws[q], s);
+      dfree(d_tickets[q], s);
       d_outs[q] = nullptr;
       d_segs[q] = nullptr;
-      d_tiles[q] = nullptr;
-      ntiles[q] = 0;
+      d_units[q] = nullptr;
+      d_ws[q] = nullptr;
+      d_tickets[q] = nullptr;
+      nunits[q] = 0;
     }
   }
-  int build(const std::vector<dmrgx_ctx*>& members) {
+  int build(const std::vector<dmrgx_ctx*>& members, int grid_ctas) {
     release();
     cs = members;
+    grid = grid_ctas;
     if (cs.empty()) return 0;
     cplx = cs[0]->dtype == DMRGX_C128;
     uintptr_t lo = UINTPTR_MAX;
@@ -771,17 +779,15 @@ struct GroupMatvec {
     auto off = [lo](const void* p) {
       return (int64_t)((reinterpret_cast<uintptr_t>(p) - lo) / sizeof(double));
     };
-    const int BK = f64_tile_k();
     for (int q = 0; q < 2; q++) {
       std::vector<DOut> outs;
       std::vector<DSeg> segs;
-      std::vector<std::pair<int64_t, DTile>> tl;
       for (dmrgx_ctx* c : cs) {
         const Stage& st = q == 0 ? c->st1 : c->st2;
         const int64_t a = off(q == 0 ? c->renv.p : c->lenv.p);
         const int64_t b = off(q == 0 ? c->din.p : c->store.p);
         const int64_t cc = off(q == 0 ? c->store.p : c->dout.p);
-        const int o0 = (int)outs.size(), s0 = (int)segs.size();
+        const int s0 = (int)segs.size();
         for (DOut o : st.outs) {
           o.c_off += cc;
           o.seg_begin += s0;
@@ -792,39 +798,34 @@ struct GroupMatvec {
           g.b_off += b;
           segs.push_back(g);
         }
-        for (DTile t : st.tiles) {
-          const DOut& o = st.outs[t.out];
-          int64_t kt = 0;
-          for (int x = 0; x < o.seg_count; x++) kt += (st.segs[o.seg_begin + x].k + BK - 1) / BK;
-          t.out += o0;
-          tl.push_back({kt, t});
-        }
       }
-      std::stable_sort(tl.begin(), tl.end(), [](const std::pair<int64_t, DTile>& x,
-                                                const std::pair<int64_t, DTile>& y) {
-        return x.first > y.first;
-      });
-      std::vector<DTile> tiles;
-      for (auto& x : tl) tiles.push_back(x.second);
-      ntiles[q] = (int)tiles.size();
+      // one assignment over every member's tiles, K-split like a single context's stage
+      std::vector<DUnit> units;
+      const int64_t nslots = make_f64_units(outs, segs, grid, f64_split_mode(), units);
+      nunits[q] = (int)units.size();
       EIG_TRY(dalloc(&d_outs[q], std::max<size_t>(1, outs.size()), s));
       EIG_TRY(dalloc(&d_segs[q], std::max<size_t>(1, segs.size()), s));
-      EIG_TRY(dalloc(&d_tiles[q], std::max<size_t>(1, tiles.size()), s));
+      EIG_TRY(dalloc(&d_units[q], std::max<size_t>(1, units.size()), s));
+      if (nslots > 0) {
+        EIG_TRY(dalloc(&d_ws[q], (size_t)nslots * f64_tile_m() * f64_tile_n(), s));
+        EIG_TRY(dalloc(&d_tickets[q], (size_t)nslots, s));
+        EIG_TRY(cudaMemsetAsync(d_tickets[q], 0, sizeof(int) * nslots, s));
+      }
       if (!outs.empty())
         EIG_TRY(cudaMemcpyAsync(d_outs[q], outs.data(), sizeof(DOut) * outs.size(),
                                 cudaMemcpyHostToDevice, s));
       if (!segs.empty())
         EIG_TRY(cudaMemcpyAsync(d_segs[q], segs.data(), sizeof(DSeg) * segs.size(),
                                 cudaMemcpyHostToDevice, s));
-      if (!tiles.empty())
-        EIG_TRY(cudaMemcpyAsync(d_tiles[q], tiles.data(), sizeof(DTile) * tiles.size(),
+      if (!units.empty())
+        EIG_TRY(cudaMemcpyAsync(d_units[q], units.data(), sizeof(DUnit) * units.size(),
                                 cudaMemcpyHostToDevice, s));
     }
     EIG_TRY(cudaStreamSynchronize(s));  // the host vectors go away
     return 0;
   }
   // out_b = H_b in_b for every member b (device vectors of n_b elements)
-  int run(const std::vector<const double*>& in, const std::vector<double*>& out, int grid) {
+  int run(const std::vector<const double*>& in, const std::vector<double*>& out) {
     for (size_t b = 0; b < cs.size(); b++) {
       dmrgx_ctx* c = cs[b];
       const size_t bytes = sizeof(double) * (size_t)c->n * c->f();
@@ -833,10 +834,10 @@ struct GroupMatvec {
         EIG_TRY(cudaMemsetAsync(c->store.p, 0, sizeof(double) * c->d_store * c->f(), s));
       if (!c->st2.full_cover) EIG_TRY(cudaMemsetAsync(c->dout.p, 0, bytes, s));
     }
-    EIG_TRY(launch_grouped_f64(base, base, base, d_tiles[0], ntiles[0], d_outs[0], d_segs[0],
-                               cplx, grid, s));
-    EIG_TRY(launch_grouped_f64(base, base, base, d_tiles[1], ntiles[1], d_outs[1], d_segs[1],
-                               cplx, grid, s));
+    EIG_TRY(launch_grouped_f64(base, base, base, d_units[0], nunits[0], d_outs[0], d_segs[0],
+                               cplx, grid, s, d_ws[0], d_tickets[0]));
+    EIG_TRY(launch_grouped_f64(base, base, base, d_units[1], nunits[1], d_outs[1], d_segs[1],
+                               cplx, grid, s, d_ws[1], d_tickets[1]));
     for (size_t b = 0; b < cs.size(); b++)
       EIG_TRY(cudaMemcpyAsync(out[b], cs[b]->dout.p, sizeof(double) * (size_t)cs[b]->n * cs[b]->f(),
                               cudaMemcpyDeviceToDevice, s));
@@ -1287,10 +1288,10 @@ int eigsolve_group(std::vector<GroupArgs>& args, cudaStream_t s, int64_t* stats)
           who.push_back(b);
         }
       if (part != gm.cs) {
-        const int rc = gm.build(part);
+        const int rc = gm.build(part, grid);
         if (rc) return rc;
       }
-      int rc = gm.run(in, out, grid);
+      int rc = gm.run(in, out);
       if (rc) return rc;
       if (stats) {
         stats[0] += 1;                     // Krylov rounds

@@ -33,4 +33,18 @@ struct DTile {
   int16_t tm, tn;    // tile coordinates inside the output block
 };
 
+// One work unit of the FP64 grouped kernel: tile (tm, tn) of output block `out`
+// over the k-tiles [kt0, kt1) of the block's segments taken in order.  A tile cut
+// along K into `nparts` parts stores part `part`'s partial sum to workspace slot
+// `slot` (64 x 64 doubles); its parts own slots slot - part ... slot - part +
+// nparts - 1, and the ticket at index slot - part counts them.  out < 0 marks a
+// padding entry of the CTA assignment.
+struct DUnit {
+  int32_t out = -1;
+  int16_t tm = 0, tn = 0;
+  int32_t kt0 = 0, kt1 = 0;
+  int32_t slot = -1;           // -1: the whole K range, written directly
+  int16_t part = 0, nparts = 1;
+};
+
 }  // namespace dmrgx

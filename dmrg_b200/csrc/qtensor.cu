@@ -140,33 +140,25 @@ int64_t label_key(const std::vector<int>& st, const std::vector<std::vector<int>
 cudaError_t run_gemms(const Engine& E, const double* A, const double* B, double* C,
                       std::vector<DOut>& outs, std::vector<DSeg>& segs) {
   if (outs.empty()) return cudaSuccess;
-  const int BM = f64_tile_m(), BN = f64_tile_n();
-  std::vector<DTile> tiles;
-  for (size_t o = 0; o < outs.size(); o++)
-    for (int a = 0; a < (outs[o].m + BM - 1) / BM; a++)
-      for (int b = 0; b < (outs[o].n + BN - 1) / BN; b++) {
-        DTile t;
-        t.out = (int32_t)o;
-        t.tm = (int16_t)a;
-        t.tn = (int16_t)b;
-        tiles.push_back(t);
-      }
-  if (tiles.empty()) return cudaSuccess;
+  const int grid = E.num_sms * 3;
+  std::vector<DUnit> units;
+  make_f64_units(outs, segs, grid, 0, units);  // whole tiles: no workspace
+  if (units.empty()) return cudaSuccess;
   DOut* d_o = nullptr;
   DSeg* d_s = nullptr;
-  DTile* d_t = nullptr;
+  DUnit* d_t = nullptr;
   cudaError_t e = dalloc(&d_o, outs.size(), E.stream);
   if (e == cudaSuccess) e = dalloc(&d_s, segs.size(), E.stream);
-  if (e == cudaSuccess) e = dalloc(&d_t, tiles.size(), E.stream);
+  if (e == cudaSuccess) e = dalloc(&d_t, units.size(), E.stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(d_o, outs.data(), sizeof(DOut) * outs.size(), cudaMemcpyHostToDevice, E.stream);
   if (e == cudaSuccess && !segs.empty())
     e = cudaMemcpyAsync(d_s, segs.data(), sizeof(DSeg) * segs.size(), cudaMemcpyHostToDevice, E.stream);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(d_t, tiles.data(), sizeof(DTile) * tiles.size(), cudaMemcpyHostToDevice, E.stream);
+    e = cudaMemcpyAsync(d_t, units.data(), sizeof(DUnit) * units.size(), cudaMemcpyHostToDevice, E.stream);
   if (e == cudaSuccess)
-    e = launch_grouped_f64(A, B, C, d_t, (int)tiles.size(), d_o, d_s, E.f == 2, E.num_sms * 3,
-                           E.stream);
+    e = launch_grouped_f64(A, B, C, d_t, (int)units.size(), d_o, d_s, E.f == 2, grid, E.stream,
+                           nullptr, nullptr);
   dfree(d_o, E.stream);
   dfree(d_s, E.stream);
   dfree(d_t, E.stream);
