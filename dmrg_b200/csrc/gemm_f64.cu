@@ -290,11 +290,27 @@ struct Tile { int out, tm, tn, kt; };
 // whole tiles, longest first onto the least-loaded CTA; per-CTA lists and the
 // largest CTA load (k-tiles + fixed unit cost)
 double assign_whole(const std::vector<Tile>& tiles, int grid, std::vector<std::vector<DUnit>>& per) {
+  per.assign(grid, {});
+  auto unit = [](const Tile& x) {
+    DUnit u;
+    u.out = x.out;
+    u.tm = (int16_t)x.tm;
+    u.tn = (int16_t)x.tn;
+    u.kt0 = 0;
+    u.kt1 = x.kt;
+    return u;
+  };
+  bool equal = true;
+  for (const Tile& x : tiles) equal = equal && x.kt == tiles[0].kt;
+  if (equal) {  // all tiles alike: longest first is round robin
+    for (size_t i = 0; i < tiles.size(); i++) per[i % grid].push_back(unit(tiles[i]));
+    const size_t most = (tiles.size() + grid - 1) / grid;
+    return most * (tiles[0].kt + kUnitOverhead);
+  }
   std::vector<int> order(tiles.size());
   for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
   std::stable_sort(order.begin(), order.end(),
                    [&](int a, int b) { return tiles[a].kt > tiles[b].kt; });
-  per.assign(grid, {});
   std::vector<std::pair<double, int>> heap;  // (load, cta), min-heap
   for (int c = 0; c < grid; c++) heap.push_back({0.0, c});
   auto cmp = [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
@@ -306,13 +322,7 @@ double assign_whole(const std::vector<Tile>& tiles, int grid, std::vector<std::v
     const Tile& x = tiles[i];
     std::pop_heap(heap.begin(), heap.end(), cmp);
     auto& top = heap.back();
-    DUnit u;
-    u.out = x.out;
-    u.tm = (int16_t)x.tm;
-    u.tn = (int16_t)x.tn;
-    u.kt0 = 0;
-    u.kt1 = x.kt;
-    per[top.second].push_back(u);
+    per[top.second].push_back(unit(x));
     top.first += x.kt + kUnitOverhead;
     worst = std::max(worst, top.first);
     std::push_heap(heap.begin(), heap.end(), cmp);
@@ -380,16 +390,38 @@ double assign_shares(const std::vector<Tile>& tiles, int grid, std::vector<std::
 int64_t make_f64_units(const std::vector<DOut>& outs, const std::vector<DSeg>& segs, int grid,
                        int mode, std::vector<DUnit>& units) {
   units.clear();
-  std::vector<Tile> tiles;
+  std::vector<int> kts(outs.size());
+  size_t ntiles = 0;
   for (size_t o = 0; o < outs.size(); o++) {
     int64_t kt = 0;
     for (int s = 0; s < outs[o].seg_count; s++) kt += (segs[outs[o].seg_begin + s].k + BK - 1) / BK;
+    kts[o] = (int)std::min<int64_t>(kt, INT_MAX / 2);
+    ntiles += (size_t)((outs[o].m + BM - 1) / BM) * ((outs[o].n + BN - 1) / BN);
+  }
+  if (ntiles == 0) return 0;
+  if (mode < 0) {  // tile order as listed, one unit per tile: O(tiles) host work
+    units.resize(ntiles);
+    size_t i = 0;
+    for (size_t o = 0; o < outs.size(); o++) {
+      const int tm = (outs[o].m + BM - 1) / BM, tn = (outs[o].n + BN - 1) / BN;
+      for (int a = 0; a < tm; a++)
+        for (int b = 0; b < tn; b++) {
+          DUnit& u = units[i++];
+          u.out = (int32_t)o;
+          u.tm = (int16_t)a;
+          u.tn = (int16_t)b;
+          u.kt1 = kts[o];
+        }
+    }
+    return 0;
+  }
+  std::vector<Tile> tiles;
+  tiles.reserve(ntiles);
+  for (size_t o = 0; o < outs.size(); o++) {
     const int tm = (outs[o].m + BM - 1) / BM, tn = (outs[o].n + BN - 1) / BN;
     for (int a = 0; a < tm; a++)
-      for (int b = 0; b < tn; b++)
-        tiles.push_back({(int)o, a, b, (int)std::min<int64_t>(kt, INT_MAX / 2)});
+      for (int b = 0; b < tn; b++) tiles.push_back({(int)o, a, b, kts[o]});
   }
-  if (tiles.empty()) return 0;
   grid = std::max(1, grid);
   std::vector<std::vector<DUnit>> per;
   int64_t nslots = 0;
@@ -404,11 +436,8 @@ int64_t make_f64_units(const std::vector<DOut>& outs, const std::vector<DSeg>& s
       nslots = ns2;
     }
   }
-  size_t len = 0, n = 0;
-  for (auto& v : per) {
-    len = std::max(len, v.size());
-    n += v.size();
-  }
+  size_t len = 0;
+  for (auto& v : per) len = std::max(len, v.size());
   if (len <= 1) {  // one unit per CTA at most: no padding entries
     for (auto& v : per)
       for (auto& u : v) units.push_back(u);
@@ -420,7 +449,6 @@ int64_t make_f64_units(const std::vector<DOut>& outs, const std::vector<DSeg>& s
   units.assign(len * (size_t)grid, pad);
   for (int c = 0; c < grid; c++)
     for (size_t j = 0; j < per[c].size(); j++) units[j * grid + c] = per[c][j];
-  (void)n;
   return nslots;
 }
 

@@ -22,8 +22,9 @@ int f64_split_mode();
 // CTA (mode 0); or (mode 1 when that shortens the longest CTA by a tenth, mode 2
 // always) the k-tiles of all tiles cut into equal per-CTA shares, a tile that
 // crosses a share boundary split along K into parts.  The units are laid out for
-// the kernel's grid-stride walk.  Returns the number of workspace slots (and
-// tickets) they use.
+// the kernel's grid-stride walk.  A negative mode lists the whole tiles in order
+// with no assignment (host work linear in the tiles, for one-off contractions of
+// many short tiles).  Returns the number of workspace slots (and tickets) they use.
 int64_t make_f64_units(const std::vector<DOut>& outs, const std::vector<DSeg>& segs, int grid,
                        int mode, std::vector<DUnit>& units);
 

@@ -136,32 +136,79 @@ int64_t label_key(const std::vector<int>& st, const std::vector<std::vector<int>
   return loc;
 }
 
+// Page-locked staging of descriptor uploads.  A cudaMemcpyAsync from pageable
+// memory larger than a few tens of KB waits for the work already on the stream,
+// which would hold the host at every contraction until the GPU catches up.  Each
+// device has a ring of page-locked buffers; a buffer is reused once the copy that
+// last read it has finished (its event), kSlots uploads later.
+struct StagingRing {
+  static constexpr int kSlots = 8;
+  struct Slot {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaEvent_t ev = nullptr;
+  };
+  std::mutex mu;
+  Slot slot[kSlots];
+  int next = 0;
+};
+
+StagingRing* staging_ring(int device) {
+  constexpr int kMaxDev = 64;
+  static StagingRing rings[kMaxDev];
+  return device >= 0 && device < kMaxDev ? &rings[device] : nullptr;
+}
+
+// dst (device) <- the n host pieces src[i] of len[i] bytes at byte offsets off[i]
+cudaError_t staged_upload(const Engine& E, void* dst, size_t total, int n, const void* const* src,
+                          const size_t* off, const size_t* len) {
+  StagingRing* R = staging_ring(E.device);
+  if (!R) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> g(R->mu);
+  StagingRing::Slot& sl = R->slot[R->next];
+  R->next = (R->next + 1) % StagingRing::kSlots;
+  cudaError_t e = sl.ev ? cudaEventSynchronize(sl.ev)
+                        : cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming);
+  if (e != cudaSuccess) return e;
+  if (sl.cap < total) {
+    if (sl.p) cudaFreeHost(sl.p);
+    sl.p = nullptr;
+    sl.cap = 0;
+    const size_t cap = std::max<size_t>(total + total / 2, 256 << 10);
+    if ((e = cudaMallocHost(&sl.p, cap)) != cudaSuccess) return e;
+    sl.cap = cap;
+  }
+  for (int i = 0; i < n; i++)
+    if (len[i]) std::memcpy(static_cast<unsigned char*>(sl.p) + off[i], src[i], len[i]);
+  if ((e = cudaMemcpyAsync(dst, sl.p, total, cudaMemcpyHostToDevice, E.stream)) != cudaSuccess)
+    return e;
+  return cudaEventRecord(sl.ev, E.stream);
+}
+
 // grouped NT GEMM over (C_o = sum_s A_s B_s^T) descriptors, uploaded per call
 cudaError_t run_gemms(const Engine& E, const double* A, const double* B, double* C,
                       std::vector<DOut>& outs, std::vector<DSeg>& segs) {
   if (outs.empty()) return cudaSuccess;
   const int grid = E.num_sms * 3;
   std::vector<DUnit> units;
-  make_f64_units(outs, segs, grid, 0, units);  // whole tiles: no workspace
+  make_f64_units(outs, segs, grid, -1, units);  // whole tiles in order: no workspace
   if (units.empty()) return cudaSuccess;
-  DOut* d_o = nullptr;
-  DSeg* d_s = nullptr;
-  DUnit* d_t = nullptr;
-  cudaError_t e = dalloc(&d_o, outs.size(), E.stream);
-  if (e == cudaSuccess) e = dalloc(&d_s, segs.size(), E.stream);
-  if (e == cudaSuccess) e = dalloc(&d_t, units.size(), E.stream);
+  // one device block [outs | segs | units], 256-byte aligned parts
+  auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+  const size_t len[3] = {sizeof(DOut) * outs.size(), sizeof(DSeg) * segs.size(),
+                         sizeof(DUnit) * units.size()};
+  const size_t off[3] = {0, up(len[0]), up(len[0]) + up(len[1])};
+  const size_t total = off[2] + len[2];
+  const void* src[3] = {outs.data(), segs.data(), units.data()};
+  unsigned char* d = nullptr;
+  cudaError_t e = dalloc(&d, total, E.stream);
+  if (e == cudaSuccess) e = staged_upload(E, d, total, 3, src, off, len);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(d_o, outs.data(), sizeof(DOut) * outs.size(), cudaMemcpyHostToDevice, E.stream);
-  if (e == cudaSuccess && !segs.empty())
-    e = cudaMemcpyAsync(d_s, segs.data(), sizeof(DSeg) * segs.size(), cudaMemcpyHostToDevice, E.stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(d_t, units.data(), sizeof(DUnit) * units.size(), cudaMemcpyHostToDevice, E.stream);
-  if (e == cudaSuccess)
-    e = launch_grouped_f64(A, B, C, d_t, (int)units.size(), d_o, d_s, E.f == 2, grid, E.stream,
+    e = launch_grouped_f64(A, B, C, reinterpret_cast<const DUnit*>(d + off[2]), (int)units.size(),
+                           reinterpret_cast<const DOut*>(d + off[0]),
+                           reinterpret_cast<const DSeg*>(d + off[1]), E.f == 2, grid, E.stream,
                            nullptr, nullptr);
-  dfree(d_o, E.stream);
-  dfree(d_s, E.stream);
-  dfree(d_t, E.stream);
+  dfree(d, E.stream);
   return e;
 }
 
