@@ -27,10 +27,15 @@
 #include <cstdlib>
 #include <vector>
 
+#include <string>
+
+#include "../../include/dmrgx.h"
 #include "grouped.h"
 #include "kernels.h"
 
 namespace dmrgx {
+
+void set_error(const std::string& msg);
 
 namespace {
 
@@ -482,3 +487,50 @@ cudaError_t launch_grouped_f64(const double* A, const double* B, double* C, cons
 }
 
 }  // namespace dmrgx
+
+extern "C" int dmrgx_f64_units(int n_outs, const int* out_desc, const int* seg_k, int grid,
+                               int mode, int* units, int64_t cap, int64_t* n_units,
+                               int64_t* n_slots) {
+  using namespace dmrgx;
+  if (n_outs < 0 || (n_outs > 0 && (!out_desc || !seg_k)) || grid < 1 || !n_units || !n_slots ||
+      cap < 0 || (cap > 0 && !units) || mode < -1 || mode > 2) {
+    set_error("f64_units: bad argument");
+    return DMRGX_E_ARG;
+  }
+  std::vector<DOut> outs(n_outs);
+  std::vector<DSeg> segs;
+  for (int i = 0; i < n_outs; i++) {
+    const int m = out_desc[3 * i], n = out_desc[3 * i + 1], ns = out_desc[3 * i + 2];
+    if (m < 0 || n < 0 || ns < 0 || (m + f64_tile_m() - 1) / f64_tile_m() > 32767 ||
+        (n + f64_tile_n() - 1) / f64_tile_n() > 32767) {
+      set_error("f64_units: bad output block extent");
+      return DMRGX_E_ARG;
+    }
+    DOut& o = outs[i];
+    o.c_off = 0;
+    o.m = m;
+    o.n = n;
+    o.seg_begin = (int32_t)segs.size();
+    o.seg_count = ns;
+    for (int q = 0; q < ns; q++) {
+      DSeg g;
+      g.a_off = g.b_off = 0;
+      g.k = seg_k[o.seg_begin + q];
+      g.pad_ = 0;
+      if (g.k < 0) {
+        set_error("f64_units: negative K extent");
+        return DMRGX_E_ARG;
+      }
+      segs.push_back(g);
+    }
+  }
+  std::vector<DUnit> u;
+  *n_slots = make_f64_units(outs, segs, grid, mode, u);
+  *n_units = (int64_t)u.size();
+  for (int64_t j = 0; j < std::min<int64_t>(cap, (int64_t)u.size()); j++) {
+    const DUnit& x = u[j];
+    const int v[8] = {x.out, x.tm, x.tn, x.kt0, x.kt1, x.slot, x.part, x.nparts};
+    for (int q = 0; q < 8; q++) units[8 * j + q] = v[q];
+  }
+  return DMRGX_OK;
+}

@@ -58,6 +58,7 @@ SIGNATURES = {
                         _dp]),
     "dmrgx_set_schedule": (_i, [_vp, _i]),
     "dmrgx_split_tuning": (_i, [_vp, _ip, _i]),
+    "dmrgx_f64_units": (_i, [_i, _ip, _ip, _i, _i, _ip, _i64, _i64p, _i64p]),
     "dmrgx_matvec_launches": (_i, [_vp, _ip]),
     "dmrgx_step_seconds": (_i, [_vp, _dp, _i64, _i64p]),
     "dmrgx_singular": (_i, [_vp, _dp, _dp, _ip, _i64, _i64p]),
@@ -124,6 +125,25 @@ def build_maps(lenv_meta, renv_meta, l_num, r_num, sector, group_n, fermion):
                                   _i64p(info), _ip(rmap), rmap.shape[0], _ip(lmap),
                                   lmap.shape[0]))
     return int(info[0]), int(info[1]), rmap[: info[2]], lmap[: info[3]]
+
+
+def f64_units(out_desc, seg_k, grid, mode):
+    """Host-only work units of the FP64 grouped kernel for one stage: out_desc rows
+    (rows, real columns, segment count) per output block, seg_k the segments' K
+    extents block by block.  Returns (units as an (n, 8) int array: out, tm, tn, kt0,
+    kt1, slot, part, nparts; workspace slots)."""
+    od = np.ascontiguousarray(np.asarray(out_desc, np.int32).reshape(-1))
+    sk = np.ascontiguousarray(np.asarray(seg_k, np.int32).reshape(-1))
+    if sk.size == 0:
+        sk = np.zeros(1, np.int32)
+    cnt = np.zeros(1, np.int64)
+    slots = np.zeros(1, np.int64)
+    _check(lib().dmrgx_f64_units(od.size // 3, _ip(od), _ip(sk), grid, mode, None, 0,
+                                 _i64p(cnt), _i64p(slots)))
+    units = np.zeros((max(1, int(cnt[0])), 8), np.int32)
+    _check(lib().dmrgx_f64_units(od.size // 3, _ip(od), _ip(sk), grid, mode, _ip(units),
+                                 int(cnt[0]), _i64p(cnt), _i64p(slots)))
+    return units[: int(cnt[0])], int(slots[0])
 
 
 def build_maps_pbc(lenv_meta, renv_meta, ledge_meta, redge_meta, l_num, r_num, sector, group_n,

@@ -100,6 +100,20 @@ int dmrgx_matvec_launches(dmrgx_ctx* ctx, int* out);
  * measured for this plan (0: from the cache).  cap >= 8. */
 int dmrgx_split_tuning(dmrgx_ctx* ctx, int* out, int cap);
 
+/* The work units the FP64 grouped kernel runs for one stage (host only: no
+ * context, no device work).  The stage is n_outs output blocks; block i is
+ * out_desc[3i..3i+2] = (rows, real columns, segment count), and seg_k lists the
+ * real K extent of every segment, block by block.  grid: CTAs; mode: 0 whole
+ * 64 x 64 tiles longest first onto the least-loaded CTA, 1 equal per-CTA shares
+ * of all k-tiles (stream-K) where they shorten the longest CTA by a tenth, 2
+ * always shares, -1 tiles in order (the matvec stages use DMRGX_F64_SPLIT, default
+ * 1).  Writes min(cap, count) units of 8 ints (out, tm, tn, kt0, kt1, slot, part,
+ * nparts; k-tiles 16 wide; out = -1 marks a padding entry; unit j runs on CTA
+ * j % grid unless mode is -1 or there are at most grid units), the count to
+ * *n_units and the K-split workspace slots to *n_slots. */
+int dmrgx_f64_units(int n_outs, const int* out_desc, const int* seg_k, int grid, int mode,
+                    int* units, int64_t cap, int64_t* n_units, int64_t* n_slots);
+
 /* Select the launch schedule of the matvec (DMRGX_SCHED_*).  Default grouped.
  * The per-block schedule is the plain FP64 GPU path: same plan, same
  * eigensolver, one library GEMM per task row with the row's sign as alpha. */
