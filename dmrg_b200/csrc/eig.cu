@@ -930,6 +930,8 @@ int eigsolve_impl(dmrgx_ctx* c, int nev, int ncv, double tol, int maxiter, const
     set_error(std::string("eigsolve: ") + err_attr);
     return DMRGX_E_CUDA;
   }
+  // before the cycles are captured: the matvec's FP64 kernel sets its attribute once
+  EIG_TRY(prepare_f64_gemm());
   int rc = L.init();
   if (rc) return rc;
   const int m = L.m, td = L.tdim;

@@ -457,10 +457,7 @@ int64_t make_f64_units(const std::vector<DOut>& outs, const std::vector<DSeg>& s
   return nslots;
 }
 
-cudaError_t launch_grouped_f64(const double* A, const double* B, double* C, const DUnit* units,
-                               int nunits, const DOut* outs, const DSeg* segs, bool cplx,
-                               int grid, cudaStream_t st, double* ws, int* tickets) {
-  if (nunits <= 0) return cudaSuccess;
+cudaError_t prepare_f64_gemm() {
   // opt the kernels in to their shared memory, once per device
   static std::atomic<unsigned long long> ready{0};
   int dev = 0;
@@ -476,6 +473,15 @@ cudaError_t launch_grouped_f64(const double* A, const double* B, double* C, cons
     if (e != cudaSuccess) return e;
     ready.fetch_or(bit);
   }
+  return cudaSuccess;
+}
+
+cudaError_t launch_grouped_f64(const double* A, const double* B, double* C, const DUnit* units,
+                               int nunits, const DOut* outs, const DSeg* segs, bool cplx,
+                               int grid, cudaStream_t st, double* ws, int* tickets) {
+  if (nunits <= 0) return cudaSuccess;
+  cudaError_t e = prepare_f64_gemm();
+  if (e != cudaSuccess) return e;
   if (grid > nunits) grid = nunits;
   if (cplx)
     grouped_gemm_nt_f64<true><<<grid, THREADS, kSmemBytes, st>>>(A, B, C, units, nunits, outs,

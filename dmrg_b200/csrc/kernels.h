@@ -28,6 +28,10 @@ int f64_split_mode();
 int64_t make_f64_units(const std::vector<DOut>& outs, const std::vector<DSeg>& segs, int grid,
                        int mode, std::vector<DUnit>& units);
 
+// Opt the FP64 grouped kernel in to its shared memory on the current device (once;
+// call outside any stream capture, launch_grouped_f64 also calls it).
+cudaError_t prepare_f64_gemm();
+
 // FP64 grouped segmented GEMM (gemm_f64.cu).  cplx: interleaved complex operands.
 // ws / tickets: workspace of 4096 doubles and one zero-initialised int per slot
 // (null when the units use none); the kernel leaves the tickets at zero.
